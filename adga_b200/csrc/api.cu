@@ -1,0 +1,901 @@
+// C ABI of libadga_b200: handle, data staging and the batched (q, omega)
+// loop of src/main.F90:486-799 on one GPU.  See include/adga.h for the
+// contract of every entry point.
+#include "adga.h"
+#include "ctx.cuh"
+#include "lu.cuh"
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+// tensor-core trailing update of the mixed path (k_tc.cu)
+cudaError_t tc_trail_setup(void **ctx, z32 *M, const LUBatch &lb, cudaStream_t st);
+cudaError_t tc_trail_run(void *ctx, int J, int jb, cudaStream_t st);
+void tc_trail_free(void *ctx);
+int tc_available();
+
+struct adga_handle {
+  adga_dims d{};
+  DevCtx c{};
+  int nw = 0, nnu_all = 0, nd4 = 0;
+  bool bigbox = false;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::string err;
+  std::vector<void *> owned;
+  // vertex store, one pair per omega
+  std::vector<z64 *> vd, vm;
+  // local block
+  int diag_iwb = INT_MIN, loc_iwb = INT_MIN;
+  z64 *c0inv = nullptr, *c0w = nullptr, *bubtmp = nullptr;
+  z64 *Frow_d = nullptr, *Frow_m = nullptr, *gam_d = nullptr, *gam_m = nullptr;
+  z64 *opg_d = nullptr, *opg_m = nullptr;
+  // accumulators
+  z64 *bubble_loc = nullptr, *chi_loc_d = nullptr, *chi_loc_m = nullptr;
+  z64 *sigma_nl = nullptr, *sigma_dmft = nullptr, *sigma_hf = nullptr;
+  z64 *chi_qw_d = nullptr, *chi_qw_m = nullptr, *bubble_nl = nullptr;
+  int out_cap = 0, last_npts = 0;
+  // batch work buffers (sized on demand)
+  int cap = 0, cap_prec = -1;
+  std::vector<void *> work;
+  z64 *chi0_all = nullptr, *chi0q_big = nullptr, *gq = nullptr, *mtot = nullptr;
+  z64 *etad = nullptr, *etam = nullptr;
+  int *qidx_d = nullptr, *qidx_h = nullptr;
+  void *Tm = nullptr, *Linv = nullptr, *Uinv = nullptr;
+  int *ipiv = nullptr, *info = nullptr;
+  int NB = 64;
+  z64 *X64 = nullptr, *XD = nullptr;
+  z32 *V32 = nullptr, *work32 = nullptr;
+  unsigned long long *norms = nullptr;
+  void *tc = nullptr;
+  // refinement settings
+  int max_iter = 8;
+  double tol = 1e-12;
+  // last-run statistics
+  adga_run_stats stats{};
+};
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t _e = (call);                                                      \
+    if (_e != cudaSuccess) {                                                      \
+      h->err = std::string(#call) + ": " + cudaGetErrorString(_e);                \
+      return ADGA_ECUDA;                                                          \
+    }                                                                             \
+  } while (0)
+
+static int fail(adga_handle *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+static void *dalloc(adga_handle *h, size_t bytes, std::vector<void *> &list) {
+  void *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  list.push_back(p);
+  return p;
+}
+
+template <typename P>
+static bool alloc_into(adga_handle *h, P *&ptr, size_t count, std::vector<void *> &list) {
+  ptr = (P *)dalloc(h, count * sizeof(P), list);
+  return ptr != nullptr;
+}
+
+static void free_list(std::vector<void *> &list) {
+  for (void *p : list) cudaFree(p);
+  list.clear();
+}
+
+extern "C" const char *adga_last_error(const adga_handle *h) {
+  return h ? h->err.c_str() : "null handle";
+}
+
+// ---------------------------------------------------------------------------
+extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga_z *hk,
+                           const adga_z *siw, const adga_z *giw, const adga_z *dc,
+                           const adga_z *u, const adga_z *u_tilde, const adga_z *n_dmft,
+                           const int *q_data, const int *k_data_eom, adga_handle **out) {
+  if (!d || !out || !iw_data || !hk || !siw || !giw || !u || !u_tilde || !n_dmft || !q_data)
+    return ADGA_EINVAL;
+  *out = nullptr;
+  if (d->ndim < 1 || d->ndim > 5) return ADGA_EINVAL;
+  if (d->nkpx < 1 || d->nkpy < 1 || d->nkpz < 1 || d->nqpx < 1 || d->nqpy < 1 || d->nqpz < 1)
+    return ADGA_EINVAL;
+  if (d->nkpx % d->nqpx || d->nkpy % d->nqpy || d->nkpz % d->nqpz) return ADGA_EINVAL;
+  if (d->iwfmax_small < 1 || d->iwbmax_small < 0) return ADGA_EINVAL;
+  if (d->iwmax < d->iwfmax_small + d->iwbmax_small) return ADGA_EINVAL;   // check_freq_range
+  if (d->iwstart > -d->iwfmax_small || d->iwstop < d->iwfmax_small - 1) return ADGA_EINVAL;
+  if (d->iwstart - d->iwbmax_small < -d->iwmax || d->iwstop + d->iwbmax_small > d->iwmax - 1)
+    return ADGA_EINVAL;
+  adga_handle *h = new adga_handle();
+  h->d = *d;
+  DevCtx &c = h->c;
+  c.nd = d->ndim; c.nd2 = d->ndim * d->ndim;
+  c.nkpx = d->nkpx; c.nkpy = d->nkpy; c.nkpz = d->nkpz;
+  c.nkp = d->nkpx * d->nkpy * d->nkpz;
+  c.nqp = d->nqpx * d->nqpy * d->nqpz;
+  c.nkp_eom = d->nkp_eom > 0 ? d->nkp_eom : c.nkp;
+  c.iwmax = d->iwmax; c.iwf = d->iwfmax_small; c.iwb = d->iwbmax_small;
+  c.N = c.nd2 * 2 * c.iwf; c.R = c.nd2;
+  c.iwstart = d->iwstart; c.iwstop = d->iwstop;
+  c.nu_lo = d->iwstart - d->iwbmax_small;
+  c.nnu = (d->iwstop + d->iwbmax_small) - c.nu_lo + 1;
+  c.beta = d->beta; c.mu = d->mu;
+  h->nw = 2 * c.iwb + 1;
+  h->nnu_all = d->iwstop - d->iwstart + 1;
+  h->bigbox = h->nnu_all != 2 * c.iwf;
+  h->nd4 = c.nd2 * c.nd2;
+  const char *ev = getenv("ADGA_NB");
+  if (ev) h->NB = std::max(16, std::min(128, atoi(ev) / 8 * 8));
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return ADGA_ECUDA;
+  }
+  cudaEventCreate(&h->e0);
+  cudaEventCreate(&h->e1);
+  auto &L = h->owned;
+  const int nd = c.nd, nd2 = c.nd2, n2w = 2 * c.iwmax;
+  double *iw; z64 *hk_d, *siw_d, *giw_d, *dc_d, *u_d, *ut_d, *nd_d, *gt;
+  int *qd, *kq, *kqe, *kde = nullptr;
+  bool ok = alloc_into(h, iw, n2w, L) && alloc_into(h, hk_d, (size_t)c.nkp * nd2, L) &&
+            alloc_into(h, siw_d, (size_t)n2w * nd, L) && alloc_into(h, giw_d, (size_t)n2w * nd, L) &&
+            alloc_into(h, dc_d, 2 * nd, L) && alloc_into(h, u_d, nd2 * nd2, L) &&
+            alloc_into(h, ut_d, nd2 * nd2, L) && alloc_into(h, nd_d, nd, L) &&
+            alloc_into(h, gt, (size_t)c.nnu * c.nkp * nd2, L) && alloc_into(h, qd, c.nqp, L) &&
+            alloc_into(h, kq, (size_t)c.nkp * c.nqp, L) && alloc_into(h, kqe, (size_t)c.nkp_eom * c.nqp, L);
+  if (ok && k_data_eom) ok = alloc_into(h, kde, c.nkp_eom, L);
+  if (!ok) { adga_destroy(h); return ADGA_ENOMEM; }
+  std::vector<z64> dcz(2 * nd, make_double2(0.0, 0.0));
+  if (dc) memcpy(dcz.data(), dc, sizeof(z64) * 2 * nd);
+  cudaStream_t st = h->st;
+#define UP(dst, src, n) CK(cudaMemcpyAsync(dst, src, (n), cudaMemcpyHostToDevice, st))
+  UP(iw, iw_data, sizeof(double) * n2w);
+  UP(hk_d, hk, sizeof(z64) * c.nkp * nd2);
+  UP(siw_d, siw, sizeof(z64) * n2w * nd);
+  UP(giw_d, giw, sizeof(z64) * n2w * nd);
+  UP(dc_d, dcz.data(), sizeof(z64) * 2 * nd);
+  UP(u_d, u, sizeof(z64) * nd2 * nd2);
+  UP(ut_d, u_tilde, sizeof(z64) * nd2 * nd2);
+  UP(nd_d, n_dmft, sizeof(z64) * nd);
+  UP(qd, q_data, sizeof(int) * c.nqp);
+  if (kde) UP(kde, k_data_eom, sizeof(int) * c.nkp_eom);
+#undef UP
+  c.iw = iw; c.hk = hk_d; c.siw = siw_d; c.giw = giw_d; c.dc = dc_d;
+  c.u = u_d; c.ut = ut_d; c.ndmft = nd_d; c.kq = kq; c.kqe = kqe; c.gtab = gt;
+  CK(launch_kq_index(c.nkpx, c.nkpy, c.nkpz, nullptr, c.nkp, qd, c.nqp, 0, kq, st));
+  if (c.nkp_eom == c.nkp && !kde)
+    CK(cudaMemcpyAsync(kqe, kq, sizeof(int) * c.nkp * c.nqp, cudaMemcpyDeviceToDevice, st));
+  else
+    CK(launch_kq_index(c.nkpx, c.nkpy, c.nkpz, kde, c.nkp_eom, qd, c.nqp, 0, kqe, st));
+  CK(launch_gtable(c, gt, st));
+  // per-omega local buffers and accumulators
+  const size_t N = c.N;
+  ok = alloc_into(h, h->c0inv, N, L) && alloc_into(h, h->c0w, N, L) &&
+       alloc_into(h, h->bubtmp, nd2 * nd2, L) && alloc_into(h, h->Frow_d, N * N, L) &&
+       alloc_into(h, h->Frow_m, N * N, L) && alloc_into(h, h->gam_d, nd2 * N, L) &&
+       alloc_into(h, h->gam_m, nd2 * N, L) && alloc_into(h, h->opg_d, nd2 * N, L) &&
+       alloc_into(h, h->opg_m, nd2 * N, L) &&
+       alloc_into(h, h->bubble_loc, (size_t)h->nd4 * h->nw, L) &&
+       alloc_into(h, h->chi_loc_d, (size_t)h->nd4 * h->nw, L) &&
+       alloc_into(h, h->chi_loc_m, (size_t)h->nd4 * h->nw, L) &&
+       alloc_into(h, h->sigma_nl, (size_t)nd2 * 2 * c.iwf * c.nkp_eom, L) &&
+       alloc_into(h, h->sigma_dmft, (size_t)nd2 * 2 * c.iwf, L) &&
+       alloc_into(h, h->sigma_hf, (size_t)nd2 * c.nkp_eom, L);
+  if (!ok) { adga_destroy(h); return ADGA_ENOMEM; }
+  h->vd.assign(h->nw, nullptr);
+  h->vm.assign(h->nw, nullptr);
+  CK(cudaStreamSynchronize(st));
+  *out = h;
+  return adga_reset_outputs(h);
+}
+
+extern "C" int adga_destroy(adga_handle *h) {
+  if (!h) return 0;
+  if (h->st) cudaStreamSynchronize(h->st);
+  if (h->tc) tc_trail_free(h->tc);
+  free_list(h->work);
+  free_list(h->owned);
+  for (auto p : h->vd) if (p) cudaFree(p);
+  for (auto p : h->vm) if (p) cudaFree(p);
+  if (h->qidx_h) cudaFreeHost(h->qidx_h);
+  if (h->e0) cudaEventDestroy(h->e0);
+  if (h->e1) cudaEventDestroy(h->e1);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return 0;
+}
+
+extern "C" int adga_device_bytes(const adga_handle *h, long long *bytes) {
+  if (!h || !bytes) return ADGA_EINVAL;
+  size_t f = 0, t = 0;
+  cudaMemGetInfo(&f, &t);
+  *bytes = (long long)(t - f);
+  return 0;
+}
+
+extern "C" int adga_reset_outputs(adga_handle *h) {
+  if (!h) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  cudaStream_t st = h->st;
+  CK(cudaMemsetAsync(h->bubble_loc, 0, sizeof(z64) * h->nd4 * h->nw, st));
+  CK(cudaMemsetAsync(h->chi_loc_d, 0, sizeof(z64) * h->nd4 * h->nw, st));
+  CK(cudaMemsetAsync(h->chi_loc_m, 0, sizeof(z64) * h->nd4 * h->nw, st));
+  CK(cudaMemsetAsync(h->sigma_nl, 0, sizeof(z64) * c.nd2 * 2 * c.iwf * c.nkp_eom, st));
+  CK(cudaMemsetAsync(h->sigma_dmft, 0, sizeof(z64) * c.nd2 * 2 * c.iwf, st));
+  CK(cudaMemsetAsync(h->sigma_hf, 0, sizeof(z64) * c.nd2 * c.nkp_eom, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+extern "C" int adga_set_vertex(adga_handle *h, int iwb, const adga_z *chi_d, const adga_z *chi_m) {
+  if (!h || !chi_d || !chi_m) return ADGA_EINVAL;
+  if (iwb < -h->c.iwb || iwb > h->c.iwb) return fail(h, ADGA_EINVAL, "iwb out of range");
+  const int w = iwb + h->c.iwb;
+  const size_t n = (size_t)h->c.N * h->c.N;
+  if (!h->vd[w]) {
+    if (cudaMalloc(&h->vd[w], n * sizeof(z64)) != cudaSuccess) return fail(h, ADGA_ENOMEM, "vertex alloc");
+    if (cudaMalloc(&h->vm[w], n * sizeof(z64)) != cudaSuccess) return fail(h, ADGA_ENOMEM, "vertex alloc");
+  }
+  CK(cudaMemcpyAsync(h->vd[w], chi_d, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->vm[w], chi_m, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  if (h->loc_iwb == iwb) h->loc_iwb = INT_MIN;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+static int ensure_diag(adga_handle *h, int iwb) {
+  if (h->diag_iwb == iwb) return 0;
+  CK(launch_local_diag(h->c, iwb, h->c0inv, h->c0w, h->bubtmp, h->st));
+  h->diag_iwb = iwb;
+  h->loc_iwb = INT_MIN;
+  return 0;
+}
+
+// src/main.F90:506-627 for omega = iwb
+static int ensure_local(adga_handle *h, int iwb) {
+  if (h->loc_iwb == iwb) return 0;
+  const int w = iwb + h->c.iwb;
+  if (!h->vd[w]) return fail(h, ADGA_ESTATE, "vertex of omega " + std::to_string(iwb) + " not set");
+  int r = ensure_diag(h, iwb);
+  if (r) return r;
+  CK(launch_local_F(h->c, h->vd[w], h->c0inv, h->Frow_d, h->st));
+  CK(launch_local_F(h->c, h->vm[w], h->c0inv, h->Frow_m, h->st));
+  CK(launch_local_gamma(h->c, h->Frow_d, h->gam_d, h->opg_d, h->st));
+  CK(launch_local_gamma(h->c, h->Frow_m, h->gam_m, h->opg_m, h->st));
+  h->loc_iwb = iwb;
+  return 0;
+}
+
+static size_t bytes_per_point(const adga_handle *h, int prec, int NB) {
+  const DevCtx &c = h->c;
+  const size_t N = c.N, R = c.R, nd2 = c.nd2;
+  const size_t nsteps = (N + NB - 1) / NB;
+  size_t b = 0;
+  b += h->nd4 * (size_t)h->nnu_all * 16 + (h->bigbox ? h->nd4 * 2 * c.iwf * 16 : 0);
+  b += 3 * nd2 * N * 16 + nd2 * c.iwf * nd2 * 16 + 2 * N * 4 + 16;
+  if (prec == ADGA_FP64) {
+    b += 2 * N * (N + R) * 16 + 2 * 2 * nsteps * NB * NB * 16;
+  } else {
+    b += 2 * N * (N + R) * 8 + 2 * 2 * nsteps * NB * NB * 8;
+    b += 2 * 2 * R * N * 16 + 2 * R * N * 8 + 2 * ((R + 15) / 16) * 16 * N * 8 + 64;
+  }
+  return b;
+}
+
+static int ensure_work(adga_handle *h, int prec, int want) {
+  const DevCtx &c = h->c;
+  if (h->cap_prec == prec && h->cap >= want) return 0;
+  cudaStreamSynchronize(h->st);
+  if (h->tc) { tc_trail_free(h->tc); h->tc = nullptr; }
+  free_list(h->work);
+  h->cap = 0;
+  h->cap_prec = -1;
+  const int NB = prec == ADGA_FP64 ? 64 : h->NB;
+  size_t per = bytes_per_point(h, prec, NB);
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  double frac = 0.6;
+  const char *e = getenv("ADGA_WORK_FRAC");
+  if (e) frac = atof(e);
+  size_t budget = (size_t)(fr * frac);
+  int cap = (int)std::min<size_t>((size_t)want, std::max<size_t>(1, budget / per));
+  const char *eb = getenv("ADGA_BATCH");
+  if (eb) cap = std::max(1, std::min(cap, atoi(eb)));
+  const size_t N = c.N, R = c.R, nd2 = c.nd2, nsteps = (N + NB - 1) / NB;
+  auto &W = h->work;
+  bool ok = alloc_into(h, h->chi0_all, (size_t)cap * h->nd4 * h->nnu_all, W) &&
+            alloc_into(h, h->gq, (size_t)cap * nd2 * N, W) &&
+            alloc_into(h, h->mtot, (size_t)cap * nd2 * c.iwf * nd2, W) &&
+            alloc_into(h, h->etad, (size_t)cap * nd2 * N, W) &&
+            alloc_into(h, h->etam, (size_t)cap * nd2 * N, W) &&
+            alloc_into(h, h->qidx_d, cap, W) && alloc_into(h, h->ipiv, (size_t)2 * cap * N, W) &&
+            alloc_into(h, h->info, (size_t)2 * cap, W);
+  if (ok && h->bigbox) ok = alloc_into(h, h->chi0q_big, (size_t)cap * h->nd4 * 2 * c.iwf, W);
+  if (ok) {
+    const size_t es = prec == ADGA_FP64 ? 16 : 8;
+    h->Tm = dalloc(h, (size_t)2 * cap * N * (N + R) * es, W);
+    h->Linv = dalloc(h, (size_t)2 * cap * nsteps * NB * NB * es, W);
+    h->Uinv = dalloc(h, (size_t)2 * cap * nsteps * NB * NB * es, W);
+    ok = h->Tm && h->Linv && h->Uinv;
+  }
+  if (ok && prec == ADGA_MIXED) {
+    ok = alloc_into(h, h->X64, (size_t)2 * cap * R * N, W) &&
+         alloc_into(h, h->XD, (size_t)2 * cap * R * N, W) &&
+         alloc_into(h, h->V32, (size_t)2 * cap * R * N, W) &&
+         alloc_into(h, h->work32, (size_t)2 * cap * ((R + 15) / 16) * 16 * N, W) &&
+         alloc_into(h, h->norms, (size_t)4 * cap, W);
+  }
+  if (!ok) {
+    free_list(h->work);
+    return fail(h, ADGA_ENOMEM, "batch work buffers (" + std::to_string(cap) + " points)");
+  }
+  if (h->qidx_h) cudaFreeHost(h->qidx_h);
+  CK(cudaMallocHost(&h->qidx_h, sizeof(int) * cap));
+  h->cap = cap;
+  h->cap_prec = prec;
+  if (prec == ADGA_MIXED && tc_available() && !getenv("ADGA_NO_TC")) {
+    LUBatch lb{(int)N, (int)(N + R), 2 * cap, NB, N * (N + R), h->ipiv, h->info, h->Linv, h->Uinv};
+    if (tc_trail_setup(&h->tc, (z32 *)h->Tm, lb, h->st) != cudaSuccess) h->tc = nullptr;
+  }
+  return 0;
+}
+
+static void stage_ms(adga_handle *h, double *acc, cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) *acc += ms;
+}
+
+// one batch of np consecutive q at omega = iwb: chi0 -> build -> LU/solve -> post -> EOM.
+// qidx_h[0..np) hold the 0-based q indices; outputs go to point slot `off`.
+static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *status,
+                     z64 *chi_qw_d, z64 *chi_qw_m, z64 *bub_nl, bool do_eom, bool do_chi) {
+  DevCtx &c = h->c;
+  cudaStream_t st = h->st;
+  const size_t N = c.N, R = c.R;
+  const int NB = prec == ADGA_FP64 ? 64 : h->NB;
+  cudaEvent_t ev[6];
+  for (int i = 0; i < 6; ++i) cudaEventCreate(&ev[i]);
+  CK(cudaMemcpyAsync(h->qidx_d, h->qidx_h, sizeof(int) * np, cudaMemcpyHostToDevice, st));
+  cudaEventRecord(ev[0], st);
+  CK(launch_chi0(c, iwb, h->qidx_d, np, h->chi0_all, h->nnu_all, st));
+  z64 *chi0q = h->bigbox ? h->chi0q_big : h->chi0_all;
+  CK(launch_chi0_finish(c, h->chi0_all, h->nnu_all, np, h->bubtmp, h->bigbox ? chi0q : nullptr,
+                        do_chi ? bub_nl + (size_t)off * h->nd4 : nullptr, st));
+  cudaEventRecord(ev[1], st);
+  const size_t strideM = N * (N + R);
+  LUBatch lb{(int)N, (int)(N + R), 2 * np, NB, strideM, h->ipiv, h->info, h->Linv, h->Uinv};
+  CK(cudaMemsetAsync(h->info, 0, sizeof(int) * 2 * np, st));
+  const z64 *X = nullptr;
+  size_t sp = 0, sc = 0;
+  int mixed_fail = 0, iters = 0;
+  double worst = 0.0;
+  std::vector<int> fallback;
+  if (prec == ADGA_FP64) {
+    z64 *T = (z64 *)h->Tm;
+    CK(launch_bse_build<z64>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
+                             strideM, h->gq, st));
+    cudaEventRecord(ev[2], st);
+    CK(lu_factor<z64>(T, lb, false, nullptr, nullptr, st));
+    CK(lu_backsolve<z64>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
+    X = T + N * N; sp = 2 * strideM; sc = strideM;
+  } else {
+    z32 *T = (z32 *)h->Tm;
+    CK(launch_bse_build<z32>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
+                             strideM, h->gq, st));
+    cudaEventRecord(ev[2], st);
+    if (h->tc) {
+      CK(lu_factor<z32>(T, lb, true, tc_trail_run, h->tc, st));
+    } else {
+      CK(lu_factor<z32>(T, lb, true, nullptr, nullptr, st));
+    }
+    CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
+    CK(launch_init_x(T, strideM, (int)N, (int)R, 2 * np, h->X64, st));
+    const int nmat = 2 * np;
+    const size_t per = N * R;
+    std::vector<unsigned long long> nh(2 * nmat);
+    std::vector<char> conv(nmat, 0);
+    for (int it = 0; it < h->max_iter; ++it) {
+      CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
+      CK(launch_residual(c, np, h->X64, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m,
+                         h->XD, h->V32, st));
+      CK(lu_fwdsolve_ws<z32>(T, lb, h->V32, per, (int)N, (int)R, h->work32, st));
+      CK(lu_backsolve<z32>(T, lb, h->V32, per, (int)N, (int)R, st));
+      CK(launch_update((int)per, nmat, h->V32, h->X64, h->norms, nullptr, st));
+      CK(cudaMemcpyAsync(nh.data(), h->norms, sizeof(unsigned long long) * 2 * nmat,
+                         cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      iters = it + 1;
+      bool all = true;
+      worst = 0.0;
+      for (int m = 0; m < nmat; ++m) {
+        double md, mx;
+        memcpy(&md, &nh[2 * m], 8);
+        memcpy(&mx, &nh[2 * m + 1], 8);
+        double rel = mx > 0 ? md / mx : md;
+        if (!(rel <= h->tol)) all = false;
+        conv[m] = rel <= h->tol;
+        if (!(rel <= worst)) worst = rel;
+      }
+      if (all) break;
+    }
+    for (int p = 0; p < np; ++p)
+      if (!conv[2 * p] || !conv[2 * p + 1]) fallback.push_back(p);
+    mixed_fail = (int)fallback.size();
+    X = h->X64; sp = 2 * per; sc = per;
+  }
+  cudaEventRecord(ev[3], st);
+  CK(launch_post(c, np, X, sp, sc, (int)N, h->opg_d, h->opg_m, h->gam_d, h->gam_m, h->gq, chi0q,
+                 h->c0w, chi_qw_d + (size_t)off * h->nd4, chi_qw_m + (size_t)off * h->nd4,
+                 do_eom ? h->mtot : nullptr, h->etad, h->etam, st));
+  for (int p : fallback)    // their EOM contribution comes from the FP64 re-solve below
+    CK(cudaMemsetAsync(h->mtot + (size_t)p * c.nd2 * c.iwf * c.nd2, 0,
+                       sizeof(z64) * c.nd2 * c.iwf * c.nd2, st));
+  cudaEventRecord(ev[4], st);
+  if (do_eom) CK(launch_eom_dynamic(c, iwb, h->qidx_d, np, h->mtot, h->sigma_nl, st));
+  cudaEventRecord(ev[5], st);
+  std::vector<int> info(2 * np);
+  CK(cudaMemcpyAsync(info.data(), h->info, sizeof(int) * 2 * np, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  stage_ms(h, &h->stats.ms_chi0, ev[0], ev[1]);
+  stage_ms(h, &h->stats.ms_bse, ev[1], ev[2]);
+  stage_ms(h, &h->stats.ms_lu, ev[2], ev[3]);
+  stage_ms(h, &h->stats.ms_post, ev[3], ev[4]);
+  stage_ms(h, &h->stats.ms_eom, ev[4], ev[5]);
+  for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+  for (int p = 0; p < np; ++p) {
+    int a = info[2 * p], b = info[2 * p + 1];
+    int s = a ? a : b;
+    if (s) h->stats.lu_info_nonzero++;
+    if (status) status[off + p] = s;
+  }
+  h->stats.points += np;
+  if (prec == ADGA_MIXED) {
+    h->stats.max_refine_iters = std::max(h->stats.max_refine_iters, iters);
+    if (!(worst <= h->stats.max_refine_resid)) h->stats.max_refine_resid = worst;
+  }
+  if (mixed_fail) {
+    // FP64 re-solve of the points whose refinement did not converge
+    std::vector<int> q(np);
+    for (int p = 0; p < np; ++p) q[p] = h->qidx_h[p];
+    const int mixed_cap = h->cap;
+    h->stats.mixed_fallbacks += mixed_fail;
+    int saved_points = h->stats.points;
+    for (int p : fallback) {
+      int r = ensure_work(h, ADGA_FP64, 1);
+      if (r) return r;
+      h->qidx_h[0] = q[p];
+      r = run_batch(h, iwb, 1, off + p, ADGA_FP64, nullptr, chi_qw_d, chi_qw_m, bub_nl, do_eom, do_chi);
+      if (r) return r;
+      if (status) status[off + p] = -1;
+    }
+    h->stats.points = saved_points;
+    int r = ensure_work(h, ADGA_MIXED, mixed_cap);
+    if (r) return r;
+  }
+  return 0;
+}
+
+static int ensure_outputs(adga_handle *h, int npts) {
+  if (h->out_cap >= npts) return 0;
+  auto &L = h->owned;
+  // outputs of earlier runs are replaced; the old buffers stay owned until destroy
+  if (!alloc_into(h, h->chi_qw_d, (size_t)npts * h->nd4, L) ||
+      !alloc_into(h, h->chi_qw_m, (size_t)npts * h->nd4, L) ||
+      !alloc_into(h, h->bubble_nl, (size_t)npts * h->nd4, L))
+    return fail(h, ADGA_ENOMEM, "per-point outputs");
+  h->out_cap = npts;
+  return 0;
+}
+
+extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision, int *status,
+                               adga_run_stats *stats) {
+  if (!h) return ADGA_EINVAL;
+  DevCtx &c = h->c;
+  const int total = c.nqp * h->nw;
+  if (qwstart < 1 || qwstop > total || qwstop < qwstart)
+    return fail(h, ADGA_EINVAL, "qw range outside 1..nqp*(2*iwbmax_small+1)");
+  if (precision != ADGA_FP64 && precision != ADGA_MIXED) return fail(h, ADGA_EINVAL, "precision");
+  const int npts = qwstop - qwstart + 1;
+  int r = ensure_outputs(h, npts);
+  if (r) return r;
+  memset(&h->stats, 0, sizeof(h->stats));
+  CK(cudaMemsetAsync(h->chi_qw_d, 0, sizeof(z64) * npts * h->nd4, h->st));
+  CK(cudaMemsetAsync(h->chi_qw_m, 0, sizeof(z64) * npts * h->nd4, h->st));
+  CK(cudaMemsetAsync(h->bubble_nl, 0, sizeof(z64) * npts * h->nd4, h->st));
+  r = ensure_work(h, precision, std::min(npts, c.nqp));
+  if (r) return r;
+  cudaEventRecord(h->e0, h->st);
+  const bool do_chi = h->d.do_chi != 0, do_eom = h->d.do_eom != 0;
+  int p = 0;
+  while (p < npts) {
+    const int qw = qwstart + p;               // 1-based compound index
+    const int iwb = -c.iwb + (qw - 1) / c.nqp;
+    const int iq0 = (qw - 1) % c.nqp;
+    const int seg = std::min(npts - p, c.nqp - iq0);
+    r = ensure_local(h, iwb);
+    if (r) return r;
+    if (iq0 == 0) {
+      if (do_chi)
+        CK(launch_chi_loc_update(c, h->gam_d, h->gam_m, h->c0w, h->bubtmp,
+                                 h->chi_loc_d + (size_t)(iwb + c.iwb) * h->nd4,
+                                 h->chi_loc_m + (size_t)(iwb + c.iwb) * h->nd4,
+                                 h->bubble_loc + (size_t)(iwb + c.iwb) * h->nd4, h->st));
+      if (do_eom) {
+        if (iwb == 0) CK(launch_eom_static(c, h->sigma_dmft, h->st));
+        CK(launch_eom_dmft(c, iwb, h->gam_d, h->sigma_dmft, h->st));
+      }
+    }
+    for (int b0 = 0; b0 < seg; b0 += h->cap) {
+      const int nb = std::min(h->cap, seg - b0);
+      for (int i = 0; i < nb; ++i) h->qidx_h[i] = iq0 + b0 + i;
+      r = run_batch(h, iwb, nb, p + b0, precision, status, h->chi_qw_d, h->chi_qw_m, h->bubble_nl,
+                    do_eom, do_chi);
+      if (r) return r;
+    }
+    p += seg;
+  }
+  cudaEventRecord(h->e1, h->st);
+  CK(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->e0, h->e1);
+  h->stats.ms_total = ms;
+  h->last_npts = npts;
+  if (stats) *stats = h->stats;
+  return 0;
+}
+
+extern "C" int adga_get_outputs(adga_handle *h, const adga_outputs *o) {
+  if (!h || !o) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  cudaStream_t st = h->st;
+  // Sigma(-nu-1) = Sigma(nu)^dagger (src/eom_module.f90:228)
+  CK(launch_mirror_sigma(c, h->sigma_nl, c.nkp_eom, st));
+  const size_t np = h->last_npts;
+#define DN(dst, src, n) \
+  if (dst) CK(cudaMemcpyAsync(dst, src, sizeof(z64) * (n), cudaMemcpyDeviceToHost, st))
+  if (np) {
+    DN(o->chi_qw_dens, h->chi_qw_d, np * h->nd4);
+    DN(o->chi_qw_magn, h->chi_qw_m, np * h->nd4);
+    DN(o->bubble_nl, h->bubble_nl, np * h->nd4);
+  }
+  DN(o->bubble_loc, h->bubble_loc, (size_t)h->nd4 * h->nw);
+  DN(o->chi_loc_dens, h->chi_loc_d, (size_t)h->nd4 * h->nw);
+  DN(o->chi_loc_magn, h->chi_loc_m, (size_t)h->nd4 * h->nw);
+  DN(o->sigma_nl, h->sigma_nl, (size_t)c.nd2 * 2 * c.iwf * c.nkp_eom);
+  DN(o->sigma_dmft, h->sigma_dmft, (size_t)c.nd2 * 2 * c.iwf);
+  DN(o->sigma_hf, h->sigma_hf, (size_t)c.nd2 * c.nkp_eom);
+#undef DN
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// per-routine entry points
+// ---------------------------------------------------------------------------
+extern "C" int adga_get_chi0_loc(adga_handle *h, int iwf, int iwb, adga_z *out) {
+  if (!h || !out) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  if (iwf < -c.iwf || iwf >= c.iwf || iwb < -c.iwb || iwb > c.iwb) return ADGA_EINVAL;
+  int r = ensure_diag(h, iwb);
+  if (r) return r;
+  std::vector<z64> d(c.nd2);
+  CK(cudaMemcpyAsync(d.data(), h->c0w + (size_t)(iwf + c.iwf) * c.nd2, sizeof(z64) * c.nd2,
+                     cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  memset(out, 0, sizeof(adga_z) * c.nd2 * c.nd2);
+  for (int i = 0; i < c.nd2; ++i) memcpy(&out[i + i * c.nd2], &d[i], sizeof(adga_z));
+  return 0;
+}
+
+extern "C" int adga_get_chi0_loc_inv(adga_handle *h, int iwf, int iwb, adga_z *out) {
+  if (!h || !out) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  if (iwf < -c.iwf || iwf >= c.iwf || iwb < -c.iwb || iwb > c.iwb) return ADGA_EINVAL;
+  int r = ensure_diag(h, iwb);
+  if (r) return r;
+  std::vector<z64> d(c.nd2);
+  CK(cudaMemcpyAsync(d.data(), h->c0inv + (size_t)(iwf + c.iwf) * c.nd2, sizeof(z64) * c.nd2,
+                     cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  memset(out, 0, sizeof(adga_z) * c.nd2 * c.nd2);
+  for (int i = 0; i < c.nd2; ++i) memcpy(&out[i + i * c.nd2], &d[i], sizeof(adga_z));
+  return 0;
+}
+
+extern "C" int adga_chi0_q(adga_handle *h, int iq, int iwb, adga_z *chi0q, adga_z *bubble_nl) {
+  if (!h) return ADGA_EINVAL;
+  DevCtx &c = h->c;
+  if (iq < 1 || iq > c.nqp || iwb < -c.iwb || iwb > c.iwb) return ADGA_EINVAL;
+  int r = ensure_diag(h, iwb);
+  if (r) return r;
+  const int prec = h->cap_prec < 0 ? ADGA_FP64 : h->cap_prec;
+  r = ensure_work(h, prec, 1);
+  if (r) return r;
+  h->qidx_h[0] = iq - 1;
+  CK(cudaMemcpyAsync(h->qidx_d, h->qidx_h, sizeof(int), cudaMemcpyHostToDevice, h->st));
+  CK(launch_chi0(c, iwb, h->qidx_d, 1, h->chi0_all, h->nnu_all, h->st));
+  z64 *bn = h->etad;   // scratch
+  CK(launch_chi0_finish(c, h->chi0_all, h->nnu_all, 1, h->bubtmp, h->bigbox ? h->chi0q_big : nullptr,
+                        bn, h->st));
+  const z64 *src = h->bigbox ? h->chi0q_big : h->chi0_all;
+  if (chi0q)
+    CK(cudaMemcpyAsync(chi0q, src, sizeof(z64) * h->nd4 * 2 * c.iwf, cudaMemcpyDeviceToHost, h->st));
+  if (bubble_nl)
+    CK(cudaMemcpyAsync(bubble_nl, bn, sizeof(z64) * h->nd4, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+extern "C" int adga_get_gamma_w(adga_handle *h, int iwb, adga_z *gd, adga_z *gm) {
+  if (!h) return ADGA_EINVAL;
+  if (iwb < -h->c.iwb || iwb > h->c.iwb) return ADGA_EINVAL;
+  int r = ensure_local(h, iwb);
+  if (r) return r;
+  const size_t n = (size_t)h->c.nd2 * h->c.N;
+  if (gd) CK(cudaMemcpyAsync(gd, h->gam_d, sizeof(z64) * n, cudaMemcpyDeviceToHost, h->st));
+  if (gm) CK(cudaMemcpyAsync(gm, h->gam_m, sizeof(z64) * n, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+extern "C" int adga_bse_point(adga_handle *h, int iq, int iwb, int precision, adga_z *etaqd,
+                              adga_z *etaqm, adga_z *gammaqd, int *lu_info) {
+  if (!h) return ADGA_EINVAL;
+  DevCtx &c = h->c;
+  if (iq < 1 || iq > c.nqp || iwb < -c.iwb || iwb > c.iwb) return ADGA_EINVAL;
+  if (precision != ADGA_FP64 && precision != ADGA_MIXED) return ADGA_EINVAL;
+  int r = ensure_local(h, iwb);
+  if (r) return r;
+  r = ensure_work(h, precision, 1);
+  if (r) return r;
+  z64 *scr = nullptr;
+  std::vector<void *> tmp;
+  if (!alloc_into(h, scr, (size_t)3 * h->nd4, tmp)) return fail(h, ADGA_ENOMEM, "scratch");
+  h->qidx_h[0] = iq - 1;
+  int st_info = 0;
+  memset(&h->stats, 0, sizeof(h->stats));
+  r = run_batch(h, iwb, 1, 0, precision, &st_info, scr, scr + h->nd4, scr + 2 * h->nd4, false, true);
+  if (!r) {
+    const size_t n = (size_t)c.nd2 * c.N;
+    if (etaqd) cudaMemcpyAsync(etaqd, h->etad, sizeof(z64) * n, cudaMemcpyDeviceToHost, h->st);
+    if (etaqm) cudaMemcpyAsync(etaqm, h->etam, sizeof(z64) * n, cudaMemcpyDeviceToHost, h->st);
+    if (gammaqd) cudaMemcpyAsync(gammaqd, h->gq, sizeof(z64) * n, cudaMemcpyDeviceToHost, h->st);
+    if (cudaStreamSynchronize(h->st) != cudaSuccess) r = fail(h, ADGA_ECUDA, "copy-out");
+  }
+  free_list(tmp);
+  if (lu_info) *lu_info = st_info;
+  return r;
+}
+
+extern "C" int adga_calc_chi_qw(adga_handle *h, adga_z *chi_qw, const adga_z *interm3,
+                                const adga_z *chi0_sum) {
+  if (!h || !chi_qw || !interm3 || !chi0_sum) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  std::vector<void *> tmp;
+  z64 *dchi, *dim3_, *dc0;
+  const size_t nI = (size_t)c.nd2 * c.N, nC = (size_t)h->nd4 * 2 * c.iwf;
+  if (!alloc_into(h, dchi, h->nd4, tmp) || !alloc_into(h, dim3_, nI, tmp) ||
+      !alloc_into(h, dc0, nC, tmp)) {
+    free_list(tmp);
+    return fail(h, ADGA_ENOMEM, "calc_chi_qw buffers");
+  }
+  cudaStream_t st = h->st;
+  cudaMemcpyAsync(dchi, chi_qw, sizeof(z64) * h->nd4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dim3_, interm3, sizeof(z64) * nI, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dc0, chi0_sum, sizeof(z64) * nC, cudaMemcpyHostToDevice, st);
+  cudaError_t e = launch_calc_chi_qw(c, dchi, dim3_, dc0, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(chi_qw, dchi, sizeof(z64) * h->nd4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  free_list(tmp);
+  if (e != cudaSuccess) return fail(h, ADGA_ECUDA, cudaGetErrorString(e));
+  return 0;
+}
+
+// m_tot from eta_d, eta_m, gamma^q_d for one point (same kernel as the batch post)
+extern "C" int adga_calc_eom_dynamic(adga_handle *h, const adga_z *etaqd, const adga_z *etaqm,
+                                     const adga_z *gammaqd, int iwb, int iq, adga_z *sigma_nl) {
+  if (!h || !etaqd || !etaqm || !gammaqd || !sigma_nl) return ADGA_EINVAL;
+  DevCtx &c = h->c;
+  if (iq < 1 || iq > c.nqp || iwb < -c.iwb || iwb > c.iwb) return ADGA_EINVAL;
+  const int prec = h->cap_prec < 0 ? ADGA_FP64 : h->cap_prec;
+  int r = ensure_work(h, prec, 1);
+  if (r) return r;
+  const size_t n = (size_t)c.nd2 * c.N, ns = (size_t)c.nd2 * 2 * c.iwf * c.nkp_eom;
+  std::vector<void *> tmp;
+  z64 *X, *scr, *chi0z, *opz, *sig;
+  if (!alloc_into(h, X, 2 * n, tmp) || !alloc_into(h, scr, 2 * h->nd4, tmp) ||
+      !alloc_into(h, chi0z, (size_t)h->nd4 * 2 * c.iwf, tmp) || !alloc_into(h, opz, n, tmp) ||
+      !alloc_into(h, sig, ns, tmp)) {
+    free_list(tmp);
+    return fail(h, ADGA_ENOMEM, "eom buffers");
+  }
+  cudaStream_t st = h->st;
+  // Feed eta through the post kernel as X = eta^T with zero (1+gamma): it
+  // rebuilds eta and forms m_tot with the reference's coefficients.
+  std::vector<adga_z> xt(2 * n);
+  for (int i1 = 0; i1 < c.nd2; ++i1)
+    for (int cc = 0; cc < c.N; ++cc) {
+      xt[cc + (size_t)i1 * c.N] = etaqd[i1 + (size_t)cc * c.nd2];
+      xt[n + cc + (size_t)i1 * c.N] = etaqm[i1 + (size_t)cc * c.nd2];
+    }
+  cudaError_t e = cudaMemcpyAsync(X, xt.data(), sizeof(z64) * 2 * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(opz, 0, sizeof(z64) * n, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(chi0z, 0, sizeof(z64) * h->nd4 * 2 * c.iwf, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->gq, gammaqd, sizeof(z64) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sig, sigma_nl, sizeof(z64) * ns, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = launch_post(c, 1, X, 2 * n, n, c.N, opz, opz, opz, opz, h->gq, chi0z, h->c0w, scr, scr + h->nd4,
+                    h->mtot, h->etad, h->etam, st);
+  h->qidx_h[0] = iq - 1;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->qidx_d, h->qidx_h, sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_eom_dynamic(c, iwb, h->qidx_d, 1, h->mtot, sig, st);
+  if (e == cudaSuccess) e = launch_mirror_sigma(c, sig, c.nkp_eom, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sigma_nl, sig, sizeof(z64) * ns, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  free_list(tmp);
+  if (e != cudaSuccess) return fail(h, ADGA_ECUDA, cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int adga_calc_eom_dmft(adga_handle *h, const adga_z *gammawd, int iwb, adga_z *sigma_dmft) {
+  if (!h || !gammawd || !sigma_dmft) return ADGA_EINVAL;
+  DevCtx &c = h->c;
+  if (iwb < -c.iwb || iwb > c.iwb) return ADGA_EINVAL;
+  const size_t n = (size_t)c.nd2 * c.N, ns = (size_t)c.nd2 * 2 * c.iwf;
+  std::vector<void *> tmp;
+  z64 *g, *s;
+  if (!alloc_into(h, g, n, tmp) || !alloc_into(h, s, ns, tmp)) {
+    free_list(tmp);
+    return fail(h, ADGA_ENOMEM, "eom_dmft buffers");
+  }
+  cudaStream_t st = h->st;
+  cudaError_t e = cudaMemcpyAsync(g, gammawd, sizeof(z64) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s, sigma_dmft, sizeof(z64) * ns, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_eom_dmft(c, iwb, g, s, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sigma_dmft, s, sizeof(z64) * ns, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  free_list(tmp);
+  if (e != cudaSuccess) return fail(h, ADGA_ECUDA, cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int adga_calc_eom_static(adga_handle *h, int iq, adga_z *sigma_dmft) {
+  if (!h || !sigma_dmft) return ADGA_EINVAL;
+  if (iq != 1) return 0;       // the local Hartree term only enters at q = 1
+  DevCtx &c = h->c;
+  const size_t ns = (size_t)c.nd2 * 2 * c.iwf;
+  std::vector<void *> tmp;
+  z64 *s;
+  if (!alloc_into(h, s, ns, tmp)) return fail(h, ADGA_ENOMEM, "eom_static buffers");
+  cudaStream_t st = h->st;
+  cudaError_t e = cudaMemcpyAsync(s, sigma_dmft, sizeof(z64) * ns, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_eom_static(c, s, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sigma_dmft, s, sizeof(z64) * ns, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  free_list(tmp);
+  if (e != cudaSuccess) return fail(h, ADGA_ECUDA, cudaGetErrorString(e));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// standalone helpers
+// ---------------------------------------------------------------------------
+extern "C" int adga_inverse_matrix_z(adga_z *M, int n, int *ierr, char *erstr) {
+  if (!M || n < 1 || n > 4096) return ADGA_EINVAL;
+  const int NB = 64, nsteps = (n + NB - 1) / NB;
+  const size_t strideM = (size_t)n * 2 * n;
+  z64 *T = nullptr, *Li = nullptr, *Ui = nullptr;
+  int *ip = nullptr, *inf = nullptr;
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return ADGA_ECUDA;
+  int rc = 0;
+  std::vector<adga_z> aug((size_t)n * 2 * n);
+  memcpy(aug.data(), M, sizeof(adga_z) * n * n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      adga_z v = {i == j ? 1.0 : 0.0, 0.0};
+      aug[(size_t)n * n + i + (size_t)j * n] = v;
+    }
+  if (cudaMalloc(&T, sizeof(z64) * strideM) != cudaSuccess ||
+      cudaMalloc(&Li, sizeof(z64) * nsteps * NB * NB) != cudaSuccess ||
+      cudaMalloc(&Ui, sizeof(z64) * nsteps * NB * NB) != cudaSuccess ||
+      cudaMalloc(&ip, sizeof(int) * n) != cudaSuccess || cudaMalloc(&inf, sizeof(int)) != cudaSuccess) {
+    rc = ADGA_ENOMEM;
+  } else {
+    LUBatch lb{n, 2 * n, 1, NB, strideM, ip, inf, Li, Ui};
+    int info = 0;
+    cudaError_t e = cudaMemcpyAsync(T, aug.data(), sizeof(z64) * strideM, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(inf, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = lu_factor<z64>(T, lb, false, nullptr, nullptr, st);
+    if (e == cudaSuccess) e = lu_backsolve<z64>(T, lb, T + (size_t)n * n, strideM, n, n, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&info, inf, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(M, T + (size_t)n * n, sizeof(z64) * n * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = ADGA_ECUDA;
+    if (ierr) *ierr = info;
+    if (erstr) {
+      if (info) snprintf(erstr, 200, "ERROR in ZGETRF");
+      else erstr[0] = 0;
+    }
+    if (rc == 0 && info) rc = info;
+  }
+  cudaFree(T); cudaFree(Li); cudaFree(Ui); cudaFree(ip); cudaFree(inf);
+  cudaStreamDestroy(st);
+  return rc;
+}
+
+extern "C" int adga_index_kq(int nkpx, int nkpy, int nkpz, const int *q_data, int nqp,
+                             const int *k_sel, int nk_sel, int *ind) {
+  if (!q_data || !ind || nqp < 1 || nkpx < 1 || nkpy < 1 || nkpz < 1) return ADGA_EINVAL;
+  const int nkp = nkpx * nkpy * nkpz;
+  const int nk = k_sel ? nk_sel : nkp;
+  int *dq = nullptr, *dk = nullptr, *di = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&dq, sizeof(int) * nqp) != cudaSuccess || cudaMalloc(&di, sizeof(int) * (size_t)nk * nqp) != cudaSuccess ||
+      (k_sel && cudaMalloc(&dk, sizeof(int) * nk) != cudaSuccess)) {
+    rc = ADGA_ENOMEM;
+  } else {
+    cudaError_t e = cudaMemcpy(dq, q_data, sizeof(int) * nqp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && k_sel) e = cudaMemcpy(dk, k_sel, sizeof(int) * nk, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_kq_index(nkpx, nkpy, nkpz, dk, nk, dq, nqp, 1, di, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(ind, di, sizeof(int) * (size_t)nk * nqp, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = ADGA_ECUDA;
+  }
+  cudaFree(dq); cudaFree(dk); cudaFree(di);
+  return rc;
+}
+
+extern "C" int adga_generate_q_vol(int nkpx, int nkpy, int nkpz, int nqpx, int nqpy, int nqpz,
+                                   int *q_data) {
+  if (!q_data || nqpx < 1 || nqpy < 1 || nqpz < 1) return ADGA_EINVAL;
+  if (nkpx % nqpx || nkpy % nqpy || nkpz % nqpz) return ADGA_EINVAL;   // config_init check
+  int i1 = 0;
+  for (int i = 0; i < nqpx; ++i)
+    for (int j = 0; j < nqpy; ++j)
+      for (int k = 0; k < nqpz; ++k)
+        q_data[i1++] = 1 + k * nkpz / nqpz + (j * nkpy / nqpy) * nkpz + (i * nkpx / nqpx) * nkpy * nkpz;
+  return 0;
+}
+
+extern "C" int adga_create_u(int nd, double U, double V, double J, double *Umat, adga_z *u,
+                             adga_z *ut) {
+  if (nd < 1 || nd > 16 || !u || !ut) return ADGA_EINVAL;
+  std::vector<double> Um((size_t)nd * nd * nd * nd, 0.0);
+  auto at = [&](int i, int j, int k, int l) -> double & {
+    return Um[i + (size_t)nd * (j + (size_t)nd * (k + (size_t)nd * l))];
+  };
+  // one atom, all bands correlated, Kanamori (interaction_mode 1)
+  for (int i = 0; i < nd; ++i)
+    for (int j = 0; j < nd; ++j)
+      for (int k = 0; k < nd; ++k)
+        for (int l = 0; l < nd; ++l) {
+          if (i == j && k == l) {
+            if (i == k) { at(i, j, k, l) = U; continue; }
+            at(i, j, k, l) = J;
+            continue;
+          }
+          if (i == k && j == l) { at(i, j, k, l) = V; continue; }
+          if (i == l && j == k) { at(i, j, k, l) = J; continue; }
+        }
+  const int nd2 = nd * nd;
+  for (int l = 0; l < nd; ++l)
+    for (int j = 0; j < nd; ++j) {
+      const int i2 = l * nd + j;
+      for (int i = 0; i < nd; ++i)
+        for (int k = 0; k < nd; ++k) {
+          const int i1 = i * nd + k;
+          u[i1 + (size_t)i2 * nd2] = {at(i, j, k, l), 0.0};
+          ut[i1 + (size_t)i2 * nd2] = {at(i, j, l, k), 0.0};
+        }
+    }
+  if (Umat) memcpy(Umat, Um.data(), sizeof(double) * Um.size());
+  return 0;
+}

@@ -1,0 +1,71 @@
+// Device-side view of one run: sizes plus pointers to the resident
+// one-particle data.  Passed by value to the kernels.
+#pragma once
+#include "common.cuh"
+
+struct DevCtx {
+  int nd, nd2, nkp, nqp, nkp_eom;
+  int nkpx, nkpy, nkpz;
+  int iwmax, iwf, iwb;           // one-particle box, two-particle half box, bosonic half box
+  int N, R;                      // BSE dimension maxdim = nd2*2*iwf; right-hand sides = nd2
+  int iwstart, iwstop;           // chi0 nu range
+  int nu_lo, nnu;                // G-table covers nu in [nu_lo, nu_lo + nnu)
+  double beta, mu;
+  const double *iw;              // iw_data, index n + iwmax
+  const z64 *hk;                 // hk(i,j,k) at k*nd2 + i + j*nd
+  const z64 *siw, *giw;          // (n + iwmax) + i*2*iwmax
+  const z64 *dc;                 // dc(s,i) at s + 2*i
+  const z64 *u, *ut;             // nd2 x nd2
+  const z64 *ndmft;              // nd
+  const int *kq;                 // k-q index, 0-based, (nkp, nqp)
+  const int *kqe;                // EOM k-q index, 0-based, (nkp_eom, nqp)
+  const z64 *gtab;               // G(k, nu): [(nu - nu_lo)*nkp + k][nd2], column-major nd x nd
+};
+
+// Kernel launchers (host functions), grouped by source file.
+// k_onepart.cu
+cudaError_t launch_gtable(const DevCtx &c, z64 *gtab, cudaStream_t st);
+cudaError_t launch_kq_index(int nkpx, int nkpy, int nkpz, const int *k_sel, int nk_sel,
+                            const int *q_data, int nqp, int one_based, int *ind, cudaStream_t st);
+cudaError_t launch_local_diag(const DevCtx &c, int iwb, z64 *c0inv, z64 *c0w, z64 *bubloc_tmp,
+                              cudaStream_t st);
+cudaError_t launch_local_F(const DevCtx &c, const z64 *chi_loc, const z64 *c0inv, z64 *Frow,
+                           cudaStream_t st);
+cudaError_t launch_local_gamma(const DevCtx &c, const z64 *Frow, z64 *gam, z64 *opg, cudaStream_t st);
+cudaError_t launch_chi_loc_update(const DevCtx &c, const z64 *gam_d, const z64 *gam_m,
+                                  const z64 *c0w, const z64 *bubloc_tmp, z64 *chi_loc_d,
+                                  z64 *chi_loc_m, z64 *bubble_loc, cudaStream_t st);
+cudaError_t launch_eom_static(const DevCtx &c, z64 *sigma_dmft, cudaStream_t st);
+cudaError_t launch_eom_dmft(const DevCtx &c, int iwb, const z64 *gam_d, z64 *sigma_dmft,
+                            cudaStream_t st);
+cudaError_t launch_mirror_sigma(const DevCtx &c, z64 *sigma, int nk, cudaStream_t st);
+cudaError_t launch_calc_chi_qw(const DevCtx &c, z64 *chi_qw, const z64 *interm3,
+                               const z64 *chi0_sum, cudaStream_t st);
+
+// k_chi0.cu: chi0q[p] (nd2, nd2, nnu_out) for a batch of points at one omega
+cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,
+                        int nnu_all, cudaStream_t st);
+cudaError_t launch_chi0_finish(const DevCtx &c, const z64 *chi0_all, int nnu_all, int npts,
+                               const z64 *bubloc_tmp, z64 *chi0q, z64 *bubble_nl, cudaStream_t st);
+
+// k_bse.cu
+template <typename T>
+cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const z64 *c0inv,
+                             const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
+                             const z64 *opg_m, T *Tmat, size_t strideM, z64 *gammaqd,
+                             cudaStream_t st);
+// X of point p, channel ch at X + p*sp + ch*sc: N x R column-major (ld ldX)
+cudaError_t launch_post(const DevCtx &c, int npts, const z64 *X, size_t sp, size_t sc, int ldX,
+                        const z64 *opg_d, const z64 *opg_m, const z64 *gam_d, const z64 *gam_m,
+                        const z64 *gammaqd, const z64 *chi0q, const z64 *c0w, z64 *chi_qw_d,
+                        z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam, cudaStream_t st);
+cudaError_t launch_eom_dynamic(const DevCtx &c, int iwb, const int *qidx, int npts,
+                               const z64 *mtot, z64 *sigma_nl, cudaStream_t st);
+
+// k_refine.cu
+cudaError_t launch_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X, cudaStream_t st);
+cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q,
+                            const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
+                            const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, cudaStream_t st);
+cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,
+                          const int *active, cudaStream_t st);

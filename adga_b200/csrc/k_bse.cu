@@ -1,0 +1,245 @@
+// Per-point BSE kernels around the LU:
+//   * build  -- A = 1 - blockdiag_nu(chi0^q chi0_loc^-1 - 1) F~ and gamma^q_d
+//               (src/main.F90:674-732), written transposed (T = A^T) with the
+//               right-hand sides (1 + gamma^w)^T appended as extra columns;
+//   * post   -- eta = (1+gamma^w)(A^-1 - 1) from the solve, the chi(q,w)
+//               frequency sums of calc_chi_qw (src/main.F90:665-667,766-769;
+//               src/susc_module.f90:34-56) and the EOM vertex m_tot
+//               (src/eom_module.f90:184-207);
+//   * eom    -- Sigma(k, nu) += m_tot G(k-q, nu-w) over a batch of points
+//               (src/eom_module.f90:209-230), one owner thread per (k, nu).
+#include "ctx.cuh"
+
+// ---------------------------------------------------------------------------
+// build: one block per (column tile of A^T rows c, channel, point).
+// T(c, r) = delta(c, r) - sum_i3 sw_nu(i1, i3) F~(i3 + nu*nd2, c), r = i1 + nu*nd2
+// sw_nu = chi0q(:,:,nu) diag(chi0_loc^-1(nu)) - 1
+// ---------------------------------------------------------------------------
+template <typename T, int ND2>
+__global__ void __launch_bounds__(128)
+k_bse_build(DevCtx c, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0inv,
+            const z64 *__restrict__ Frow_d, const z64 *__restrict__ Frow_m,
+            const z64 *__restrict__ opg_d, const z64 *__restrict__ opg_m, T *Tm, size_t strideM,
+            z64 *gammaqd) {
+  __shared__ z64 sw[ND2 * ND2];
+  const int N = c.N;
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ch = blockIdx.y, p = blockIdx.z;
+  const z64 *F = ch == 0 ? Frow_d : Frow_m;
+  const z64 *opg = ch == 0 ? opg_d : opg_m;
+  T *Tp = Tm + (size_t)(2 * p + ch) * strideM;
+  const z64 *c0 = chi0q + (size_t)p * ND2 * ND2 * 2 * c.iwf;
+  z64 gq[ND2];
+#pragma unroll
+  for (int a = 0; a < ND2; ++a) gq[a] = make_double2(0.0, 0.0);
+  for (int dum = 0; dum < 2 * c.iwf; ++dum) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < ND2 * ND2; e += blockDim.x) {
+      int i1 = e % ND2, i3 = e / ND2;
+      z64 v = cmul(c0[(size_t)dum * ND2 * ND2 + e], c0inv[dum * ND2 + i3]);
+      if (i1 == i3) v.x -= 1.0;
+      sw[e] = v;                       // sw(i1, i3) at i1 + i3*nd2
+    }
+    __syncthreads();
+    if (cc < N) {
+      z64 f[ND2];
+#pragma unroll
+      for (int i3 = 0; i3 < ND2; ++i3) f[i3] = F[(size_t)(i3 + dum * ND2) * N + cc];
+#pragma unroll
+      for (int i1 = 0; i1 < ND2; ++i1) {
+        z64 w = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int i3 = 0; i3 < ND2; ++i3) cfma(w, sw[i1 + i3 * ND2], f[i3]);
+        int r = i1 + dum * ND2;
+        z64 t = make_double2(-w.x, -w.y);
+        if (r == cc) t.x += 1.0;
+        Tp[cc + (size_t)r * N] = from64<T>(t);
+        if (ch == 0) gq[i1] = cadd(gq[i1], w);
+      }
+    }
+  }
+  if (cc < N) {
+#pragma unroll
+    for (int i1 = 0; i1 < ND2; ++i1) Tp[cc + (size_t)(N + i1) * N] = from64<T>(opg[i1 + (size_t)cc * ND2]);
+    if (ch == 0 && gammaqd) {
+      z64 *g = gammaqd + (size_t)p * ND2 * N;
+#pragma unroll
+      for (int i1 = 0; i1 < ND2; ++i1) g[i1 + (size_t)cc * ND2] = gq[i1];
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const z64 *c0inv,
+                             const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
+                             const z64 *opg_m, T *Tmat, size_t strideM, z64 *gammaqd,
+                             cudaStream_t st) {
+  if (npts <= 0) return cudaSuccess;
+  dim3 grid(cdiv_u(c.N, 128), 2, npts);
+#define BUILD(NDD)                                                                            \
+  k_bse_build<T, NDD><<<grid, 128, 0, st>>>(c, chi0q, c0inv, Frow_d, Frow_m, opg_d, opg_m,     \
+                                            Tmat, strideM, gammaqd)
+  switch (c.nd2) {
+    case 1: BUILD(1); break;
+    case 4: BUILD(4); break;
+    case 9: BUILD(9); break;
+    case 16: BUILD(16); break;
+    case 25: BUILD(25); break;
+    default: return cudaErrorInvalidValue;
+  }
+#undef BUILD
+  return ADGA_LAUNCH_CHECK();
+}
+template cudaError_t launch_bse_build<z64>(const DevCtx &, int, const z64 *, const z64 *,
+                                           const z64 *, const z64 *, const z64 *, const z64 *,
+                                           z64 *, size_t, z64 *, cudaStream_t);
+template cudaError_t launch_bse_build<z32>(const DevCtx &, int, const z64 *, const z64 *,
+                                           const z64 *, const z64 *, const z64 *, const z64 *,
+                                           z32 *, size_t, z64 *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// post: one block per point.
+//   X_ch(c, i1) (column-major, ld ldX) = ((1+gamma^w) A^-1)^T  -> eta = X^T - (1+gamma^w)
+//   chi_ch = beta^-2 sum gamma (chi0q - chi0w) + beta^-2 sum eta chi0q
+//   m_tot(:, nu >= 0 half) = -(u - u~/2) eta_d/(beta nqp) + 1.5 u~ eta_m/(beta nqp)
+//                            + u gamma^q_d/(beta nqp)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_post(DevCtx c, const z64 *__restrict__ X, size_t sp, size_t sc, int ldX, const z64 *__restrict__ opg_d,
+       const z64 *__restrict__ opg_m, const z64 *__restrict__ gam_d, const z64 *__restrict__ gam_m,
+       const z64 *__restrict__ gammaqd, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0w,
+       z64 *chi_qw_d, z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam) {
+  const int p = blockIdx.x;
+  const int N = c.N, nd2 = c.nd2, iwf = c.iwf;
+  const size_t nd2N = (size_t)nd2 * N;
+  z64 *ed = etad + p * nd2N, *em = etam + p * nd2N;
+  const z64 *Xd = X + (size_t)p * sp, *Xm = Xd + sc;
+  // 1. eta
+  for (size_t e = threadIdx.x; e < nd2N; e += blockDim.x) {
+    int i1 = (int)(e % nd2), cc = (int)(e / nd2);
+    ed[e] = csub(Xd[cc + (size_t)i1 * ldX], opg_d[e]);
+    em[e] = csub(Xm[cc + (size_t)i1 * ldX], opg_m[e]);
+  }
+  __syncthreads();
+  const z64 *c0 = chi0q + (size_t)p * nd2 * nd2 * 2 * iwf;
+  const double b2 = c.beta * c.beta;
+  // 2. chi sums, one thread per (i1, i2, channel)
+  for (int t = threadIdx.x; t < 2 * nd2 * nd2; t += blockDim.x) {
+    int ch = t / (nd2 * nd2), e = t % (nd2 * nd2);
+    int i1 = e % nd2, i2 = e / nd2;
+    const z64 *g = ch ? gam_m : gam_d;
+    const z64 *et = ch ? em : ed;
+    z64 s1 = make_double2(0.0, 0.0), s2 = make_double2(0.0, 0.0);
+    for (int dum = 0; dum < 2 * iwf; ++dum) {
+      const z64 *cq = c0 + (size_t)dum * nd2 * nd2 + (size_t)i2 * nd2;
+      for (int i3 = 0; i3 < nd2; ++i3) {
+        size_t col = (size_t)(i3 + dum * nd2) * nd2;
+        z64 q = cq[i3];
+        z64 nl = q;
+        if (i3 == i2) nl = csub(q, c0w[dum * nd2 + i2]);
+        cfma(s1, g[i1 + col], nl);
+        cfma(s2, et[i1 + col], q);
+      }
+    }
+    z64 *out = (ch ? chi_qw_m : chi_qw_d) + (size_t)p * nd2 * nd2 + e;
+    z64 v = make_double2(s1.x / b2, s1.y / b2);
+    v = cadd(v, make_double2(s2.x / b2, s2.y / b2));
+    *out = v;
+  }
+  // 3. m_tot for the nu >= 0 half of the columns
+  if (mtot) {
+    const double inv = 1.0 / c.beta / (double)c.nqp;
+    const z64 *gq = gammaqd + (size_t)p * nd2N;
+    z64 *m = mtot + (size_t)p * nd2 * iwf * nd2;
+    for (int t = threadIdx.x; t < nd2 * iwf * nd2; t += blockDim.x) {
+      int i1 = t % nd2, cl = t / nd2;          // local column
+      size_t col = (size_t)(cl + iwf * nd2) * nd2;
+      z64 a1 = make_double2(0.0, 0.0), a2 = a1, a3 = a1;
+      for (int i3 = 0; i3 < nd2; ++i3) {
+        z64 uu = c.u[i1 + i3 * nd2], tt = c.ut[i1 + i3 * nd2];
+        z64 uw = make_double2(uu.x - 0.5 * tt.x, uu.y - 0.5 * tt.y);
+        cfma(a1, uw, ed[i3 + col]);
+        cfma(a2, tt, em[i3 + col]);
+        cfma(a3, uu, gq[i3 + col]);
+      }
+      z64 v = cscale(a1, -inv);
+      v = cadd(cscale(a2, 1.5 * inv), v);
+      v = cadd(cscale(a3, inv), v);
+      m[t] = v;
+    }
+  }
+}
+
+cudaError_t launch_post(const DevCtx &c, int npts, const z64 *X, size_t sp, size_t sc, int ldX,
+                        const z64 *opg_d, const z64 *opg_m, const z64 *gam_d, const z64 *gam_m,
+                        const z64 *gammaqd, const z64 *chi0q, const z64 *c0w, z64 *chi_qw_d,
+                        z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam, cudaStream_t st) {
+  if (npts <= 0) return cudaSuccess;
+  k_post<<<npts, 256, 0, st>>>(c, X, sp, sc, ldX, opg_d, opg_m, gam_d, gam_m, gammaqd, chi0q, c0w,
+                               chi_qw_d, chi_qw_m, mtot, etad, etam);
+  return ADGA_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// eom: Sigma(i,l,nu,k) += sum_p sum_{k',j} m_tot_p({j,i},{k',l,nu}) G_jk'(k - q_p, nu - w)
+// One block per (k tile, nu >= 0); the m_tot slice of each point is staged in
+// shared memory, G is gathered from the resident table.  Summation order per
+// element follows the reference: points in order, k' outer, j inner.
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(128)
+k_eom_dyn(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, const z64 *__restrict__ mtot,
+          z64 *sigma) {
+  constexpr int ND2 = ND * ND;
+  __shared__ z64 M[ND2 * ND2];
+  const int nu = blockIdx.y;                  // 0..iwf-1
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iwf = c.iwf;
+  const bool act = k < c.nkp_eom;
+  z64 acc[ND2];
+  z64 *so = sigma + ((size_t)k * 2 * iwf + nu + iwf) * ND2;
+#pragma unroll
+  for (int a = 0; a < ND2; ++a) acc[a] = act ? so[a] : make_double2(0.0, 0.0);
+  const z64 *gt = c.gtab + (size_t)(nu - iwb - c.nu_lo) * c.nkp * ND2;
+  for (int p = 0; p < npts; ++p) {
+    __syncthreads();
+    const z64 *mp = mtot + (size_t)p * ND2 * iwf * ND2 + (size_t)nu * ND2 * ND2;
+    for (int e = threadIdx.x; e < ND2 * ND2; e += blockDim.x) M[e] = mp[e];
+    __syncthreads();
+    if (act) {
+      int kk = c.kqe[k + (size_t)qidx[p] * c.nkp_eom];
+      const z64 *g = gt + (size_t)kk * ND2;
+      z64 G[ND2];
+#pragma unroll
+      for (int a = 0; a < ND2; ++a) G[a] = __ldg(g + a);
+#pragma unroll
+      for (int l = 0; l < ND; ++l)
+#pragma unroll
+        for (int k2 = 0; k2 < ND; ++k2)
+#pragma unroll
+          for (int i = 0; i < ND; ++i)
+#pragma unroll
+            for (int j = 0; j < ND; ++j)
+              cfma(acc[i + l * ND], M[(i * ND + j) + (l * ND + k2) * ND2], G[j + k2 * ND]);
+    }
+  }
+  if (act) {
+#pragma unroll
+    for (int a = 0; a < ND2; ++a) so[a] = acc[a];
+  }
+}
+
+cudaError_t launch_eom_dynamic(const DevCtx &c, int iwb, const int *qidx, int npts,
+                               const z64 *mtot, z64 *sigma_nl, cudaStream_t st) {
+  if (npts <= 0) return cudaSuccess;
+  dim3 grid(cdiv_u(c.nkp_eom, 128), c.iwf);
+  switch (c.nd) {
+    case 1: k_eom_dyn<1><<<grid, 128, 0, st>>>(c, iwb, qidx, npts, mtot, sigma_nl); break;
+    case 2: k_eom_dyn<2><<<grid, 128, 0, st>>>(c, iwb, qidx, npts, mtot, sigma_nl); break;
+    case 3: k_eom_dyn<3><<<grid, 128, 0, st>>>(c, iwb, qidx, npts, mtot, sigma_nl); break;
+    case 4: k_eom_dyn<4><<<grid, 128, 0, st>>>(c, iwb, qidx, npts, mtot, sigma_nl); break;
+    case 5: k_eom_dyn<5><<<grid, 128, 0, st>>>(c, iwb, qidx, npts, mtot, sigma_nl); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return ADGA_LAUNCH_CHECK();
+}

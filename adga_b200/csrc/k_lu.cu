@@ -1,0 +1,568 @@
+// Batched blocked right-looking LU with partial pivoting (complex FP64 or
+// FP32) and blocked triangular solves; see lu.cuh for the layout.
+//
+// Per step J (panel width NB):
+//   k_panel      one CTA per matrix factors rows J..N of the NB panel columns
+//                in 8-column sub-panels held in registers (pivot search,
+//                row swap and rank-1 updates never leave the SM), with
+//                right-looking rank-8 updates of the rest of the panel;
+//   k_triinv     inverts the unit-lower and upper NB x NB diagonal blocks;
+//   k_swap_trsm  applies the panel's row interchanges to the other columns
+//                and forms U12 = L11^-1 A12 as a small GEMM;
+//   trailing     A22 -= L21 U12 (CUDA-core GEMM below, or the tensor-core
+//                BF16x3 kernel of the mixed path).
+// Pivot choice follows izamax: the largest |re|+|im|, the lowest row on ties.
+#include "lu.cuh"
+#include <climits>
+
+#define SWD 8          // sub-panel width
+#define MAXNB 128      // largest outer panel width
+
+// ---------------------------------------------------------------------------
+template <int RPT> struct PanelThreads { static constexpr int v = RPT == 1 ? 1024 : RPT == 2 ? 640 : 512; };
+
+template <typename T> struct PanelShared {
+  typename cx<T>::real red_v[32];
+  int red_i[32];
+  int s_p;
+  int s_info;
+  int s_piv[SWD];
+  T bufP[SWD], bufC[SWD];
+  T Lss[SWD * SWD];
+  T Us[SWD * MAXNB];
+};
+
+// One column CC of the register-resident sub-panel: pivot search, row swap,
+// scaling and rank-1 update.  CC is a compile-time constant so that every
+// index into the register array a[][] is static.
+template <typename T, int RPT, int CC>
+__device__ __forceinline__ void panel_column(T (&a)[RPT][SWD], PanelShared<T> &S, int J, int N,
+                                             int c0, int sw, int t, int nt) {
+  typedef typename cx<T>::real R;
+  if (CC >= sw) return;
+  const int lane = t & 31, warp = t >> 5, nw = nt >> 5;
+  const int col = c0 + CC;
+  R best = R(-1);
+  int bidx = INT_MAX;
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    const int r = J + t + q * nt;
+    if (r >= col && r < N) {
+      R v = cabs1(a[q][CC]);
+      if (v > best) { best = v; bidx = r; }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    R ov = __shfl_xor_sync(0xffffffffu, best, o);
+    int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+    if (ov > best || (ov == best && oi < bidx)) { best = ov; bidx = oi; }
+  }
+  if (lane == 0) { S.red_v[warp] = best; S.red_i[warp] = bidx; }
+  __syncthreads();
+  if (warp == 0) {
+    best = lane < nw ? S.red_v[lane] : R(-1);
+    bidx = lane < nw ? S.red_i[lane] : INT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      R ov = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+      if (ov > best || (ov == best && oi < bidx)) { best = ov; bidx = oi; }
+    }
+    if (lane == 0) S.s_p = (bidx == INT_MAX || bidx < col || bidx >= N) ? col : bidx;
+  }
+  __syncthreads();
+  const int p = S.s_p;
+  const int oc = col - J, op = p - J;
+  const bool own_c = (oc % nt) == t, own_p = (op % nt) == t;
+  const int qc = oc / nt, qp = op / nt;
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    if (own_p && q == qp)
+#pragma unroll
+      for (int c2 = 0; c2 < SWD; ++c2) S.bufP[c2] = a[q][c2];
+    if (own_c && q == qc)
+#pragma unroll
+      for (int c2 = 0; c2 < SWD; ++c2) S.bufC[c2] = a[q][c2];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    if (own_c && q == qc)
+#pragma unroll
+      for (int c2 = 0; c2 < SWD; ++c2) a[q][c2] = S.bufP[c2];
+    if (own_p && p != col && q == qp)
+#pragma unroll
+      for (int c2 = 0; c2 < SWD; ++c2) a[q][c2] = S.bufC[c2];
+  }
+  const T piv = S.bufP[CC];
+  const bool zero = (piv.x == R(0) && piv.y == R(0));
+  if (zero && t == 0 && S.s_info == 0) S.s_info = col + 1;
+  const T rcp = zero ? czero<T>() : crcp(piv);
+  T prow[SWD];
+#pragma unroll
+  for (int c2 = CC + 1; c2 < SWD; ++c2) prow[c2] = S.bufP[c2];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    const int r = J + t + q * nt;
+    if (r > col && r < N) {
+      const T l = zero ? a[q][CC] : cmul(a[q][CC], rcp);
+      a[q][CC] = l;
+#pragma unroll
+      for (int c2 = CC + 1; c2 < SWD; ++c2)
+        if (c2 < sw) cfms(a[q][c2], l, prow[c2]);
+    }
+  }
+  if (t == 0) S.s_piv[CC] = p;
+}
+
+template <typename T, int RPT>
+__global__ void __launch_bounds__(PanelThreads<RPT>::v)
+k_panel(T *M, size_t strideM, int N, int J, int jb, int *ipiv_all, int *info_all) {
+  const int b = blockIdx.x;
+  T *A = M + (size_t)b * strideM;
+  int *ipiv = ipiv_all + (size_t)b * N;
+  const int nt = blockDim.x, t = threadIdx.x;
+  __shared__ PanelShared<T> S;
+  if (t == 0) S.s_info = info_all[b];
+  T a[RPT][SWD];
+
+  for (int s = 0; s < jb; s += SWD) {
+    const int sw = min(SWD, jb - s), c0 = J + s;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int r = J + t + q * nt;
+#pragma unroll
+      for (int cc = 0; cc < SWD; ++cc)
+        a[q][cc] = (r >= c0 && r < N && cc < sw) ? A[r + (size_t)(c0 + cc) * N] : czero<T>();
+    }
+    panel_column<T, RPT, 0>(a, S, J, N, c0, sw, t, nt);
+    panel_column<T, RPT, 1>(a, S, J, N, c0, sw, t, nt);
+    panel_column<T, RPT, 2>(a, S, J, N, c0, sw, t, nt);
+    panel_column<T, RPT, 3>(a, S, J, N, c0, sw, t, nt);
+    panel_column<T, RPT, 4>(a, S, J, N, c0, sw, t, nt);
+    panel_column<T, RPT, 5>(a, S, J, N, c0, sw, t, nt);
+    panel_column<T, RPT, 6>(a, S, J, N, c0, sw, t, nt);
+    panel_column<T, RPT, 7>(a, S, J, N, c0, sw, t, nt);
+    // ---- write the sub-panel back; keep its L block for the TRSM below
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int r = J + t + q * nt;
+      if (r >= c0 && r < N) {
+#pragma unroll
+        for (int cc = 0; cc < SWD; ++cc)
+          if (cc < sw) A[r + (size_t)(c0 + cc) * N] = a[q][cc];
+        const int i = r - c0;
+        if (i < sw)
+#pragma unroll
+          for (int cc = 0; cc < SWD; ++cc) S.Lss[i + cc * SWD] = a[q][cc];
+      }
+    }
+    __syncthreads();
+    if (t < sw) ipiv[c0 + t] = S.s_piv[t];
+    // ---- apply the sub-panel's interchanges to the other panel columns
+    const int nother = jb - sw;
+    for (int u = t; u < nother; u += nt) {
+      const int col = (u < s) ? J + u : c0 + sw + (u - s);
+      T *Ac = A + (size_t)col * N;
+      for (int i = 0; i < sw; ++i) {
+        const int pr = S.s_piv[i], r = c0 + i;
+        if (pr != r) { T x = Ac[r]; Ac[r] = Ac[pr]; Ac[pr] = x; }
+      }
+    }
+    __syncthreads();
+    // ---- U rows of the right panel columns: unit-lower solve with Lss
+    const int nright = jb - s - sw;
+    for (int u = t; u < nright; u += nt) {
+      const int col = c0 + sw + u;
+      T *Ac = A + (size_t)col * N;
+      T x[SWD];
+#pragma unroll
+      for (int i = 0; i < SWD; ++i) x[i] = (i < sw) ? Ac[c0 + i] : czero<T>();
+#pragma unroll
+      for (int i = 1; i < SWD; ++i)
+#pragma unroll
+        for (int k = 0; k < i; ++k) cfms(x[i], S.Lss[i + k * SWD], x[k]);
+#pragma unroll
+      for (int i = 0; i < SWD; ++i)
+        if (i < sw) { Ac[c0 + i] = x[i]; S.Us[i * MAXNB + u] = x[i]; }
+    }
+    __syncthreads();
+    // ---- rank-sw update of the rows below, right panel columns
+    if (nright > 0) {
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const int r = J + t + q * nt;
+        if (r >= c0 + sw && r < N) {
+          for (int u = 0; u < nright; ++u) {
+            T *ap = A + r + (size_t)(c0 + sw + u) * N;
+            T v = *ap;
+#pragma unroll
+            for (int i = 0; i < SWD; ++i)
+              if (i < sw) cfms(v, a[q][i], S.Us[i * MAXNB + u]);
+            *ap = v;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (t == 0) info_all[b] = S.s_info;
+}
+
+// ---------------------------------------------------------------------------
+// Inverses of the diagonal block: strictly-lower part -> unit-lower inverse
+// (columns right to left), upper part -> upper inverse (columns left to right),
+// both in place in shared memory as LAPACK's xTRTI2 does.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_triinv(const T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Linv, T *Uinv) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *D = reinterpret_cast<T *>(smraw);
+  T *tmp = D + NB * NB;
+  __shared__ T s_d;
+  const int b = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
+  const T *A = M + (size_t)b * strideM;
+  const int n = jb;
+  for (int e = t; e < n * n; e += nt) {
+    int i = e % n, j = e / n;
+    D[i + j * NB] = A[(size_t)(J + i) + (size_t)(J + j) * N];
+  }
+  __syncthreads();
+  for (int j = n - 2; j >= 0; --j) {
+    for (int i = j + 1 + t; i < n; i += nt) tmp[i] = D[i + j * NB];
+    __syncthreads();
+    for (int i = j + 1 + t; i < n; i += nt) {
+      T s = tmp[i];
+      for (int k = j + 1; k < i; ++k) cfma(s, D[i + k * NB], tmp[k]);
+      D[i + j * NB] = cneg(s);
+    }
+    __syncthreads();
+  }
+  for (int j = 0; j < n; ++j) {
+    if (t == 0) { T d = crcp(D[j + j * NB]); D[j + j * NB] = d; s_d = d; }
+    for (int i = t; i < j; i += nt) tmp[i] = D[i + j * NB];
+    __syncthreads();
+    const T d = s_d;
+    for (int i = t; i < j; i += nt) {
+      T s = czero<T>();
+      for (int k = i; k < j; ++k) cfma(s, D[i + k * NB], tmp[k]);
+      D[i + j * NB] = cneg(cmul(d, s));
+    }
+    __syncthreads();
+  }
+  const size_t off = ((size_t)b * nsteps + J / NB) * NB * NB;
+  for (int e = t; e < NB * NB; e += nt) {
+    int i = e % NB, k = e / NB;
+    T lv = czero<T>(), uv = czero<T>();
+    if (i < n && k < n) {
+      if (i > k) lv = D[i + k * NB];
+      else if (i == k) lv = cx<T>::make(1, 0);
+      if (i <= k) uv = D[i + k * NB];
+    }
+    Linv[off + e] = lv;
+    Uinv[off + e] = uv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row interchanges of one step on the columns outside the panel, then
+// U12 = L11^-1 A12 on the right columns (a jb x jb x TW product).
+// ---------------------------------------------------------------------------
+#define TW 32
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps,
+            const int *ipiv_all, const T *Linv, int nleft_tiles) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *Ls = reinterpret_cast<T *>(smraw);
+  T *Xs = Ls + NB * NB;
+  __shared__ int s_ip[MAXNB];
+  const int tile = blockIdx.x, b = blockIdx.y, t = threadIdx.x, nt = blockDim.x;
+  T *A = M + (size_t)b * strideM;
+  const bool right = tile >= nleft_tiles;
+  int cs, ce;
+  if (!right) { cs = tile * TW; ce = min(J, cs + TW); }
+  else { cs = J + jb + (tile - nleft_tiles) * TW; ce = min(ncols, cs + TW); }
+  const int nc = ce - cs;
+  for (int i = t; i < jb; i += nt) s_ip[i] = ipiv_all[(size_t)b * N + J + i];
+  if (right) {
+    const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
+    for (int e = t; e < NB * jb; e += nt) Ls[e] = L[e];
+  }
+  __syncthreads();
+  if (t < nc) {
+    T *Ac = A + (size_t)(cs + t) * N;
+    for (int i = 0; i < jb; ++i) {
+      const int pr = s_ip[i], r = J + i;
+      if (pr != r) { T x = Ac[r]; Ac[r] = Ac[pr]; Ac[pr] = x; }
+    }
+  }
+  if (!right) return;
+  __syncthreads();
+  for (int e = t; e < jb * nc; e += nt) {
+    int k = e % jb, c = e / jb;
+    Xs[k + c * NB] = A[(size_t)(J + k) + (size_t)(cs + c) * N];
+  }
+  __syncthreads();
+  for (int e = t; e < jb * nc; e += nt) {
+    int i = e % jb, c = e / jb;
+    T s = czero<T>();
+    for (int k = 0; k <= i; ++k) cfma(s, Ls[i + k * NB], Xs[k + c * NB]);
+    A[(size_t)(J + i) + (size_t)(cs + c) * N] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Trailing update on CUDA cores: C[J+jb.., J+jb..] -= A[J+jb.., J:J+jb] * A[J:J+jb, J+jb..]
+// 64 x 64 tiles, BK = 16, 256 threads with 4 x 4 complex outputs each.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_gemm_update(T *M, size_t strideM, int N, int ncols, int J, int jb) {
+  __shared__ T As[16][64];
+  __shared__ T Bs[16][64];
+  const int b = blockIdx.z, t = threadIdx.x;
+  const int tx = t & 15, ty = t >> 4;
+  T *A = M + (size_t)b * strideM;
+  const int r0 = J + jb + blockIdx.y * 64, c0 = J + jb + blockIdx.x * 64;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = czero<T>();
+  for (int k0 = 0; k0 < jb; k0 += 16) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int e = t + 256 * i;
+      int rr = e & 63, kk = e >> 6;
+      int r = r0 + rr, k = k0 + kk;
+      As[kk][rr] = (r < N && k < jb) ? A[r + (size_t)(J + k) * N] : czero<T>();
+      int kk2 = e & 15, cc = e >> 4;
+      int c = c0 + cc, k2 = k0 + kk2;
+      Bs[kk2][cc] = (c < ncols && k2 < jb) ? A[(size_t)(J + k2) + (size_t)c * N] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cfma(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = c0 + ty + 16 * j;
+    if (c >= ncols) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = r0 + tx + 16 * i;
+      if (r < N) {
+        T *p = A + r + (size_t)c * N;
+        *p = csub(*p, acc[i][j]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Blocked triangular solves with the inverted diagonal blocks.
+// backsolve: U Y = C (bottom block first); fwdsolve: L z = P r (top first).
+// ---------------------------------------------------------------------------
+#define RT 16
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256)
+k_trisolve(const T *M, size_t strideM, int N, int NB, int nsteps, const T *Dinv, T *C,
+           size_t strideC, int ldc, int R, const int *ipiv_all, T *work) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nph = 256 / NB;
+  T *red = reinterpret_cast<T *>(smraw);          // [nph][NB][RT]
+  T *W = red + (size_t)nph * NB * RT;             // [NB][RT]
+  int *perm = reinterpret_cast<int *>(W + (size_t)NB * RT);
+  const int b = blockIdx.y, r0 = blockIdx.x * RT, t = threadIdx.x;
+  const T *A = M + (size_t)b * strideM;
+  T *Cb = C + (size_t)b * strideC;
+  const int nr = min(RT, R - r0);
+  if (!UPPER) {
+    // apply the row interchanges P to the right-hand sides (through work)
+    if (t == 0) {
+      for (int i = 0; i < N; ++i) perm[i] = i;
+      const int *ip = ipiv_all + (size_t)b * N;
+      for (int i = 0; i < N; ++i) {
+        int p = ip[i];
+        if (p != i) { int x = perm[i]; perm[i] = perm[p]; perm[p] = x; }
+      }
+    }
+    __syncthreads();
+    T *Wk = work + (size_t)b * N * RT * gridDim.x + (size_t)blockIdx.x * N * RT;
+    for (int e = t; e < N * nr; e += 256) {
+      int i = e % N, r = e / N;
+      Wk[e] = Cb[perm[i] + (size_t)(r0 + r) * ldc];
+    }
+    __syncthreads();
+    for (int e = t; e < N * nr; e += 256) {
+      int i = e % N, r = e / N;
+      Cb[i + (size_t)(r0 + r) * ldc] = Wk[e];
+    }
+    __syncthreads();
+  }
+  const int row = t % NB, kph = t / NB;
+  for (int s = 0; s < nsteps; ++s) {
+    const int blk = UPPER ? nsteps - 1 - s : s;
+    const int J = blk * NB, jb = min(NB, N - J);
+    T acc[RT];
+#pragma unroll
+    for (int r = 0; r < RT; ++r) acc[r] = czero<T>();
+    if (row < jb) {
+      const int kb = UPPER ? J + jb : 0, ke = UPPER ? N : J;
+      for (int k = kb + kph; k < ke; k += nph) {
+        const T u = A[(size_t)(J + row) + (size_t)k * N];
+#pragma unroll
+        for (int r = 0; r < RT; ++r)
+          if (r < nr) cfma(acc[r], u, Cb[k + (size_t)(r0 + r) * ldc]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < RT; ++r) red[((size_t)kph * NB + row) * RT + r] = acc[r];
+    __syncthreads();
+    for (int e = t; e < jb * nr; e += 256) {
+      int i = e % jb, r = e / jb;
+      T v = Cb[(size_t)(J + i) + (size_t)(r0 + r) * ldc];
+      for (int ph = 0; ph < nph; ++ph) v = csub(v, red[((size_t)ph * NB + i) * RT + r]);
+      W[i * RT + r] = v;
+    }
+    __syncthreads();
+    const T *Di = Dinv + ((size_t)b * nsteps + blk) * NB * NB;
+    for (int e = t; e < jb * nr; e += 256) {
+      int i = e % jb, r = e / jb;
+      T v = czero<T>();
+      const int kb = UPPER ? i : 0, ke = UPPER ? jb : i + 1;
+      for (int k = kb; k < ke; ++k) cfma(v, Di[i + k * NB], W[k * RT + r]);
+      Cb[(size_t)(J + i) + (size_t)(r0 + r) * ldc] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+template <typename T>
+static cudaError_t launch_panel(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
+  const int rows = lb.N - J;
+  auto nthreads = [&](int rpt) { int n = ((rows + rpt - 1) / rpt + 31) / 32 * 32; return n < 32 ? 32 : n; };
+  if (rows <= 1024) {
+    k_panel<T, 1><<<lb.batch, nthreads(1), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+  } else if (rows <= 1280) {
+    k_panel<T, 2><<<lb.batch, nthreads(2), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+  } else if (rows <= 2048) {
+    k_panel<T, 4><<<lb.batch, nthreads(4), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+  } else if (rows <= 4096) {
+    k_panel<T, 8><<<lb.batch, nthreads(8), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+  } else {
+    return cudaErrorInvalidValue;   // N > 4096 is not supported
+  }
+  return ADGA_LAUNCH_CHECK();
+}
+
+template <typename T>
+cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
+  const int m = lb.N - J - jb, n = lb.ncols - J - jb;
+  if (m <= 0 || n <= 0) return cudaSuccess;
+  dim3 grid(cdiv_u(n, 64), cdiv_u(m, 64), lb.batch);
+  k_gemm_update<T><<<grid, 256, 0, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb);
+  return ADGA_LAUNCH_CHECK();
+}
+
+template <typename T>
+cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
+                      cudaStream_t st) {
+  if (lb.NB > MAXNB || lb.NB % SWD) return cudaErrorInvalidValue;
+  const int nsteps = lb.nsteps();
+  cudaError_t e;
+  const size_t sm_tri = sizeof(T) * ((size_t)lb.NB * lb.NB + lb.NB);
+  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * lb.NB + (size_t)lb.NB * TW);
+  static bool attr_done[2] = {false, false};
+  const int ti = sizeof(T) == sizeof(z64) ? 0 : 1;
+  if (!attr_done[ti]) {
+    cudaFuncSetAttribute(k_triinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_swap_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done[ti] = true;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
+    if ((e = launch_panel<T>(M, lb, J, jb, st)) != cudaSuccess) return e;
+    k_triinv<T><<<lb.batch, 256, sm_tri, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps,
+                                               (T *)lb.Linv, (T *)lb.Uinv);
+    if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+    const int nleft = apply_left ? (J + TW - 1) / TW : 0;
+    const int nright = (lb.ncols - J - jb + TW - 1) / TW;
+    if (nleft + nright > 0) {
+      dim3 g(nleft + nright, lb.batch);
+      k_swap_trsm<T><<<g, 256, sm_trsm, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps,
+                                              lb.ipiv, (const T *)lb.Linv, nleft);
+      if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+    }
+    if (J + jb < lb.N) {
+      e = trail ? trail(trail_ctx, J, jb, st) : lu_trail_cuda<T>(M, lb, J, jb, st);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+template <typename T>
+static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
+                            bool upper, T *work, cudaStream_t st) {
+  const int nph = 256 / lb.NB;
+  size_t sm = sizeof(T) * ((size_t)nph * lb.NB * RT + (size_t)lb.NB * RT) + sizeof(int) * lb.N;
+  static bool attr_done[4] = {false, false, false, false};
+  const int ti = (sizeof(T) == sizeof(z64) ? 0 : 1) * 2 + (upper ? 1 : 0);
+  if (!attr_done[ti]) {
+    if (upper)
+      cudaFuncSetAttribute(k_trisolve<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    else
+      cudaFuncSetAttribute(k_trisolve<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done[ti] = true;
+  }
+  dim3 g(cdiv_u(R, RT), lb.batch);
+  if (upper)
+    k_trisolve<T, true><<<g, 256, sm, st>>>(M, lb.strideM, lb.N, lb.NB, lb.nsteps(), (const T *)lb.Uinv,
+                                            C, strideC, ldc, R, lb.ipiv, work);
+  else
+    k_trisolve<T, false><<<g, 256, sm, st>>>(M, lb.strideM, lb.N, lb.NB, lb.nsteps(), (const T *)lb.Linv,
+                                             C, strideC, ldc, R, lb.ipiv, work);
+  return ADGA_LAUNCH_CHECK();
+}
+
+template <typename T>
+cudaError_t lu_backsolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
+                         cudaStream_t st) {
+  return trisolve<T>(M, lb, C, strideC, ldc, R, true, nullptr, st);
+}
+
+// work: batch * ceil(R/16) * N * 16 elements
+template <typename T>
+cudaError_t lu_fwdsolve_ws(const T *M, const LUBatch &lb, T *V, size_t strideV, int ldv, int R,
+                           T *work, cudaStream_t st) {
+  return trisolve<T>(M, lb, V, strideV, ldv, R, false, work, st);
+}
+
+template cudaError_t lu_factor<z64>(z64 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t);
+template cudaError_t lu_factor<z32>(z32 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t);
+template cudaError_t lu_trail_cuda<z64>(z64 *, const LUBatch &, int, int, cudaStream_t);
+template cudaError_t lu_trail_cuda<z32>(z32 *, const LUBatch &, int, int, cudaStream_t);
+template cudaError_t lu_backsolve<z64>(const z64 *, const LUBatch &, z64 *, size_t, int, int, cudaStream_t);
+template cudaError_t lu_backsolve<z32>(const z32 *, const LUBatch &, z32 *, size_t, int, int, cudaStream_t);
+template cudaError_t lu_fwdsolve_ws<z64>(const z64 *, const LUBatch &, z64 *, size_t, int, int, z64 *,
+                                         cudaStream_t);
+template cudaError_t lu_fwdsolve_ws<z32>(const z32 *, const LUBatch &, z32 *, size_t, int, int, z32 *,
+                                         cudaStream_t);

@@ -1,0 +1,167 @@
+// FP64 iterative refinement of the mixed-precision BSE solve.
+//
+// The unknown is X = (1+gamma^w) A^-1 (ndim2 x N), solved from
+// X A = B with A = 1 - D F~ (D = blockdiag_nu(chi0^q chi0_loc^-1 - 1)).
+// The residual never needs A in FP64:
+//     r = B - X A = B - X + (X D) F~ ,
+// a (ndim2 x N) x (N x N) product per point with F~ shared by all q of one
+// omega (L2-resident), computed here as one batched FP64 GEMM per channel.
+// The correction d A = r is solved with the FP32 LU factors (forward with
+// L and the pivots, backward with U), and X += d in FP64.
+//
+// Buffers follow the LU batch order m = 2*p + ch.  X (FP64) and the FP32
+// right-hand sides V are N x R column-major per matrix, which is the same
+// memory as X stored R x N row-major.
+#include "ctx.cuh"
+
+// X64 = up(Y32) from the RHS columns of the FP32 factorised matrices
+__global__ void k_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X) {
+  size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t per = (size_t)N * R;
+  if (idx >= per * nmat) return;
+  size_t m = idx / per, e = idx % per;
+  X[idx] = to64(T32[m * strideM + (size_t)N * N + e]);
+}
+
+// XD(i1, i3 + nu*nd2) = sum_i2 X(i1, i2 + nu*nd2) sw_nu(i2, i3), row-major R x N
+__global__ void k_xd(DevCtx c, int npts, const z64 *X, const z64 *chi0q, const z64 *c0inv, z64 *XD) {
+  const int nd2 = c.nd2, N = c.N;
+  size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t per = (size_t)nd2 * N;
+  if (idx >= per * 2 * npts) return;
+  size_t m = idx / per, e = idx % per;
+  int i1 = (int)(e / N), col = (int)(e % N);
+  int nu = col / nd2, i3 = col % nd2;
+  int p = (int)(m >> 1);
+  const z64 *x = X + m * per + (size_t)i1 * N + (size_t)nu * nd2;
+  const z64 *cq = chi0q + (size_t)p * nd2 * nd2 * 2 * c.iwf + (size_t)nu * nd2 * nd2 + (size_t)i3 * nd2;
+  const z64 ci = c0inv[nu * nd2 + i3];
+  z64 s = make_double2(0.0, 0.0);
+  for (int i2 = 0; i2 < nd2; ++i2) {
+    z64 sw = cmul(cq[i2], ci);
+    if (i2 == i3) sw.x -= 1.0;
+    cfma(s, x[i2], sw);
+  }
+  XD[m * per + e] = s;
+}
+
+// residual GEMM for one channel: rows (p, i1), K = N, columns c:
+//   r(p,i1,c) = B(i1,c) - X(p,i1,c) + sum_m XD(p,i1,m) F~(m,c)  -> V32 (FP32)
+// 64 x 64 tiles, BK = 16, 256 threads, 4 x 4 complex outputs per thread.
+__global__ void __launch_bounds__(256)
+k_resid(int N, int R, int npts, int ch, const z64 *__restrict__ XD, const z64 *__restrict__ X,
+        const z64 *__restrict__ Frow, const z64 *__restrict__ opg, z32 *V) {
+  __shared__ z64 As[16][64];
+  __shared__ z64 Bs[16][64];
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+  const int rows = npts * R;
+  const int r0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
+  z64 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+  const size_t per = (size_t)R * N;
+  for (int k0 = 0; k0 < N; k0 += 16) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int e = t + 256 * i;
+      int kk = e & 15, rr = e >> 4;
+      int row = r0 + rr, k = k0 + kk;
+      z64 v = make_double2(0.0, 0.0);
+      if (row < rows && k < N) {
+        int p = row / R, i1 = row % R;
+        v = XD[(size_t)(2 * p + ch) * per + (size_t)i1 * N + k];
+      }
+      As[kk][rr] = v;
+      int cc = e & 63, kk2 = e >> 6;
+      int cl = c0 + cc, k2 = k0 + kk2;
+      Bs[kk2][cc] = (cl < N && k2 < N) ? Frow[(size_t)k2 * N + cl] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      z64 av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cfma(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int row = r0 + ty + 16 * i;
+    if (row >= rows) continue;
+    int p = row / R, i1 = row % R;
+    size_t m = (size_t)(2 * p + ch);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int cl = c0 + tx + 16 * j;
+      if (cl >= N) continue;
+      z64 b = opg[i1 + (size_t)cl * R];
+      z64 x = X[m * per + (size_t)i1 * N + cl];
+      z64 r = make_double2(b.x - x.x + acc[i][j].x, b.y - x.y + acc[i][j].y);
+      V[m * per + (size_t)i1 * N + cl] = to32(r);
+    }
+  }
+}
+
+// X += up(V); per-matrix max |d| and max |X| (|re|+|im|) into norms[2*m], norms[2*m+1]
+__global__ void k_update(int per, const z32 *V, z64 *X, unsigned long long *norms, const int *active) {
+  const int m = blockIdx.y;
+  if (active && !active[m]) return;
+  __shared__ double sd[8], sx[8];
+  double md = 0.0, mx = 0.0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < per; e += gridDim.x * blockDim.x) {
+    z64 d = to64(V[(size_t)m * per + e]);
+    z64 x = X[(size_t)m * per + e];
+    x.x += d.x; x.y += d.y;
+    X[(size_t)m * per + e] = x;
+    md = fmax(md, fabs(d.x) + fabs(d.y));
+    mx = fmax(mx, fabs(x.x) + fabs(x.y));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) { sd[threadIdx.x >> 5] = md; sx[threadIdx.x >> 5] = mx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { md = fmax(md, sd[w]); mx = fmax(mx, sx[w]); }
+    // non-negative doubles order like their bit patterns
+    atomicMax(norms + 2 * m, (unsigned long long)__double_as_longlong(md));
+    atomicMax(norms + 2 * m + 1, (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+cudaError_t launch_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X, cudaStream_t st) {
+  size_t total = (size_t)N * R * nmat;
+  k_init_x<<<cdiv_u(total, 256), 256, 0, st>>>(T32, strideM, N, R, nmat, X);
+  return ADGA_LAUNCH_CHECK();
+}
+
+cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q,
+                            const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
+                            const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, cudaStream_t st) {
+  size_t total = (size_t)c.nd2 * c.N * 2 * npts;
+  k_xd<<<cdiv_u(total, 256), 256, 0, st>>>(c, npts, X, chi0q, c0inv, XD);
+  cudaError_t e = ADGA_LAUNCH_CHECK();
+  if (e != cudaSuccess) return e;
+  dim3 g(cdiv_u(c.N, 64), cdiv_u((size_t)npts * c.R, 64));
+  k_resid<<<g, 256, 0, st>>>(c.N, c.R, npts, 0, XD, X, Frow_d, opg_d, V);
+  if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  k_resid<<<g, 256, 0, st>>>(c.N, c.R, npts, 1, XD, X, Frow_m, opg_m, V);
+  return ADGA_LAUNCH_CHECK();
+}
+
+cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,
+                          const int *active, cudaStream_t st) {
+  dim3 g(cdiv_u(per, 256 * 4), nmat);
+  k_update<<<g, 256, 0, st>>>(per, V, X, norms, active);
+  return ADGA_LAUNCH_CHECK();
+}

@@ -1,0 +1,45 @@
+// Batched complex LU with partial pivoting and blocked triangular solves.
+//
+// Replaces the zgetrf/zgetri pair of inverse_matrix_z (src/lapack_module.f90:40-70)
+// on the BSE matrices of src/main.F90:734-737.  The matrices are the
+// transposed BSE matrices T = A^T with the right-hand sides (1+gamma^w)^T
+// appended as extra columns, so that one factorisation P T = L U also
+// produces L^-1 P B^T, and X = B A^-1 follows from one back substitution
+// with U (the reference forms the full inverse instead).
+//
+// Layout: matrix b at base + b*strideM, column-major, ld = N rows,
+// ncols = N + R columns.  ipiv[b*N + i] holds the 0-based row swapped with
+// row i (LAPACK convention), info[b] the 1-based index of the first exactly
+// zero pivot.  Linv / Uinv hold the inverses of the NB x NB diagonal blocks
+// (ld NB) per matrix and step: they turn every triangular solve into small
+// GEMMs.
+#pragma once
+#include "common.cuh"
+
+struct LUBatch {
+  int N, ncols, batch, NB;
+  size_t strideM;
+  int *ipiv, *info;
+  void *Linv, *Uinv;        // [batch][nsteps][NB*NB] of the element type
+  int nsteps() const { return (N + NB - 1) / NB; }
+};
+
+// Trailing update C -= A B of one step (rows r0.., cols c0..), pluggable so
+// that the mixed path can route it to the tensor cores.
+typedef cudaError_t (*trail_fn)(void *ctx, int J, int jb, cudaStream_t st);
+
+template <typename T>
+cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
+                      cudaStream_t st);
+template <typename T>
+cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st);
+// U Y = C in place (C: N x R columns at C + b*strideC, ld ldc)
+template <typename T>
+cudaError_t lu_backsolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
+                         cudaStream_t st);
+// z = L^-1 P r in place (r: N x R columns at V + b*strideV, ld ldv); needs the
+// interchanges applied to the left columns too (apply_left in lu_factor).
+// work: batch * ceil(R/16) * N * 16 elements.
+template <typename T>
+cudaError_t lu_fwdsolve_ws(const T *M, const LUBatch &lb, T *V, size_t strideV, int ldv, int R,
+                           T *work, cudaStream_t st);

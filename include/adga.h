@@ -1,0 +1,195 @@
+/*
+ * adga.h -- C ABI of the B200 ladder hot path (libadga_b200.so).
+ *
+ * Every entry point replaces one call site or routine of the reference's
+ * per-(q, omega) loop (paths relative to the reference project root).  All
+ * arrays use the reference's Fortran layouts: column-major, complex values as
+ * interleaved (re, im) doubles (adga_z is layout-identical to Fortran
+ * complex(kind=8), C99 double _Complex and cuDoubleComplex), frequency axes
+ * stored from their lowest index.  Indices that the Fortran code passes
+ * 1-based (iq, k-point indices, q_data) stay 1-based here.
+ *
+ * Return value of every int function: 0 = ok; > 0 = LAPACK-style info (the
+ * 1-based index of the first exactly-zero pivot of an LU); < 0 = one of the
+ * ADGA_E* codes below.  adga_last_error() gives the message, in the spirit
+ * of the reference's (erstr, ierr) pairs (src/lapack_module.f90:40-70).
+ *
+ * Threading: calls on one handle must not overlap; distinct handles are
+ * independent.  Streams and CUDA graphs stay internal to the library.
+ */
+#ifndef ADGA_B200_H
+#define ADGA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct adga_z { double re, im; } adga_z;
+
+/* error codes (negative returns) */
+#define ADGA_EINVAL   (-1)   /* bad argument or inconsistent sizes          */
+#define ADGA_ECUDA    (-2)   /* CUDA runtime / driver error                  */
+#define ADGA_ENOMEM   (-3)   /* device allocation failed                     */
+#define ADGA_ETIMEOUT (-4)   /* a bounded device wait gave up                */
+#define ADGA_ESTATE   (-5)   /* call order violated (e.g. vertex not set)    */
+#define ADGA_ENOCONV  (-6)   /* mixed-precision refinement did not converge  */
+
+/* precision modes of the BSE solve */
+#define ADGA_FP64  0   /* complex FP64 LU + solves (the plain GPU path)            */
+#define ADGA_MIXED 1   /* complex FP32 LU, BF16x3 tensor-core updates, FP64 refine */
+
+/*
+ * Sizes and scalars of the run.  The reference keeps these as module
+ * globals (src/parameters_module.f90:43-58) that every hot routine reads
+ * implicitly; here they are passed once.
+ */
+typedef struct adga_dims {
+  int ndim;                    /* orbitals                                   */
+  int nkpx, nkpy, nkpz;        /* k-grid (nkp = product)                      */
+  int nqpx, nqpy, nqpz;        /* q-volume (nqp = product), q-grid on k-grid  */
+  int iwmax;                   /* one-particle box -iwmax..iwmax-1            */
+  int iwfmax_small;            /* two-particle box -iwf..iwf-1                */
+  int iwbmax_small;            /* bosonic -iwb..iwb                           */
+  int iwstart, iwstop;         /* chi0 nu range (src/config_module.f90:467-477)*/
+  int do_chi, do_eom;          /* calc-chi / calc-eom                          */
+  int nkp_eom;                 /* k points of the EOM (nkp for the full mesh) */
+  double beta, mu;
+} adga_dims;
+
+typedef struct adga_handle adga_handle;
+
+/*
+ * Upload the one-particle data, build G(k, nu) on the device and the k-q
+ * lookup tables.  Replaces the set-up of src/main.F90:161-375 that the loop
+ * depends on: iw_data (config_init, src/config_module.f90:510-513), hk
+ * (read_hk_w2w), siw/giw/dc, u/u_tilde (create_u / read_u), n_dmft
+ * (get_ndmft), q_data (generate_q_vol, src/kq_tools.f90:42-57) and
+ * k_data_eom.  Shapes (Fortran): iw_data(-iwmax:iwmax-1), hk(ndim,ndim,nkp),
+ * siw/giw(-iwmax:iwmax-1,ndim), dc(2,ndim), u/u_tilde(ndim2,ndim2),
+ * n_dmft(ndim), q_data(nqp) 1-based k indices, k_data_eom(nkp_eom) 1-based
+ * (NULL = 1..nkp).
+ */
+int adga_create(const adga_dims *d, const double *iw_data, const adga_z *hk,
+                const adga_z *siw, const adga_z *giw, const adga_z *dc,
+                const adga_z *u, const adga_z *u_tilde, const adga_z *n_dmft,
+                const int *q_data, const int *k_data_eom, adga_handle **out);
+int adga_destroy(adga_handle *h);
+const char *adga_last_error(const adga_handle *h);
+int adga_device_bytes(const adga_handle *h, long long *bytes);
+
+/*
+ * Stage chi_loc^{dens,magn}(omega = iwb) on the device, as returned by
+ * read_vertex (src/hdf5_module.f90:629-773): two maxdim x maxdim complex
+ * matrices in the compound index (i1 + nu*ndim2, i2 + nu'*ndim2).  Replaces
+ * the per-omega read at src/main.F90:525.  Every omega of a later
+ * adga_ladder_run must have been staged.
+ */
+int adga_set_vertex(adga_handle *h, int iwb, const adga_z *chi_loc_dens,
+                    const adga_z *chi_loc_magn);
+
+/* Zero the device accumulators (chi, bubble, Sigma) before a run. */
+int adga_reset_outputs(adga_handle *h);
+
+/* statistics of the last adga_ladder_run */
+typedef struct adga_run_stats {
+  int points;                  /* (q, omega) points processed                  */
+  int lu_info_nonzero;         /* points whose LU hit an exactly-zero pivot    */
+  int mixed_fallbacks;         /* mixed points re-solved in FP64               */
+  int max_refine_iters;        /* largest refinement count of a mixed point    */
+  double max_refine_resid;     /* largest final relative correction            */
+  double ms_total;             /* device time of the run (CUDA events)         */
+  double ms_chi0, ms_bse, ms_lu, ms_post, ms_eom;   /* per-stage device time   */
+} adga_run_stats;
+
+/*
+ * The batched (q, omega) loop of src/main.F90:486-799 over the compound
+ * points qwstart..qwstop (1-based, omega outer, q inner: qw(1,i) = iwb,
+ * qw(2,i) = iq, src/main.F90:381-389).  Results accumulate in device
+ * buffers exactly as the reference's arrays do (read them with
+ * adga_get_outputs): chi_qw_dens/magn and bubble_nl per point, bubble_loc,
+ * chi_loc_dens/magn per omega (only where the block holds iq = 1, like the
+ * reference), sigma_nl (ndim,ndim,-iwf:iwf-1,nkp_eom), sigma_dmft, sigma_hf.
+ * precision is ADGA_FP64 or ADGA_MIXED.  status (qwstop-qwstart+1 ints, may
+ * be NULL) receives the per-point LU info (> 0 zero pivot) or -1 for a
+ * mixed point that fell back to FP64.
+ */
+int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
+                    int *status, adga_run_stats *stats);
+
+/* Host copies of the accumulators; any pointer may be NULL. */
+typedef struct adga_outputs {
+  adga_z *chi_qw_dens;     /* (ndim2, ndim2, qwstart:qwstop) of the last run   */
+  adga_z *chi_qw_magn;
+  adga_z *bubble_nl;
+  adga_z *bubble_loc;      /* (ndim2, ndim2, -iwb:iwb)                          */
+  adga_z *chi_loc_dens;
+  adga_z *chi_loc_magn;
+  adga_z *sigma_nl;        /* (ndim, ndim, -iwf:iwf-1, nkp_eom), mirrored       */
+  adga_z *sigma_dmft;      /* (ndim, ndim, -iwf:iwf-1)                          */
+  adga_z *sigma_hf;        /* (ndim, ndim, nkp_eom)                             */
+} adga_outputs;
+int adga_get_outputs(adga_handle *h, const adga_outputs *o);
+
+/* ---- per-routine entry points (one (q, omega) point, host buffers) ---- */
+
+/* diag of chi0_loc / chi0_loc^-1 at (iwf, iwb) as ndim2 x ndim2 matrices;
+ * get_chi0_loc / get_chi0_loc_inv (src/one_particle_quant_module.f90:192-225) */
+int adga_get_chi0_loc(adga_handle *h, int iwf, int iwb, adga_z *chi0_loc);
+int adga_get_chi0_loc_inv(adga_handle *h, int iwf, int iwb, adga_z *chi0_loc_inv);
+
+/* k-summed bubble chi0q(ndim2,ndim2,-iwf:iwf-1) at (iq, iwb) and the
+ * bubble_nl update of src/main.F90:644-663 (bubble_nl may be NULL; it is
+ * overwritten with sum_nu chi0 / beta^2 - bubble_loc(iwb)).  Replaces the
+ * accumulate_chi0 k-loop (src/one_particle_quant_module.f90:228-290). */
+int adga_chi0_q(adga_handle *h, int iq, int iwb, adga_z *chi0q, adga_z *bubble_nl);
+
+/* BSE build + both inversions + eta for one point, src/main.F90:674-757.
+ * Needs adga_set_vertex(iwb).  Outputs (ndim2, maxdim): etaqd, etaqm,
+ * gammaqd (any may be NULL). */
+int adga_bse_point(adga_handle *h, int iq, int iwb, int precision,
+                   adga_z *etaqd, adga_z *etaqm, adga_z *gammaqd, int *lu_info);
+
+/* local gamma^w_d/m (ndim2, maxdim) of omega = iwb (src/main.F90:557-571) */
+int adga_get_gamma_w(adga_handle *h, int iwb, adga_z *gammawd, adga_z *gammawm);
+
+/* chi_qw += beta^-2 sum_{nu,i3} interm3(:,{i3,nu}) chi0_sum(i3,:,nu);
+ * calc_chi_qw (src/susc_module.f90:34-56) */
+int adga_calc_chi_qw(adga_handle *h, adga_z *chi_qw, const adga_z *interm3,
+                     const adga_z *chi0_sum);
+
+/* calc_eom_dynamic (src/eom_module.f90:165-233), V(q) = 0:
+ * sigma_nl(ndim,ndim,-iwf:iwf-1,nkp_eom) is accumulated in place. */
+int adga_calc_eom_dynamic(adga_handle *h, const adga_z *etaqd, const adga_z *etaqm,
+                          const adga_z *gammaqd, int iwb, int iq, adga_z *sigma_nl);
+
+/* calc_eom_dmft (src/eom_module.f90:115-161) and the local Hartree term of
+ * calc_eom_static (src/eom_module.f90:52-70); sigma_dmft(ndim,ndim,-iwf:iwf-1)
+ * is accumulated in place. */
+int adga_calc_eom_dmft(adga_handle *h, const adga_z *gammawd, int iwb, adga_z *sigma_dmft);
+int adga_calc_eom_static(adga_handle *h, int iq, adga_z *sigma_dmft);
+
+/* In-place inverse of an n x n complex matrix (lda = n) on the GPU:
+ * drop-in for inverse_matrix_z (src/lapack_module.f90:40-70).  ierr gets the
+ * LAPACK-style info, erstr (>= 200 chars, may be NULL) the reference's
+ * message ("ERROR in ZGETRF") on failure. */
+int adga_inverse_matrix_z(adga_z *M, int n, int *ierr, char *erstr);
+
+/* k - q index table ind(nkp_sel, nqp) (1-based), index_kq / index_kq_eom
+ * (src/kq_tools.f90:59-108); k_sel NULL = all k. */
+int adga_index_kq(int nkpx, int nkpy, int nkpz, const int *q_data, int nqp,
+                  const int *k_sel, int nk_sel, int *ind);
+
+/* q-volume q_data(nqp), generate_q_vol (src/kq_tools.f90:42-57). */
+int adga_generate_q_vol(int nkpx, int nkpy, int nkpz, int nqpx, int nqpy,
+                        int nqpz, int *q_data);
+
+/* Kanamori U for one atom of ndim correlated bands (interaction_mode 1):
+ * u({k,i},{j,l}) = U_ijkl, u_tilde({k,i},{j,l}) = U_ijlk;
+ * create_u (src/interaction_module.f90:182-291). Umat (ndim^4, may be NULL). */
+int adga_create_u(int ndim, double Udd, double Vdd, double Jdd, double *Umat,
+                  adga_z *u, adga_z *u_tilde);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADGA_B200_H */
