@@ -36,7 +36,9 @@ class RunStats(C.Structure):
     _fields_ = [("points", C.c_int), ("lu_info_nonzero", C.c_int), ("mixed_fallbacks", C.c_int),
                 ("max_refine_iters", C.c_int), ("max_refine_resid", C.c_double),
                 ("ms_total", C.c_double), ("ms_chi0", C.c_double), ("ms_bse", C.c_double),
-                ("ms_lu", C.c_double), ("ms_post", C.c_double), ("ms_eom", C.c_double)]
+                ("ms_lu", C.c_double), ("ms_post", C.c_double), ("ms_eom", C.c_double),
+                ("kernel_launches", C.c_longlong), ("ms_trail", C.c_double),
+                ("trail_gflop", C.c_double), ("trail_launches", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -18,6 +18,7 @@ cudaError_t tc_trail_setup(void **ctx, z32 *M, const LUBatch &lb, cudaStream_t s
 cudaError_t tc_trail_run(void *ctx, int J, int jb, cudaStream_t st);
 void tc_trail_free(void *ctx);
 int tc_available();
+int tc_trail_error(void *ctx);
 
 struct adga_handle {
   adga_dims d{};
@@ -378,12 +379,17 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   int mixed_fail = 0, iters = 0;
   double worst = 0.0;
   std::vector<int> fallback;
+  const int nst = (int)((N + NB - 1) / NB);
+  std::vector<cudaEvent_t> tev(2 * nst);
+  for (auto &x : tev) cudaEventCreate(&x);
+  TrailTiming tt;
+  tt.ev = tev.data();
   if (prec == ADGA_FP64) {
     z64 *T = (z64 *)h->Tm;
     CK(launch_bse_build<z64>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
                              strideM, h->gq, st));
     cudaEventRecord(ev[2], st);
-    CK(lu_factor<z64>(T, lb, false, nullptr, nullptr, st));
+    CK(lu_factor<z64>(T, lb, false, nullptr, nullptr, st, &tt));
     CK(lu_backsolve<z64>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     X = T + N * N; sp = 2 * strideM; sc = strideM;
   } else {
@@ -392,9 +398,9 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
                              strideM, h->gq, st));
     cudaEventRecord(ev[2], st);
     if (h->tc) {
-      CK(lu_factor<z32>(T, lb, true, tc_trail_run, h->tc, st));
+      CK(lu_factor<z32>(T, lb, true, tc_trail_run, h->tc, st, &tt));
     } else {
-      CK(lu_factor<z32>(T, lb, true, nullptr, nullptr, st));
+      CK(lu_factor<z32>(T, lb, true, nullptr, nullptr, st, &tt));
     }
     CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     CK(launch_init_x(T, strideM, (int)N, (int)R, 2 * np, h->X64, st));
@@ -444,12 +450,18 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   std::vector<int> info(2 * np);
   CK(cudaMemcpyAsync(info.data(), h->info, sizeof(int) * 2 * np, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if (prec == ADGA_MIXED && h->tc && tc_trail_error(h->tc))
+    return fail(h, ADGA_ETIMEOUT, "tensor-core trailing update: a bounded wait gave up");
   stage_ms(h, &h->stats.ms_chi0, ev[0], ev[1]);
   stage_ms(h, &h->stats.ms_bse, ev[1], ev[2]);
   stage_ms(h, &h->stats.ms_lu, ev[2], ev[3]);
   stage_ms(h, &h->stats.ms_post, ev[3], ev[4]);
   stage_ms(h, &h->stats.ms_eom, ev[4], ev[5]);
   for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+  for (int i = 0; i < tt.n; ++i) stage_ms(h, &h->stats.ms_trail, tev[2 * i], tev[2 * i + 1]);
+  h->stats.trail_launches += tt.n;
+  h->stats.trail_gflop += tt.gflop;
+  for (auto &x : tev) cudaEventDestroy(x);
   for (int p = 0; p < np; ++p) {
     int a = info[2 * p], b = info[2 * p + 1];
     int s = a ? a : b;
@@ -507,6 +519,7 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   int r = ensure_outputs(h, npts);
   if (r) return r;
   memset(&h->stats, 0, sizeof(h->stats));
+  const long long launches0 = g_adga_launches.load();
   CK(cudaMemsetAsync(h->chi_qw_d, 0, sizeof(z64) * npts * h->nd4, h->st));
   CK(cudaMemsetAsync(h->chi_qw_m, 0, sizeof(z64) * npts * h->nd4, h->st));
   CK(cudaMemsetAsync(h->bubble_nl, 0, sizeof(z64) * npts * h->nd4, h->st));
@@ -547,6 +560,7 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   float ms = 0.f;
   cudaEventElapsedTime(&ms, h->e0, h->e1);
   h->stats.ms_total = ms;
+  h->stats.kernel_launches = g_adga_launches.load() - launches0;
   h->last_npts = npts;
   if (stats) *stats = h->stats;
   return 0;

@@ -78,5 +78,8 @@ ADGA_HD z64 up64(z32 a) { return to64(a); }
 
 static inline unsigned cdiv_u(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 
-// Host-side launch check used by every launcher: returns cudaError_t.
-#define ADGA_LAUNCH_CHECK() cudaGetLastError()
+// Host-side launch check used after every kernel launch: counts the launch
+// (reported in adga_run_stats.kernel_launches) and returns cudaError_t.
+#include <atomic>
+inline std::atomic<long long> g_adga_launches{0};
+#define ADGA_LAUNCH_CHECK() (g_adga_launches.fetch_add(1, std::memory_order_relaxed), cudaGetLastError())

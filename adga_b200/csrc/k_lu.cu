@@ -484,7 +484,7 @@ cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t s
 
 template <typename T>
 cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
-                      cudaStream_t st) {
+                      cudaStream_t st, TrailTiming *tt) {
   if (lb.NB > MAXNB || lb.NB % SWD) return cudaErrorInvalidValue;
   const int nsteps = lb.nsteps();
   cudaError_t e;
@@ -512,8 +512,14 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
       if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
     }
     if (J + jb < lb.N) {
+      if (tt && tt->ev) cudaEventRecord(tt->ev[2 * tt->n], st);
       e = trail ? trail(trail_ctx, J, jb, st) : lu_trail_cuda<T>(M, lb, J, jb, st);
       if (e != cudaSuccess) return e;
+      if (tt && tt->ev) {
+        cudaEventRecord(tt->ev[2 * tt->n + 1], st);
+        tt->gflop += 8.0 * (lb.N - J - jb) * (double)(lb.ncols - J - jb) * jb * lb.batch * 1e-9;
+        tt->n++;
+      }
     }
   }
   return cudaSuccess;
@@ -556,8 +562,8 @@ cudaError_t lu_fwdsolve_ws(const T *M, const LUBatch &lb, T *V, size_t strideV, 
   return trisolve<T>(M, lb, V, strideV, ldv, R, false, work, st);
 }
 
-template cudaError_t lu_factor<z64>(z64 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t);
-template cudaError_t lu_factor<z32>(z32 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t);
+template cudaError_t lu_factor<z64>(z64 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t, TrailTiming *);
+template cudaError_t lu_factor<z32>(z32 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t, TrailTiming *);
 template cudaError_t lu_trail_cuda<z64>(z64 *, const LUBatch &, int, int, cudaStream_t);
 template cudaError_t lu_trail_cuda<z32>(z32 *, const LUBatch &, int, int, cudaStream_t);
 template cudaError_t lu_backsolve<z64>(const z64 *, const LUBatch &, z64 *, size_t, int, int, cudaStream_t);

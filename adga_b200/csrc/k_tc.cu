@@ -1,12 +1,395 @@
-// Tensor-core (tcgen05) trailing update of the mixed-precision LU.
-// Placeholder until the BF16x3 kernel lands: reports "not available" so the
-// mixed path uses the CUDA-core FP32 update.
+// Tensor-core (tcgen05) trailing update of the mixed-precision BSE LU:
+//     C -= L21 * U12        (complex FP32 storage, per matrix of the batch)
+// computed as a real BF16 GEMM with FP32 accumulation in TMEM using the
+// 3-term split x = x_hi + x_lo (x_hi = bf16(x), x_lo = bf16(x - x_hi)):
+//     L U ~= L_hi U_hi + L_hi U_lo + L_lo U_hi .
+// Complex arithmetic is embedded as
+//     [Re C | Im C] = [Lr | Li] . [[Ur, Ui], [-Ui, Ur]]
+// so one MMA with N = 2*BN produces the real (columns 0..BN) and imaginary
+// (BN..2BN) parts of BN complex columns.  Operands are staged per step by
+// k_split_a / k_split_b in K-major BF16 with every 3-term segment NB long:
+//     A[m]     = [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo]
+//     Bre[n]   = [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo, Ur_hi, -Ui_hi]
+//     Bim[n]   = [Ui_hi,  Ur_hi, Ui_lo,  Ur_lo, Ui_hi,  Ur_hi]
+// (K = 6*NB).  The GEMM kernel: warp 0 issues TMA loads (128B swizzle) into
+// a ring of shared-memory stages, warp 1 allocates TMEM and issues
+// tcgen05.mma (M=128, N=256, K=16) from one thread, warps 2-5 read the
+// accumulator with tcgen05.ld and apply C -= acc with coalesced FP32 stores.
+// Every mbarrier wait is bounded; on timeout the kernel records an error and
+// leaves.  Loads use no cluster multicast.
 #include "lu.cuh"
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cstdio>
 
-int tc_available() { return 0; }
-cudaError_t tc_trail_setup(void **ctx, z32 *, const LUBatch &, cudaStream_t) {
-  *ctx = nullptr;
-  return cudaErrorNotSupported;
+namespace {
+
+constexpr int BM = 128;          // rows per tile (MMA M)
+constexpr int BN = 128;          // complex columns per tile (MMA N = 2*BN)
+constexpr int BK = 64;           // bf16 per stage row (one 128 B swizzle atom)
+constexpr int STAGES = 2;
+constexpr int A_BYTES = BM * BK * 2;           // 16 KB
+constexpr int B_BYTES = 2 * BN * BK * 2;       // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int TMEM_COLS = 2 * BN;              // 256 fp32 columns
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s bound on any wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
 }
-cudaError_t tc_trail_run(void *, int, int, cudaStream_t) { return cudaErrorNotSupported; }
-void tc_trail_free(void *) {}
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: returns false (and records the error) after WAIT_NS
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *err, int code) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  for (;;) {
+    for (int i = 0; i < 64; ++i)
+      if (mbar_try(bar, parity)) return true;
+    if (gtimer() - t0 > WAIT_NS) {
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
+                                            int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"((unsigned long long)map), "r"(bar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+// K-major, 128 B swizzle: LBO = 16 B (unused), SBO = 1024 B between 8-row groups
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;                 // leading byte offset (16 B units)
+  d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+  d |= (uint64_t)1 << 46;                 // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
+  return d;
+}
+// kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 256
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(2 * BN / 8) << 17) |
+                           ((uint32_t)(BM / 16) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(IDESC), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(192, 1)
+k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+            z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int Ncols, int Ncap, int nkb,
+            int *err) {
+  extern __shared__ unsigned char smraw[];
+  const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
+  unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * STAGE_BYTES);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 1);
+  const uint32_t bar_full = smem_u32(bars), bar_empty = bar_full + 8 * STAGES,
+                 bar_acc = bar_full + 16 * STAGES;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM, b = blockIdx.z;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(bar_full + 8 * s, 1);
+      mbar_init(bar_empty + 8 * s, 1);
+    }
+    mbar_init(bar_acc, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  bool ok = true;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kb = 0; kb < nkb && ok; ++kb) {
+        const int s = kb % STAGES;
+        if (kb >= STAGES) ok = mbar_wait(bar_empty + 8 * s, ((kb / STAGES) - 1) & 1, err, 1);
+        if (!ok) break;
+        const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
+        mbar_expect_tx(bar_full + 8 * s, STAGE_BYTES);
+        tma_load_3d(sa, &mapA, bar_full + 8 * s, kb * BK, m0, b);
+        tma_load_3d(sb, &mapB, bar_full + 8 * s, kb * BK, n0, b);
+        tma_load_3d(sb + B_BYTES / 2, &mapB, bar_full + 8 * s, kb * BK, Ncap + n0, b);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      for (int kb = 0; kb < nkb && ok; ++kb) {
+        const int s = kb % STAGES;
+        ok = mbar_wait(bar_full + 8 * s, (kb / STAGES) & 1, err, 2);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
+#pragma unroll
+        for (int k = 0; k < BK / 16; ++k)
+          mma_bf16(tmem, smem_desc(sa + 32 * k), smem_desc(sb + 32 * k), (kb > 0 || k > 0) ? 1u : 0u);
+        mma_commit(bar_empty + 8 * s);
+      }
+      mma_commit(bar_acc);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32*(w%4).. (= tile rows)
+    const int quad = warp & 3;
+    const int row = quad * 32 + lane;
+    ok = mbar_wait(bar_acc, 0, err, 3);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok) {
+      const int m = m0 + row;
+      z32 *Cb = M + (size_t)b * strideM + (size_t)(J + jb + m);
+      const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16);
+#pragma unroll 1
+      for (int c = 0; c < BN; c += 16) {
+        float re[16], im[16];
+        tmem_ld16(tl + c, re);
+        tmem_ld16(tl + BN + c, im);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (m < Mrows) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int n = n0 + c + j;
+            if (n < Ncols) {
+              z32 *p = Cb + (size_t)(J + jb + n) * N;
+              z32 v = *p;
+              v.x -= re[j];
+              v.y -= im[j];
+              *p = v;
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 1) {
+    // every MMA has completed once bar_acc fired; on an error path the MMA
+    // thread issued no further work after its last commit
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// operand staging
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// A[b][m][6*NB]: rows m = 0..Mrows-1 are matrix rows J+jb+m, k = 0..NB-1 (zero for k >= jb)
+__global__ void __launch_bounds__(256)
+k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB, __nv_bfloat16 *A) {
+  __shared__ z32 tile[64][65];
+  const int b = blockIdx.y, m0 = blockIdx.x * 64;
+  const z32 *L = M + (size_t)b * strideM;
+  for (int kc = 0; kc < NB; kc += 64) {
+    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+      int mm = e & 63, kk = e >> 6;
+      int m = m0 + mm, k = kc + kk;
+      tile[mm][kk] = (m < Mrows && k < jb) ? L[(size_t)(J + jb + m) + (size_t)(J + k) * N]
+                                           : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+      int kk = e & 63, mm = e >> 6;
+      int m = m0 + mm;
+      if (m < Mrows) {
+        z32 v = tile[mm][kk];
+        __nv_bfloat16 rh, rl, ih, il;
+        split2(v.x, rh, rl);
+        split2(v.y, ih, il);
+        __nv_bfloat16 *row = A + ((size_t)b * N + m) * 6 * NB + kc + kk;
+        row[0 * NB] = rh; row[1 * NB] = ih;
+        row[2 * NB] = rh; row[3 * NB] = ih;
+        row[4 * NB] = rl; row[5 * NB] = il;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// B[b][n][6*NB] (real-part rows) and B[b][Ncap + n][6*NB] (imaginary-part rows)
+// for U rows J..J+jb-1 and columns n = 0..Ncols-1 (matrix columns J+jb+n)
+__global__ void __launch_bounds__(256)
+k_split_b(const z32 *M, size_t strideM, int N, int J, int jb, int Ncols, int Ncap, int NB,
+          __nv_bfloat16 *B) {
+  const int b = blockIdx.y;
+  const z32 *U = M + (size_t)b * strideM;
+  const int n = blockIdx.x * (blockDim.x / NB) + threadIdx.x / NB;
+  const int k = threadIdx.x % NB;
+  if (n >= Ncols) return;
+  z32 v = (k < jb) ? U[(size_t)(J + k) + (size_t)(J + jb + n) * N] : make_float2(0.f, 0.f);
+  __nv_bfloat16 rh, rl, ih, il;
+  split2(v.x, rh, rl);
+  split2(v.y, ih, il);
+  const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
+  __nv_bfloat16 *re = B + ((size_t)b * 2 * Ncap + n) * 6 * NB + k;
+  __nv_bfloat16 *im = B + ((size_t)b * 2 * Ncap + Ncap + n) * 6 * NB + k;
+  re[0 * NB] = rh; re[1 * NB] = nih; re[2 * NB] = rl; re[3 * NB] = nil; re[4 * NB] = rh; re[5 * NB] = nih;
+  im[0 * NB] = ih; im[1 * NB] = rh;  im[2 * NB] = il; im[3 * NB] = rl;  im[4 * NB] = ih; im[5 * NB] = rh;
+}
+
+// ---------------------------------------------------------------------------
+struct TcCtx {
+  z32 *M;
+  LUBatch lb;
+  __nv_bfloat16 *A = nullptr, *B = nullptr;
+  int *err = nullptr;
+  int Ncap = 0;
+  CUtensorMap mapA, mapB;
+};
+
+typedef CUresult (*encode_fn_t)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                CUtensorMapFloatOOBfill);
+
+encode_fn_t get_encode() {
+  static encode_fn_t fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void *p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (encode_fn_t)p;
+  }
+  return fn;
+}
+
+bool make_map(CUtensorMap *map, void *base, uint64_t inner, uint64_t rows, uint64_t batch) {
+  encode_fn_t enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[3] = {inner, rows, batch};
+  cuuint64_t strides[2] = {inner * 2, inner * rows * 2};
+  cuuint32_t box[3] = {BK, 128, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+int tc_available() {
+  int dev = 0, major = 0, minor = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+  return (major == 10 && minor == 0 && get_encode() != nullptr) ? 1 : 0;
+}
+
+cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream_t st) {
+  *ctx_out = nullptr;
+  if (lb.NB % 64) return cudaErrorInvalidValue;
+  TcCtx *c = new TcCtx();
+  c->M = M;
+  c->lb = lb;
+  c->Ncap = lb.ncols;
+  const size_t K6 = 6 * (size_t)lb.NB;
+  cudaError_t e = cudaMalloc(&c->A, sizeof(__nv_bfloat16) * K6 * lb.N * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->B, sizeof(__nv_bfloat16) * K6 * 2 * c->Ncap * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->err, 0, sizeof(int), st);
+  if (e == cudaSuccess && (!make_map(&c->mapA, c->A, K6, lb.N, lb.batch) ||
+                           !make_map(&c->mapB, c->B, K6, 2 * (uint64_t)c->Ncap, lb.batch)))
+    e = cudaErrorInvalidValue;
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  if (e != cudaSuccess) {
+    cudaFree(c->A); cudaFree(c->B); cudaFree(c->err);
+    delete c;
+    return e;
+  }
+  *ctx_out = c;
+  return cudaSuccess;
+}
+
+cudaError_t tc_trail_run(void *ctxp, int J, int jb, cudaStream_t st) {
+  TcCtx *c = (TcCtx *)ctxp;
+  const LUBatch &lb = c->lb;
+  const int Mrows = lb.N - J - jb, Ncols = lb.ncols - J - jb;
+  if (Mrows <= 0 || Ncols <= 0) return cudaSuccess;
+  const int NB = lb.NB;
+  k_split_a<<<dim3(cdiv_u(Mrows, 64), lb.batch), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Mrows, NB, c->A);
+  cudaError_t e = ADGA_LAUNCH_CHECK();
+  if (e != cudaSuccess) return e;
+  const int per = 256 / NB;
+  k_split_b<<<dim3(cdiv_u(Ncols, per), lb.batch), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Ncols,
+                                                                 c->Ncap, NB, c->B);
+  if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), lb.batch);
+  k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA, c->mapB, c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
+                                             c->Ncap, 6 * NB / BK, c->err);
+  return ADGA_LAUNCH_CHECK();
+}
+
+int tc_trail_error(void *ctxp) {
+  TcCtx *c = (TcCtx *)ctxp;
+  int v = 0;
+  if (cudaMemcpy(&v, c->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return v;
+}
+
+void tc_trail_free(void *ctxp) {
+  TcCtx *c = (TcCtx *)ctxp;
+  if (!c) return;
+  cudaFree(c->A);
+  cudaFree(c->B);
+  cudaFree(c->err);
+  delete c;
+}

@@ -28,9 +28,16 @@ struct LUBatch {
 // that the mixed path can route it to the tensor cores.
 typedef cudaError_t (*trail_fn)(void *ctx, int J, int jb, cudaStream_t st);
 
+// Optional timing of the trailing updates: events[2*s], events[2*s+1]
+// bracket the update of step s (pass nullptr to skip).
+struct TrailTiming {
+  cudaEvent_t *ev = nullptr;   // 2 * nsteps events, created by the caller
+  int n = 0;                   // number of pairs recorded
+  double gflop = 0.0;          // algorithmic flops of the recorded updates
+};
 template <typename T>
 cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
-                      cudaStream_t st);
+                      cudaStream_t st, TrailTiming *tt = nullptr);
 template <typename T>
 cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st);
 // U Y = C in place (C: N x R columns at C + b*strideC, ld ldc)

@@ -89,6 +89,8 @@ SPECS: Dict[str, Spec] = {
                hop=dict(t=0.26, tp=0.03, tpp=0.08), filling=0.2, seed=13, offdiag=0.04),
     "t3b": Spec("t3b", 3, (6, 6, 6), (3, 3, 3), 8, 2, 10.0, 5.0, 0.75, 3.5, model="t2g",
                 hop=dict(t=0.26, tp=0.03, tpp=0.08), filling=1.0 / 6.0, seed=14, offdiag=0.03),
+    "t3m": Spec("t3m", 3, (4, 4, 4), (2, 2, 2), 12, 1, 10.0, 5.0, 0.75, 3.5, model="t2g",
+                hop=dict(t=0.26, tp=0.03, tpp=0.08), filling=1.0 / 6.0, seed=16, offdiag=0.03),
     "t5": Spec("t5", 5, (2, 2, 2), (2, 1, 1), 2, 1, 10.0, 3.0, 0.5, model="d5",
                hop=dict(t=0.2, t2=0.12), filling=0.3, seed=15, offdiag=0.03),
 }

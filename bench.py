@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the ladder hot path: BSE q.omega points/s on the SrVO3-like
+t2g workload (3 orbitals, 20^3 k, 10^3 q, 2x60 fermionic and 21 bosonic
+frequencies, BSE matrices 1080 x 1080 complex, 21,000 points).
+
+One step = one bosonic slice: the full (q, omega) loop body for all 1000 q
+points of one omega (chi0 bubble, both BSE channels, chi sums, EOM).
+`value` is the mixed-precision path (FP32 LU with BF16x3 tensor-core updates
+and FP64 refinement); the plain FP64 GPU path is timed on the same steps and
+reported beside it, with the relative error between the two and against the
+FP64 oracle on sampled points.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank drives one GPU on its own omega slices (weak
+scaling, no data-path collective); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BSE q·ω pts/s at 1e-8 rel err vs FP64 oracle: mixed-prec vs plain FP64 on B200"
+UNIT = "qw_points/s"
+WORKLOAD = "c1"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 arm")
+    ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle on host cores, one (q, omega) point per worker
+# ---------------------------------------------------------------------------
+_W = {}
+
+
+def _cpu_init(workload, iwb):
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from adga_b200 import synth
+    from oracle.adga_oracle import LadderInputs, Oracle
+    p = synth.make_problem(workload)
+    s = p.spec
+    inp = LadderInputs(ndim=s.ndim, nk=s.nk, nq=s.nq, iwmax=p.iwmax, iwfmax_small=s.iwf,
+                       iwbmax_small=s.iwb, beta=p.beta, mu=p.mu, hk=p.hk, siw=p.siw, giw=p.giw,
+                       dc=p.dc, u=p.u, u_tilde=p.u_tilde, n_dmft=p.n_dmft, vertex=p.vertex,
+                       iw_data=p.iw_data)
+    o = Oracle(inp)
+    import numpy as np
+    scratch = {k: np.zeros((p.ndim2, p.ndim2, 2 * s.iwb + 1), complex)
+               for k in ("bubble_loc", "chi_loc_dens", "chi_loc_magn")}
+    _W.update(o=o, loc=o.local_block(iwb, 1, scratch), iwb=iwb, p=p)
+
+
+def _cpu_point(iq):
+    """One point of the reference loop body: chi0, BSE build, two zgetrf+zgetri
+    inversions, eta, chi sums and the EOM contribution."""
+    import numpy as np
+    o, loc, iwb, p = _W["o"], _W["loc"], _W["iwb"], _W["p"]
+    t = time.perf_counter()
+    res = o.point(iq, iwb, loc)
+    sig = np.zeros((p.ndim, p.ndim, 2 * p.spec.iwf, p.spec.nkp), complex, order="F")
+    o.calc_eom_dynamic(res["etaqd"], res["etaqm"], res["gammaqd"], iwb, iq, sig)
+    return time.perf_counter() - t, res["chi_qw_dens"], res["chi_qw_magn"]
+
+
+class CpuPool:
+    def __init__(self, workload, iwb, nproc):
+        import multiprocessing as mp
+        self.n = nproc
+        self.pool = mp.get_context("spawn").Pool(nproc, initializer=_cpu_init, initargs=(workload, iwb))
+        self.pool.map(_cpu_point, [0] * nproc)          # warm every worker once
+
+    def step(self, iqs):
+        t = time.perf_counter()
+        res = self.pool.map(_cpu_point, iqs, chunksize=1)
+        return time.perf_counter() - t, res
+
+    def close(self):
+        self.pool.terminate()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.samples, self.proc, self.gpu = [], None, gpu_index
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        import statistics
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import numpy as np
+    from adga_b200 import synth
+    spec = synth.SPECS[args.workload]
+    cores = os.cpu_count() or 1
+    pool = CpuPool(args.workload, 0, cores)
+    rng = np.random.default_rng(0)
+    times = []
+    npts = cores
+    for it in range(args.warmup + args.steps):
+        iqs = [int(x) for x in rng.integers(0, spec.nqp, npts)]
+        dt, _ = pool.step(iqs)
+        if it >= args.warmup:
+            times.append(dt)
+    pool.close()
+    v = npts * len(times) / sum(times)
+    sample = (f"{npts} (q, omega=0) points per step of the {args.workload} slice, one per process "
+              f"on {cores} host cores, FP64 oracle port (zgetrf+zgetri via OpenBLAS, 1 thread each)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)",
+            "data": "synthetic",
+            "config": config(args, spec),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config(args, spec):
+    return {"workload": f"{args.workload}: SrVO3-like t2g, ndim={spec.ndim}, k={spec.nk}, q={spec.nq}, "
+                        f"2x{spec.iwf} fermionic x {2 * spec.iwb + 1} bosonic, BSE N={spec.maxdim} complex",
+            "points_per_step": spec.nqp, "step": "one omega slice (all q at one bosonic frequency)",
+            "l2": "inputs larger than L2 (BSE matrices of one slice: ~19 GB FP32 / ~38 GB FP64)",
+            "parallelism": f"replicas x{args.gpus} (independent omega slices per GPU)"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        # one GPU per process: the library's runtime and torch both see device 0
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    if args.impl == "reference":
+        if world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", init_method="env://")
+        run_reference(args, rank)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    import numpy as np
+    from adga_b200 import synth
+    spec = synth.SPECS[args.workload]
+    cores = os.cpu_count() or 1
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = CpuPool(args.workload, 0, args.cpu_points or cores)   # spawned before any GPU call
+
+    import torch
+    import torch.distributed as dist
+    from adga_b200 import Ladder
+    if world > 1:
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", init_method="env://")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p = synth.make_problem(args.workload)
+    nw = 2 * spec.iwb + 1
+    nsteps = args.warmup + args.steps
+    omegas = [(-spec.iwb + (rank * nsteps + s) % nw) for s in range(nsteps)]
+    # pinned host copies of the vertices (the e2e inputs)
+    pinned = {}
+    for iwb in sorted(set(omegas) | {0}):     # omega = 0 is also the CPU-sample slice
+        d, m = p.vertex(iwb)
+        pd = torch.empty(d.size, dtype=torch.complex128).pin_memory().numpy().reshape(d.shape, order="F")
+        pm = torch.empty(m.size, dtype=torch.complex128).pin_memory().numpy().reshape(m.shape, order="F")
+        pd[...] = d
+        pm[...] = m
+        pinned[iwb] = (pd, pm)
+    p.clear_vertex_cache()
+    lad = Ladder.from_problem(p)
+    for iwb, (d, m) in pinned.items():
+        lad.set_vertex(iwb, d, m)
+
+    def slice_range(iwb):
+        q0 = (iwb + spec.iwb) * spec.nqp + 1
+        return q0, q0 + spec.nqp - 1
+
+    def timed(prec):
+        for s in range(args.warmup):
+            lad.ladder_run(*slice_range(omegas[s]), prec)
+        barrier()
+        ms, stats = 0.0, []
+        with ClockSampler() as clk:
+            for s in range(args.warmup, nsteps):
+                _, st = lad.ladder_run(*slice_range(omegas[s]), prec)
+                ms += st["ms_total"]
+                stats.append(st)
+            barrier()
+        return allmax(ms), stats, clk.summary()
+
+    ms_mixed, st_mixed, clk = timed("mixed")
+    v_mixed = world * spec.nqp * args.steps / (ms_mixed * 1e-3)
+    res = {}
+    if not args.no_fp64:
+        ms64, st64, clk64 = timed("fp64")
+        res["fp64"] = world * spec.nqp * args.steps / (ms64 * 1e-3)
+
+    # accuracy: mixed vs FP64 on the same slice, and vs the oracle on sampled points
+    iwb_chk = omegas[-1]
+    acc = {}
+    lad.reset_outputs()
+    lad.ladder_run(*slice_range(iwb_chk), "fp64")
+    o64 = lad.get_outputs()
+    lad.reset_outputs()
+    lad.ladder_run(*slice_range(iwb_chk), "mixed")
+    omx = lad.get_outputs()
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+    a64 = lad.assemble(o64, p.siw)
+    amx = lad.assemble(omx, p.siw)
+    acc["mixed_vs_fp64"] = {k: rel(amx[k], a64[k]) for k in ("chi_dens", "chi_magn", "sigma")}
+
+    # e2e: through the C ABI with host buffers (pinned h2d of the slice's
+    # vertex, the run, d2h of every accumulator) on the device already set up
+    e2e_t, h2d, d2h = 0.0, 0, 0
+    barrier()
+    for s in range(args.warmup, nsteps):
+        iwb = omegas[s]
+        t = time.perf_counter()
+        lad.set_vertex(iwb, *pinned[iwb])
+        lad.ladder_run(*slice_range(iwb), "mixed")
+        out = lad.get_outputs()
+        e2e_t += time.perf_counter() - t
+        h2d = sum(x.nbytes for x in pinned[iwb])
+        d2h = sum(v.nbytes for v in out.values())
+    e2e_t = allmax(e2e_t)
+    e2e = {"value": world * spec.nqp * args.steps / e2e_t, "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    # CPU baseline + oracle check on sampled points (rank 0)
+    cpu_line = None
+    if cpu is not None:
+        rng = np.random.default_rng(1)
+        iqs = [int(x) for x in rng.integers(0, spec.nqp, cpu.n)]
+        dt, pts = cpu.step(iqs)
+        cpu.close()
+        cpu_line = {"value": len(iqs) / dt, "unit": UNIT, "cores": cpu.n, "kind": "port",
+                    "sample": f"{len(iqs)} random q points of the {args.workload} omega=0 slice, one per "
+                              f"process (single-threaded OpenBLAS), FP64 oracle port"}
+        lad.reset_outputs()
+        lad.ladder_run(*slice_range(0), "mixed")
+        om = lad.get_outputs()
+        q0 = slice_range(0)[0]
+        errs = []
+        for iq, (_, cd, cm) in zip(iqs, pts):
+            errs.append(max(rel(om["chi_qw_dens"][:, :, iq], cd), rel(om["chi_qw_magn"][:, :, iq], cm)))
+        acc["mixed_vs_oracle_chi_nl_sampled"] = max(errs)
+
+    # roofline of the dominant kernel: the LU trailing update
+    pk, pk_kind = peaks()
+    gflop = sum(s["trail_gflop"] for s in st_mixed)
+    mst = sum(s["ms_trail"] for s in st_mixed)
+    nlaunch = sum(s["trail_launches"] for s in st_mixed)
+    achieved = gflop / mst if mst else 0.0          # TFLOP/s (GF / ms)
+    peak = pk.get("bf16_tflops_sustained") or pk.get("bf16_tflops")
+    roof = {"kernel": "LU trailing update (mixed path)", "bound": "tensor", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+            "traffic": None, "peak_kind": f"bf16 sustained, {pk_kind}",
+            "flops_per_launch": gflop * 1e9 / max(nlaunch, 1),
+            "avg_launch_ms": mst / max(nlaunch, 1)}
+    stage = {k: sum(s[k] for s in st_mixed) / args.steps for k in
+             ("ms_chi0", "ms_bse", "ms_lu", "ms_trail", "ms_post", "ms_eom", "ms_total")}
+    line = {"metric": METRIC, "value": v_mixed, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed: c64 LU (bf16x3 tensor-core updates, f32 accumulate) + c128 refinement; "
+                     "chi0/EOM c128",
+            "data": "synthetic (seeded SrVO3-like t2g model, chi_loc = (chi0_loc^-1 + Gamma)^-1)",
+            "config": config(args, spec), "fp64_value": res.get("fp64"),
+            "mixed_over_fp64": (v_mixed / res["fp64"]) if res.get("fp64") else None,
+            "accuracy": acc, "stage_ms_per_step": stage,
+            "refine": {"max_iters": max(s["max_refine_iters"] for s in st_mixed),
+                       "fallbacks": sum(s["mixed_fallbacks"] for s in st_mixed)},
+            "roofline": roof, "cpu_baseline": cpu_line, "e2e": e2e,
+            "gpu_launches": int(sum(s["kernel_launches"] for s in st_mixed)),
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+    lad.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -29,7 +29,7 @@ def compare(got, want, tol, keys=KEYS):
     return errs
 
 
-@pytest.mark.parametrize("name", ["t1", "t2", "t3", "t5"])
+@pytest.mark.parametrize("name", ["t1", "t2", "t3", "t5", "t3m"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_full_ladder_matches_oracle(name, prec):
     p = problem(name)
@@ -37,6 +37,10 @@ def test_full_ladder_matches_oracle(name, prec):
     want = oracle_run(p)
     assert np.all(got["status"] >= 0)
     compare(got, want, TOL[prec])
+    if prec == "mixed":
+        # the mixed LU must converge on its own (no FP64 re-solve)
+        assert got["stats"]["mixed_fallbacks"] == 0
+        assert got["stats"]["max_refine_iters"] <= 4
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
