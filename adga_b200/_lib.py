@@ -21,6 +21,7 @@ EXPORTS = [
     "adga_get_chi0_loc_inv", "adga_chi0_q", "adga_bse_point", "adga_get_gamma_w",
     "adga_calc_chi_qw", "adga_calc_eom_dynamic", "adga_calc_eom_dmft", "adga_calc_eom_static",
     "adga_inverse_matrix_z", "adga_index_kq", "adga_generate_q_vol", "adga_create_u",
+    "adga_inverse_matrix_z_noalloc",
 ]
 
 
@@ -81,6 +82,7 @@ def load():
         "adga_calc_eom_dmft": [vp, vp, i, vp],
         "adga_calc_eom_static": [vp, i, vp],
         "adga_inverse_matrix_z": [vp, i, ip, C.c_char_p],
+        "adga_inverse_matrix_z_noalloc": [vp, vp, i, ip, vp],
         "adga_index_kq": [i, i, i, vp, i, vp, i, vp],
         "adga_generate_q_vol": [i, i, i, i, i, i, vp],
         "adga_create_u": [i, d, d, d, vp, vp, vp],

@@ -178,6 +178,22 @@ int adga_calc_eom_static(adga_handle *h, int iq, adga_z *sigma_dmft);
  * message ("ERROR in ZGETRF") on failure. */
 int adga_inverse_matrix_z(adga_z *M, int n, int *ierr, char *erstr);
 
+/* Inverse of an n x n complex matrix held in device memory, allocating no
+ * device memory: for callers that cannot call cudaMalloc (their device
+ * memory belongs to another allocator, or the library must not grow the
+ * footprint).  M_dev (n x n, column-major) is read, Minv_dev receives the
+ * inverse; both are device pointers owned by the caller.  All scratch sits in
+ * one file-scope device array of ADGA_NOALLOC_MAX_N-sized buffers (about
+ * 2.6 MB per GPU, held until exit); n > ADGA_NOALLOC_MAX_N returns
+ * ADGA_EINVAL.  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress): make it before any stream capture.  Calls share
+ * the array, so calls that overlap on the GPU race.  stream may be NULL (the
+ * default stream); when ierr is non-NULL the call waits for the stream and
+ * stores the LAPACK-style info.  No counterpart in the reference. */
+#define ADGA_NOALLOC_MAX_N 256
+int adga_inverse_matrix_z_noalloc(const adga_z *M_dev, adga_z *Minv_dev, int n, int *ierr,
+                                  void *stream);
+
 /* k - q index table ind(nkp_sel, nqp) (1-based), index_kq / index_kq_eom
  * (src/kq_tools.f90:59-108); k_sel NULL = all k. */
 int adga_index_kq(int nkpx, int nkpy, int nkpz, const int *q_data, int nqp,
