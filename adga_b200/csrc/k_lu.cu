@@ -453,6 +453,83 @@ k_trisolve(const T *M, size_t strideM, int N, int NB, int nsteps, const T *Dinv,
 }
 
 // ---------------------------------------------------------------------------
+// Blocked triangular solve with the right-hand sides resident in shared
+// memory (R <= RMAX columns, N*R elements): one CTA per matrix, right-looking
+// over the NB-row blocks.  Per block: X_blk = Dinv * C_blk, then the rows not
+// yet solved are updated with the matching column block of U (backward) or L
+// (forward), one thread per row, so every element of the triangle is read
+// from HBM exactly once with coalesced column accesses.  The forward solve
+// applies the row interchanges P while loading the right-hand sides.
+// ---------------------------------------------------------------------------
+template <typename T, bool UPPER, int RMAX>
+__global__ void __launch_bounds__(512)
+k_trisolve_smem(const T *M, size_t strideM, int N, int NB, int nsteps, const T *Dinv, T *C,
+                size_t strideC, int ldc, int R, const int *ipiv_all) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *Cs = reinterpret_cast<T *>(smraw);            // [R][N]
+  T *Yt = Cs + (size_t)N * R;                        // [R][NB]
+  int *perm = reinterpret_cast<int *>(Yt + (size_t)NB * R);
+  const int b = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
+  const T *A = M + (size_t)b * strideM;
+  T *Cb = C + (size_t)b * strideC;
+  if (!UPPER) {
+    if (t == 0) {
+      for (int i = 0; i < N; ++i) perm[i] = i;
+      const int *ip = ipiv_all + (size_t)b * N;
+      for (int i = 0; i < N; ++i) {
+        const int p = ip[i];
+        if (p != i) { int x = perm[i]; perm[i] = perm[p]; perm[p] = x; }
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = t; e < N * R; e += nt) {
+    const int i = e % N, r = e / N;
+    Cs[e] = Cb[(size_t)(UPPER ? i : perm[i]) + (size_t)r * ldc];
+  }
+  __syncthreads();
+  for (int s = 0; s < nsteps; ++s) {
+    const int blk = UPPER ? nsteps - 1 - s : s;
+    const int J = blk * NB, jb = min(NB, N - J);
+    const T *Di = Dinv + ((size_t)b * nsteps + blk) * NB * NB;
+    for (int e = t; e < jb * R; e += nt) {
+      const int i = e % jb, r = e / jb;
+      T v = czero<T>();
+      const int kb = UPPER ? i : 0, ke = UPPER ? jb : i + 1;
+      for (int k = kb; k < ke; ++k) cfma(v, Di[i + k * NB], Cs[(size_t)r * N + J + k]);
+      Yt[(size_t)r * NB + i] = v;
+    }
+    __syncthreads();
+    for (int e = t; e < jb * R; e += nt) {
+      const int i = e % jb, r = e / jb;
+      Cs[(size_t)r * N + J + i] = Yt[(size_t)r * NB + i];
+    }
+    const int rb = UPPER ? 0 : J + jb, re = UPPER ? J : N;
+    for (int i = rb + t; i < re; i += nt) {
+      T acc[RMAX];
+#pragma unroll
+      for (int r = 0; r < RMAX; ++r) acc[r] = czero<T>();
+      const T *col = A + i + (size_t)J * N;
+#pragma unroll 4
+      for (int k = 0; k < jb; ++k) {
+        const T u = col[(size_t)k * N];
+#pragma unroll
+        for (int r = 0; r < RMAX; ++r)
+          if (r < R) cfma(acc[r], u, Yt[(size_t)r * NB + k]);
+      }
+#pragma unroll
+      for (int r = 0; r < RMAX; ++r)
+        if (r < R) Cs[(size_t)r * N + i] = csub(Cs[(size_t)r * N + i], acc[r]);
+    }
+    __syncthreads();
+  }
+  for (int e = t; e < N * R; e += nt) {
+    const int i = e % N, r = e / N;
+    Cb[(size_t)i + (size_t)r * ldc] = Cs[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -528,6 +605,31 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
 template <typename T>
 static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
                             bool upper, T *work, cudaStream_t st) {
+  // few right-hand sides that fit in shared memory: the resident-RHS kernel
+  const size_t sm_small = sizeof(T) * ((size_t)lb.N * R + (size_t)lb.NB * R) + sizeof(int) * lb.N;
+  if (R <= 25 && sm_small <= 200 * 1024) {
+    static bool attr_small[8] = {false};
+    const int ti = (sizeof(T) == sizeof(z64) ? 0 : 1) * 4 + (upper ? 2 : 0) + (R <= 16 ? 0 : 1);
+    const int np = lb.nsteps();
+#define TS_LAUNCH(UP, RM)                                                                            \
+    do {                                                                                             \
+      if (!attr_small[ti]) {                                                                         \
+        cudaFuncSetAttribute(k_trisolve_smem<T, UP, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             200 * 1024);                                                            \
+        attr_small[ti] = true;                                                                       \
+      }                                                                                              \
+      k_trisolve_smem<T, UP, RM><<<lb.batch, 512, sm_small, st>>>(                                   \
+          M, lb.strideM, lb.N, lb.NB, np, (const T *)(UP ? lb.Uinv : lb.Linv), C, strideC, ldc, R,   \
+          lb.ipiv);                                                                                  \
+    } while (0)
+    if (upper) {
+      if (R <= 16) TS_LAUNCH(true, 16); else TS_LAUNCH(true, 25);
+    } else {
+      if (R <= 16) TS_LAUNCH(false, 16); else TS_LAUNCH(false, 25);
+    }
+#undef TS_LAUNCH
+    return ADGA_LAUNCH_CHECK();
+  }
   const int nph = 256 / lb.NB;
   size_t sm = sizeof(T) * ((size_t)nph * lb.NB * RT + (size_t)lb.NB * RT) + sizeof(int) * lb.N;
   static bool attr_done[4] = {false, false, false, false};
@@ -539,6 +641,7 @@ static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC,
       cudaFuncSetAttribute(k_trisolve<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_done[ti] = true;
   }
+  if (!upper && !work) return cudaErrorInvalidValue;
   dim3 g(cdiv_u(R, RT), lb.batch);
   if (upper)
     k_trisolve<T, true><<<g, 256, sm, st>>>(M, lb.strideM, lb.N, lb.NB, lb.nsteps(), (const T *)lb.Uinv,

@@ -190,23 +190,31 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
       const int m = m0 + row;
       z32 *Cb = M + (size_t)b * strideM + (size_t)(J + jb + m);
       const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16);
+      const bool rowok = m < Mrows;
 #pragma unroll 1
-      for (int c = 0; c < BN; c += 16) {
-        float re[16], im[16];
-        tmem_ld16(tl + c, re);
-        tmem_ld16(tl + BN + c, im);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (m < Mrows) {
+      for (int c = 0; c < BN; c += 32) {
+        // all loads of the chunk are issued before any store, so the 32
+        // read-modify-writes of this thread overlap in the memory system
+        z32 cv[32];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int n = n0 + c + j;
-            if (n < Ncols) {
-              z32 *p = Cb + (size_t)(J + jb + n) * N;
-              z32 v = *p;
-              v.x -= re[j];
-              v.y -= im[j];
-              *p = v;
-            }
+        for (int j = 0; j < 32; ++j) {
+          const int n = n0 + c + j;
+          cv[j] = (rowok && n < Ncols) ? Cb[(size_t)(J + jb + n) * N] : make_float2(0.f, 0.f);
+        }
+        float re[32], im[32];
+        tmem_ld16(tl + c, *reinterpret_cast<float(*)[16]>(re));
+        tmem_ld16(tl + c + 16, *reinterpret_cast<float(*)[16]>(re + 16));
+        tmem_ld16(tl + BN + c, *reinterpret_cast<float(*)[16]>(im));
+        tmem_ld16(tl + BN + c + 16, *reinterpret_cast<float(*)[16]>(im + 16));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int n = n0 + c + j;
+          if (rowok && n < Ncols) {
+            z32 v = cv[j];
+            v.x -= re[j];
+            v.y -= im[j];
+            Cb[(size_t)(J + jb + n) * N] = v;
           }
         }
       }
