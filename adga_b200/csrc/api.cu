@@ -48,7 +48,7 @@ struct adga_handle {
   z64 *etad = nullptr, *etam = nullptr;
   int *qidx_d = nullptr, *qidx_h = nullptr;
   void *Tm = nullptr, *Linv = nullptr, *Uinv = nullptr;
-  int *ipiv = nullptr, *info = nullptr;
+  int *ipiv = nullptr, *info = nullptr, *rmap = nullptr;
   int NB = 64;
   z64 *X64 = nullptr, *XD = nullptr;
   z32 *V32 = nullptr, *work32 = nullptr;
@@ -56,7 +56,7 @@ struct adga_handle {
   void *tc = nullptr;
   // refinement settings
   int max_iter = 8;
-  double tol = 1e-12;
+  double tol = 1e-10;   // stop when max|dX| <= tol * max|X| (the error is then far below)
   // last-run statistics
   adga_run_stats stats{};
 };
@@ -318,7 +318,8 @@ static int ensure_work(adga_handle *h, int prec, int want) {
             alloc_into(h, h->etad, (size_t)cap * nd2 * N, W) &&
             alloc_into(h, h->etam, (size_t)cap * nd2 * N, W) &&
             alloc_into(h, h->qidx_d, cap, W) && alloc_into(h, h->ipiv, (size_t)2 * cap * N, W) &&
-            alloc_into(h, h->info, (size_t)2 * cap, W);
+            alloc_into(h, h->info, (size_t)2 * cap, W) &&
+            alloc_into(h, h->rmap, (size_t)2 * cap * RMAP_STRIDE, W);
   if (ok && h->bigbox) ok = alloc_into(h, h->chi0q_big, (size_t)cap * h->nd4 * 2 * c.iwf, W);
   if (ok) {
     const size_t es = prec == ADGA_FP64 ? 16 : 8;
@@ -343,7 +344,7 @@ static int ensure_work(adga_handle *h, int prec, int want) {
   h->cap = cap;
   h->cap_prec = prec;
   if (prec == ADGA_MIXED && tc_available() && !getenv("ADGA_NO_TC")) {
-    LUBatch lb{(int)N, (int)(N + R), 2 * cap, NB, N * (N + R), h->ipiv, h->info, h->Linv, h->Uinv};
+    LUBatch lb{(int)N, (int)(N + R), 2 * cap, NB, N * (N + R), h->ipiv, h->info, h->Linv, h->Uinv, h->rmap};
     if (tc_trail_setup(&h->tc, (z32 *)h->Tm, lb, h->st) != cudaSuccess) h->tc = nullptr;
   }
   return 0;
@@ -372,7 +373,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
                         do_chi ? bub_nl + (size_t)off * h->nd4 : nullptr, st));
   cudaEventRecord(ev[1], st);
   const size_t strideM = N * (N + R);
-  LUBatch lb{(int)N, (int)(N + R), 2 * np, NB, strideM, h->ipiv, h->info, h->Linv, h->Uinv};
+  LUBatch lb{(int)N, (int)(N + R), 2 * np, NB, strideM, h->ipiv, h->info, h->Linv, h->Uinv, h->rmap};
   CK(cudaMemsetAsync(h->info, 0, sizeof(int) * 2 * np, st));
   const z64 *X = nullptr;
   size_t sp = 0, sc = 0;
@@ -807,7 +808,7 @@ extern "C" int adga_inverse_matrix_z(adga_z *M, int n, int *ierr, char *erstr) {
   const int NB = 64, nsteps = (n + NB - 1) / NB;
   const size_t strideM = (size_t)n * 2 * n;
   z64 *T = nullptr, *Li = nullptr, *Ui = nullptr;
-  int *ip = nullptr, *inf = nullptr;
+  int *ip = nullptr, *inf = nullptr, *rm = nullptr;
   cudaStream_t st;
   if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return ADGA_ECUDA;
   int rc = 0;
@@ -821,10 +822,11 @@ extern "C" int adga_inverse_matrix_z(adga_z *M, int n, int *ierr, char *erstr) {
   if (cudaMalloc(&T, sizeof(z64) * strideM) != cudaSuccess ||
       cudaMalloc(&Li, sizeof(z64) * nsteps * NB * NB) != cudaSuccess ||
       cudaMalloc(&Ui, sizeof(z64) * nsteps * NB * NB) != cudaSuccess ||
-      cudaMalloc(&ip, sizeof(int) * n) != cudaSuccess || cudaMalloc(&inf, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&ip, sizeof(int) * n) != cudaSuccess || cudaMalloc(&inf, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&rm, sizeof(int) * RMAP_STRIDE) != cudaSuccess) {
     rc = ADGA_ENOMEM;
   } else {
-    LUBatch lb{n, 2 * n, 1, NB, strideM, ip, inf, Li, Ui};
+    LUBatch lb{n, 2 * n, 1, NB, strideM, ip, inf, Li, Ui, rm};
     int info = 0;
     cudaError_t e = cudaMemcpyAsync(T, aug.data(), sizeof(z64) * strideM, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(inf, 0, sizeof(int), st);
@@ -841,7 +843,7 @@ extern "C" int adga_inverse_matrix_z(adga_z *M, int n, int *ierr, char *erstr) {
     }
     if (rc == 0 && info) rc = info;
   }
-  cudaFree(T); cudaFree(Li); cudaFree(Ui); cudaFree(ip); cudaFree(inf);
+  cudaFree(T); cudaFree(Li); cudaFree(Ui); cudaFree(ip); cudaFree(inf); cudaFree(rm);
   cudaStreamDestroy(st);
   return rc;
 }

@@ -217,14 +217,42 @@ k_panel(T *M, size_t strideM, int N, int J, int jb, int *ipiv_all, int *info_all
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256)
-k_triinv(const T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Linv, T *Uinv) {
+k_triinv(const T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Linv, T *Uinv,
+         const int *ipiv_all, int *rmap_all) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T *D = reinterpret_cast<T *>(smraw);
   T *tmp = D + NB * NB;
   __shared__ T s_d;
+  __shared__ int keys[2 * MAXNB], content[2 * MAXNB];
   const int b = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
   const T *A = M + (size_t)b * strideM;
   const int n = jb;
+  if (t == 0) {
+    // compose the step's interchanges (row J+i <-> ipiv[J+i], in order) into
+    // one map over the rows they touch
+    const int *ip = ipiv_all + (size_t)b * N + J;
+    int nk = jb;
+    for (int i = 0; i < jb; ++i) { keys[i] = J + i; content[i] = J + i; }
+    for (int i = 0; i < jb; ++i) {
+      const int p = ip[i];
+      if (p == J + i) continue;
+      int k;
+      if (p < J + jb) {
+        k = p - J;
+      } else {
+        k = -1;
+        for (int q = jb; q < nk; ++q)
+          if (keys[q] == p) { k = q; break; }
+        if (k < 0) { k = nk++; keys[k] = p; content[k] = p; }
+      }
+      const int x = content[i]; content[i] = content[k]; content[k] = x;
+    }
+    int *rm = rmap_all + (size_t)b * RMAP_STRIDE;
+    int cnt = 0;
+    for (int k = 0; k < nk; ++k)
+      if (content[k] != keys[k]) { rm[1 + 2 * cnt] = keys[k]; rm[2 + 2 * cnt] = content[k]; ++cnt; }
+    rm[0] = cnt;
+  }
   for (int e = t; e < n * n; e += nt) {
     int i = e % n, j = e / n;
     D[i + j * NB] = A[(size_t)(J + i) + (size_t)(J + j) * N];
@@ -274,11 +302,12 @@ k_triinv(const T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps,
-            const int *ipiv_all, const T *Linv, int nleft_tiles) {
+            const int *rmap_all, const T *Linv, int nleft_tiles) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T *Ls = reinterpret_cast<T *>(smraw);
-  T *Xs = Ls + NB * NB;
-  __shared__ int s_ip[MAXNB];
+  T *Xs = Ls + NB * NB;          // [TW][NB]; first reused as the gather buffer [TW][2*NB]
+  __shared__ int s_map[2 * 2 * MAXNB];
+  __shared__ int s_cnt;
   const int tile = blockIdx.x, b = blockIdx.y, t = threadIdx.x, nt = blockDim.x;
   T *A = M + (size_t)b * strideM;
   const bool right = tile >= nleft_tiles;
@@ -286,18 +315,24 @@ k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int n
   if (!right) { cs = tile * TW; ce = min(J, cs + TW); }
   else { cs = J + jb + (tile - nleft_tiles) * TW; ce = min(ncols, cs + TW); }
   const int nc = ce - cs;
-  for (int i = t; i < jb; i += nt) s_ip[i] = ipiv_all[(size_t)b * N + J + i];
+  const int *rm = rmap_all + (size_t)b * RMAP_STRIDE;
+  if (t == 0) s_cnt = rm[0];
+  for (int i = t; i < 2 * rm[0]; i += nt) s_map[i] = rm[1 + i];
   if (right) {
     const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
     for (int e = t; e < NB * jb; e += nt) Ls[e] = L[e];
   }
   __syncthreads();
-  if (t < nc) {
-    T *Ac = A + (size_t)(cs + t) * N;
-    for (int i = 0; i < jb; ++i) {
-      const int pr = s_ip[i], r = J + i;
-      if (pr != r) { T x = Ac[r]; Ac[r] = Ac[pr]; Ac[pr] = x; }
-    }
+  // row interchanges as one gather (all loads) then one scatter (all stores)
+  const int cnt = s_cnt;
+  for (int e = t; e < cnt * nc; e += nt) {
+    const int k = e % cnt, c = e / cnt;
+    Xs[c * 2 * NB + k] = A[(size_t)s_map[2 * k + 1] + (size_t)(cs + c) * N];
+  }
+  __syncthreads();
+  for (int e = t; e < cnt * nc; e += nt) {
+    const int k = e % cnt, c = e / cnt;
+    A[(size_t)s_map[2 * k] + (size_t)(cs + c) * N] = Xs[c * 2 * NB + k];
   }
   if (!right) return;
   __syncthreads();
@@ -510,7 +545,7 @@ k_trisolve_smem(const T *M, size_t strideM, int N, int NB, int nsteps, const T *
 #pragma unroll
       for (int r = 0; r < RMAX; ++r) acc[r] = czero<T>();
       const T *col = A + i + (size_t)J * N;
-#pragma unroll 4
+#pragma unroll 8
       for (int k = 0; k < jb; ++k) {
         const T u = col[(size_t)k * N];
 #pragma unroll
@@ -536,9 +571,12 @@ template <typename T>
 static cudaError_t launch_panel(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
   const int rows = lb.N - J;
   auto nthreads = [&](int rpt) { int n = ((rows + rpt - 1) / rpt + 31) / 32 * 32; return n < 32 ? 32 : n; };
-  if (rows <= 1024) {
+  // fewer, fuller threads per CTA: more matrices resident per SM and cheaper
+  // block-wide pivot reductions (FP32 rows cost half the registers of FP64)
+  const bool f32 = sizeof(T) == sizeof(z32);
+  if (rows <= (f32 ? 0 : 640)) {
     k_panel<T, 1><<<lb.batch, nthreads(1), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
-  } else if (rows <= 1280) {
+  } else if (rows <= (f32 ? 0 : 1280)) {
     k_panel<T, 2><<<lb.batch, nthreads(2), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
   } else if (rows <= 2048) {
     k_panel<T, 4><<<lb.batch, nthreads(4), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
@@ -550,8 +588,11 @@ static cudaError_t launch_panel(T *M, const LUBatch &lb, int J, int jb, cudaStre
   return ADGA_LAUNCH_CHECK();
 }
 
+cudaError_t lu_trail_z64(z64 *M, const LUBatch &lb, int J, int jb, cudaStream_t st);
+
 template <typename T>
 cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
+  if constexpr (sizeof(T) == sizeof(z64)) return lu_trail_z64((z64 *)M, lb, J, jb, st);
   const int m = lb.N - J - jb, n = lb.ncols - J - jb;
   if (m <= 0 || n <= 0) return cudaSuccess;
   dim3 grid(cdiv_u(n, 64), cdiv_u(m, 64), lb.batch);
@@ -566,7 +607,7 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
   const int nsteps = lb.nsteps();
   cudaError_t e;
   const size_t sm_tri = sizeof(T) * ((size_t)lb.NB * lb.NB + lb.NB);
-  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * lb.NB + (size_t)lb.NB * TW);
+  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * lb.NB + (size_t)2 * lb.NB * TW);
   static bool attr_done[2] = {false, false};
   const int ti = sizeof(T) == sizeof(z64) ? 0 : 1;
   if (!attr_done[ti]) {
@@ -578,14 +619,14 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
     const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
     if ((e = launch_panel<T>(M, lb, J, jb, st)) != cudaSuccess) return e;
     k_triinv<T><<<lb.batch, 256, sm_tri, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps,
-                                               (T *)lb.Linv, (T *)lb.Uinv);
+                                               (T *)lb.Linv, (T *)lb.Uinv, lb.ipiv, lb.rmap);
     if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
     const int nleft = apply_left ? (J + TW - 1) / TW : 0;
     const int nright = (lb.ncols - J - jb + TW - 1) / TW;
     if (nleft + nright > 0) {
       dim3 g(nleft + nright, lb.batch);
       k_swap_trsm<T><<<g, 256, sm_trsm, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps,
-                                              lb.ipiv, (const T *)lb.Linv, nleft);
+                                              lb.rmap, (const T *)lb.Linv, nleft);
       if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
     }
     if (J + jb < lb.N) {
@@ -608,8 +649,9 @@ static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC,
   // few right-hand sides that fit in shared memory: the resident-RHS kernel
   const size_t sm_small = sizeof(T) * ((size_t)lb.N * R + (size_t)lb.NB * R) + sizeof(int) * lb.N;
   if (R <= 25 && sm_small <= 200 * 1024) {
-    static bool attr_small[8] = {false};
-    const int ti = (sizeof(T) == sizeof(z64) ? 0 : 1) * 4 + (upper ? 2 : 0) + (R <= 16 ? 0 : 1);
+    static bool attr_small[16] = {false};
+    const int ti = (sizeof(T) == sizeof(z64) ? 0 : 1) * 8 + (upper ? 4 : 0) +
+                   (R == 9 ? 0 : R <= 4 ? 1 : R <= 16 ? 2 : 3);
     const int np = lb.nsteps();
 #define TS_LAUNCH(UP, RM)                                                                            \
     do {                                                                                             \
@@ -623,9 +665,11 @@ static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC,
           lb.ipiv);                                                                                  \
     } while (0)
     if (upper) {
-      if (R <= 16) TS_LAUNCH(true, 16); else TS_LAUNCH(true, 25);
+      if (R == 9) TS_LAUNCH(true, 9); else if (R <= 4) TS_LAUNCH(true, 4);
+      else if (R <= 16) TS_LAUNCH(true, 16); else TS_LAUNCH(true, 25);
     } else {
-      if (R <= 16) TS_LAUNCH(false, 16); else TS_LAUNCH(false, 25);
+      if (R == 9) TS_LAUNCH(false, 9); else if (R <= 4) TS_LAUNCH(false, 4);
+      else if (R <= 16) TS_LAUNCH(false, 16); else TS_LAUNCH(false, 25);
     }
 #undef TS_LAUNCH
     return ADGA_LAUNCH_CHECK();

@@ -14,6 +14,10 @@
 // memory as X stored R x N row-major.
 #include "ctx.cuh"
 
+cudaError_t launch_resid_z64(const DevCtx &c, int npts, const z64 *XD, const z64 *X,
+                             const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
+                             const z64 *opg_m, z32 *V, cudaStream_t st);
+
 // X64 = up(Y32) from the RHS columns of the FP32 factorised matrices
 __global__ void k_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X) {
   size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -152,11 +156,7 @@ cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *
   k_xd<<<cdiv_u(total, 256), 256, 0, st>>>(c, npts, X, chi0q, c0inv, XD);
   cudaError_t e = ADGA_LAUNCH_CHECK();
   if (e != cudaSuccess) return e;
-  dim3 g(cdiv_u(c.N, 64), cdiv_u((size_t)npts * c.R, 64));
-  k_resid<<<g, 256, 0, st>>>(c.N, c.R, npts, 0, XD, X, Frow_d, opg_d, V);
-  if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-  k_resid<<<g, 256, 0, st>>>(c.N, c.R, npts, 1, XD, X, Frow_m, opg_m, V);
-  return ADGA_LAUNCH_CHECK();
+  return launch_resid_z64(c, npts, XD, X, Frow_d, Frow_m, opg_d, opg_m, V, st);
 }
 
 cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,

@@ -119,7 +119,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(192, 2)
 k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int Ncols, int Ncap, int nkb,
             int *err) {
@@ -192,23 +192,21 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
       const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16);
       const bool rowok = m < Mrows;
 #pragma unroll 1
-      for (int c = 0; c < BN; c += 32) {
-        // all loads of the chunk are issued before any store, so the 32
+      for (int c = 0; c < BN; c += 16) {
+        // all loads of the chunk are issued before any store, so the 16
         // read-modify-writes of this thread overlap in the memory system
-        z32 cv[32];
+        z32 cv[16];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < 16; ++j) {
           const int n = n0 + c + j;
           cv[j] = (rowok && n < Ncols) ? Cb[(size_t)(J + jb + n) * N] : make_float2(0.f, 0.f);
         }
-        float re[32], im[32];
-        tmem_ld16(tl + c, *reinterpret_cast<float(*)[16]>(re));
-        tmem_ld16(tl + c + 16, *reinterpret_cast<float(*)[16]>(re + 16));
-        tmem_ld16(tl + BN + c, *reinterpret_cast<float(*)[16]>(im));
-        tmem_ld16(tl + BN + c + 16, *reinterpret_cast<float(*)[16]>(im + 16));
+        float re[16], im[16];
+        tmem_ld16(tl + c, re);
+        tmem_ld16(tl + BN + c, im);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < 16; ++j) {
           const int n = n0 + c + j;
           if (rowok && n < Ncols) {
             z32 v = cv[j];

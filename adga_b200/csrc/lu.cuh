@@ -16,11 +16,16 @@
 #pragma once
 #include "common.cuh"
 
+// Row-interchange map of one step, per matrix: [count, dst0, src0, dst1, src1, ...]
+// (after the step's interchanges row dst holds what row src held before).
+constexpr int RMAP_STRIDE = 520;   // >= 1 + 2 * (2 * 128) entries
+
 struct LUBatch {
   int N, ncols, batch, NB;
   size_t strideM;
   int *ipiv, *info;
   void *Linv, *Uinv;        // [batch][nsteps][NB*NB] of the element type
+  int *rmap;                // [batch][RMAP_STRIDE]
   int nsteps() const { return (N + NB - 1) / NB; }
 };
 

@@ -37,7 +37,8 @@ constexpr size_t NA_OFF_LINV = NA_T_BYTES;
 constexpr size_t NA_OFF_UINV = NA_OFF_LINV + NA_BLK_BYTES;
 constexpr size_t NA_OFF_PIV = NA_OFF_UINV + NA_BLK_BYTES;
 constexpr size_t NA_OFF_INFO = NA_OFF_PIV + NA_PIV_BYTES;
-constexpr size_t NOALLOC_SCRATCH_BYTES = NA_OFF_INFO + 256;
+constexpr size_t NA_OFF_RMAP = NA_OFF_INFO + 256;
+constexpr size_t NOALLOC_SCRATCH_BYTES = NA_OFF_RMAP + 256 * ((sizeof(int) * RMAP_STRIDE + 255) / 256);
 static_assert(NA_OFF_LINV % 256 == 0 && NA_OFF_PIV % 256 == 0 && NA_OFF_INFO % 256 == 0,
               "scratch regions must stay 256-byte aligned");
 
@@ -85,7 +86,8 @@ extern "C" int adga_inverse_matrix_z_noalloc(const adga_z *M_dev, adga_z *Minv_d
   int *ipiv = (int *)(sb + NA_OFF_PIV);
   int *info = (int *)(sb + NA_OFF_INFO);
   const size_t strideM = (size_t)n * 2 * n;
-  LUBatch lb{n, 2 * n, 1, NA_NB, strideM, ipiv, info, sb + NA_OFF_LINV, sb + NA_OFF_UINV};
+  LUBatch lb{n, 2 * n, 1, NA_NB, strideM, ipiv, info, sb + NA_OFF_LINV, sb + NA_OFF_UINV,
+             (int *)(sb + NA_OFF_RMAP)};
   cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), st);
   if (e == cudaSuccess) {
     k_noalloc_fill<<<cdiv_u(strideM, 256) < 1024 ? cdiv_u(strideM, 256) : 1024, 256, 0, st>>>(
