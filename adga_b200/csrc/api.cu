@@ -16,6 +16,14 @@
 // tensor-core trailing update of the mixed path (k_tc.cu)
 cudaError_t tc_trail_setup(void **ctx, z32 *M, const LUBatch &lb, cudaStream_t st);
 cudaError_t tc_trail_run(void *ctx, int J, int jb, cudaStream_t st);
+cudaError_t tc_trail_run_range(void *ctx, int first, int count, int J, int jb, cudaStream_t st);
+
+// a matrix range of the tensor-core trailing-update context
+struct TcRange { void *ctx; int first, count; };
+static cudaError_t tc_trail_range_fn(void *r, int J, int jb, cudaStream_t st) {
+  TcRange *x = (TcRange *)r;
+  return tc_trail_run_range(x->ctx, x->first, x->count, J, jb, st);
+}
 void tc_trail_free(void *ctx);
 int tc_available();
 int tc_trail_error(void *ctx);
@@ -25,8 +33,8 @@ struct adga_handle {
   DevCtx c{};
   int nw = 0, nnu_all = 0, nd4 = 0;
   bool bigbox = false;
-  cudaStream_t st = nullptr;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaStream_t st = nullptr, st2 = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, fork = nullptr, join = nullptr;
   std::string err;
   std::vector<void *> owned;
   // vertex store, one pair per omega
@@ -141,6 +149,9 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   }
   cudaEventCreate(&h->e0);
   cudaEventCreate(&h->e1);
+  cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
+  if (cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking) != cudaSuccess) h->st2 = nullptr;
   auto &L = h->owned;
   const int nd = c.nd, nd2 = c.nd2, n2w = 2 * c.iwmax;
   double *iw; z64 *hk_d, *siw_d, *giw_d, *dc_d, *u_d, *ut_d, *nd_d, *gt;
@@ -208,6 +219,9 @@ extern "C" int adga_destroy(adga_handle *h) {
   if (h->qidx_h) cudaFreeHost(h->qidx_h);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
+  if (h->fork) cudaEventDestroy(h->fork);
+  if (h->join) cudaEventDestroy(h->join);
+  if (h->st2) { cudaStreamSynchronize(h->st2); cudaStreamDestroy(h->st2); }
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
   return 0;
@@ -355,6 +369,39 @@ static void stage_ms(adga_handle *h, double *acc, cudaEvent_t a, cudaEvent_t b) 
   if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) *acc += ms;
 }
 
+// LU of the whole batch.  Optionally (ADGA_TWO_STREAMS) the batch is split in
+// halves whose steps are issued alternately on two streams, so that the
+// latency-bound phases of one half (panel, block inverses, interchanges) can
+// overlap the trailing updates of the other.  Timing events bracket the
+// (first half's) trailing updates.
+template <typename T>
+static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool apply_left, bool tc,
+                                TrailTiming *tt) {
+  cudaStream_t st = h->st;
+  // measured: the trailing-update grids fill every SM, so the split gives no
+  // overlap on the t2g workload; kept as an option (ADGA_TWO_STREAMS=1)
+  const bool split = h->st2 && lb.batch >= 8 && getenv("ADGA_TWO_STREAMS");
+  if (!split) {
+    TcRange r{h->tc, 0, lb.batch};
+    return lu_factor<T>(M, lb, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &r : nullptr, st, tt);
+  }
+  const int na = lb.batch / 2, nb = lb.batch - na;
+  LUBatch la = lu_sub<T>(lb, 0, na), lbb = lu_sub<T>(lb, na, nb);
+  T *Mb = M + (size_t)na * lb.strideM;
+  TcRange ra{h->tc, 0, na}, rb{h->tc, na, nb};
+  cudaError_t e = cudaEventRecord(h->fork, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h->st2, h->fork, 0);
+  for (int s = 0; e == cudaSuccess && s < lb.nsteps(); ++s) {
+    e = lu_step<T>(M, la, s, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &ra : nullptr, st, tt);
+    if (e == cudaSuccess)
+      e = lu_step<T>(Mb, lbb, s, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &rb : nullptr, h->st2,
+                     nullptr);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(h->join, h->st2);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->join, 0);
+  return e;
+}
+
 // one batch of np consecutive q at omega = iwb: chi0 -> build -> LU/solve -> post -> EOM.
 // qidx_h[0..np) hold the 0-based q indices; outputs go to point slot `off`.
 static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *status,
@@ -390,7 +437,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     CK(launch_bse_build<z64>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
                              strideM, h->gq, st));
     cudaEventRecord(ev[2], st);
-    CK(lu_factor<z64>(T, lb, false, nullptr, nullptr, st, &tt));
+    CK(factor_batch<z64>(h, T, lb, false, false, &tt));
     CK(lu_backsolve<z64>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     X = T + N * N; sp = 2 * strideM; sc = strideM;
   } else {
@@ -398,11 +445,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     CK(launch_bse_build<z32>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
                              strideM, h->gq, st));
     cudaEventRecord(ev[2], st);
-    if (h->tc) {
-      CK(lu_factor<z32>(T, lb, true, tc_trail_run, h->tc, st, &tt));
-    } else {
-      CK(lu_factor<z32>(T, lb, true, nullptr, nullptr, st, &tt));
-    }
+    CK(factor_batch<z32>(h, T, lb, true, h->tc != nullptr, &tt));
     CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     CK(launch_init_x(T, strideM, (int)N, (int)R, 2 * np, h->X64, st));
     const int nmat = 2 * np;

@@ -2,94 +2,77 @@
 // for a batch of q points at one omega -- the k-loop of src/main.F90:646-657
 // over accumulate_chi0 (src/one_particle_quant_module.f90:228-290).
 //
-// One thread block per (nu, point).  Warp w owns the rows i1 = i*nd + j of
-// one i (and, for nd > 3, one j); its lanes stride over k, gathering
-// G(k, nu) and G(k-q, nu-omega) from the resident G table with 16-byte
-// loads, and the partial sums are reduced with warp shuffles.  The kernel
-// is bound by the FP64 pipe (81 complex MACs per 288 gathered bytes at
-// nd = 3), the table slices it reads stay in L2 across the batch.
+// The kernel is bound by the FP64 pipe (nd2 complex MACs per gathered
+// 16-byte G(k-q) value); the G-table slices it reads stay in L2 across the
+// batch.
 #include "ctx.cuh"
 
-template <int ND>
-__global__ void __launch_bounds__(32 * ND * (ND <= 3 ? 1 : ND))
-k_chi0(DevCtx c, int iwb, const int *__restrict__ qidx, z64 *__restrict__ out, int nnu_all) {
-  constexpr int ND2 = ND * ND;
-  constexpr int JB = (ND <= 3) ? ND : 1;      // j values per warp
-  const int inu = blockIdx.x;                 // 0..nnu_all-1, nu = iwstart + inu
-  const int p = blockIdx.y;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = warp / (ND / JB);
-  const int j0 = (warp % (ND / JB)) * JB;
+// Thread (q, b) of a CTA owns one column b = (k', j) of G(k-q, nu-omega) and
+// one point q, and accumulates the nd2 products with every entry a = (i, l)
+// of G(k, nu) over k.  G(k, nu) is staged in shared memory in chunks of KC
+// k-points and read as broadcasts; the k-q indices of the CTA's points are
+// staged beside it.  Each gathered G(k-q) value feeds nd2 complex FMAs.
+template <int ND, int QG>
+__global__ void __launch_bounds__(QG * ND * ND)
+k_chi0(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, z64 *__restrict__ out, int nnu_all) {
+  constexpr int ND2 = ND * ND, KC = 64, NTH = QG * ND2;
+  __shared__ z64 g1s[KC][ND2];
+  __shared__ int kqs[KC][QG];
+  const int inu = blockIdx.x, p0 = blockIdx.y * QG;
+  const int t = threadIdx.x, ql = t / ND2, bcol = t % ND2;
+  const int p = p0 + ql;
+  const bool act = p < npts;
   const int nu = c.iwstart + inu;
-  const int q = qidx[p];
   const z64 *g1t = c.gtab + (size_t)(nu - c.nu_lo) * c.nkp * ND2;
   const z64 *g2t = c.gtab + (size_t)(nu - iwb - c.nu_lo) * c.nkp * ND2;
-  const int *kq = c.kq + (size_t)q * c.nkp;
-
-  z64 acc[JB][ND2];
+  z64 acc[ND2];
 #pragma unroll
-  for (int a = 0; a < JB; ++a)
-#pragma unroll
-    for (int b = 0; b < ND2; ++b) acc[a][b] = make_double2(0.0, 0.0);
-
-  for (int k = lane; k < c.nkp; k += 32) {
-    const z64 *g1 = g1t + (size_t)k * ND2;
-    const z64 *g2 = g2t + (size_t)__ldg(kq + k) * ND2;
-    z64 a1[ND];
-#pragma unroll
-    for (int l = 0; l < ND; ++l) a1[l] = __ldg(g1 + i + l * ND);      // G_il(k)
-    z64 b2[ND][JB];
-#pragma unroll
-    for (int kk = 0; kk < ND; ++kk)
-#pragma unroll
-      for (int jj = 0; jj < JB; ++jj) b2[kk][jj] = __ldg(g2 + kk + (j0 + jj) * ND);  // G_kj(k-q)
-#pragma unroll
-    for (int jj = 0; jj < JB; ++jj)
-#pragma unroll
-      for (int l = 0; l < ND; ++l)
-#pragma unroll
-        for (int kk = 0; kk < ND; ++kk) cfma(acc[jj][l * ND + kk], a1[l], b2[kk][jj]);
-  }
-  // warp reduction
-#pragma unroll
-  for (int jj = 0; jj < JB; ++jj)
-#pragma unroll
-    for (int b = 0; b < ND2; ++b) {
-      double x = acc[jj][b].x, y = acc[jj][b].y;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        x += __shfl_xor_sync(0xffffffffu, x, o);
-        y += __shfl_xor_sync(0xffffffffu, y, o);
-      }
-      acc[jj][b] = make_double2(x, y);
+  for (int a = 0; a < ND2; ++a) acc[a] = make_double2(0.0, 0.0);
+  for (int k0 = 0; k0 < c.nkp; k0 += KC) {
+    const int kc = min(KC, c.nkp - k0);
+    __syncthreads();
+    for (int e = t; e < kc * ND2; e += NTH) g1s[e / ND2][e % ND2] = __ldg(g1t + (size_t)k0 * ND2 + e);
+    for (int e = t; e < kc * QG; e += NTH) {
+      const int q_l = e / kc, kk = e % kc, pp = p0 + q_l;
+      kqs[kk][q_l] = pp < npts ? __ldg(c.kq + (k0 + kk) + (size_t)qidx[pp] * c.nkp) : 0;
     }
-  // lanes share the stores: output (i1, i2) at i1 + i2*nd2 of block (p, inu)
+    __syncthreads();
+    if (act) {
+#pragma unroll 4
+      for (int kk = 0; kk < kc; ++kk) {
+        const z64 g2 = __ldg(g2t + (size_t)kqs[kk][ql] * ND2 + bcol);
+#pragma unroll
+        for (int a = 0; a < ND2; ++a) cfma(acc[a], g1s[kk][a], g2);
+      }
+    }
+  }
+  if (!act) return;
+  // a = i + l*nd (G_il(k)), bcol = k' + j*nd (G_k'j(k-q)): chi0({i,j},{l,k'})
   z64 *o = out + ((size_t)p * nnu_all + inu) * ND2 * ND2;
   const double f = -c.beta / (double)c.nkp;
+  const int kp = bcol % ND, j = bcol / ND;
 #pragma unroll
-  for (int jj = 0; jj < JB; ++jj)
-#pragma unroll
-    for (int b = 0; b < ND2; ++b) {
-      if ((jj * ND2 + b) % 32 == lane) {
-        int i1 = i * ND + j0 + jj;
-        // -beta * sum / nkp; b = l*nd + k is already the column index {l,k}
-        o[i1 + b * ND2] = make_double2(acc[jj][b].x * f, acc[jj][b].y * f);
-      }
-    }
+  for (int a = 0; a < ND2; ++a) {
+    const int i = a % ND, l = a / ND;
+    o[(i * ND + j) + (l * ND + kp) * ND2] = make_double2(acc[a].x * f, acc[a].y * f);
+  }
 }
 
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,
                         int nnu_all, cudaStream_t st) {
   if (npts <= 0) return cudaSuccess;
-  dim3 grid(nnu_all, npts);
+#define CHI0(NDD, QGG)                                                                      \
+  k_chi0<NDD, QGG><<<dim3(nnu_all, cdiv_u(npts, QGG)), QGG * NDD * NDD, 0, st>>>(c, iwb, qidx, \
+                                                                                npts, chi0_all, nnu_all)
   switch (c.nd) {
-    case 1: k_chi0<1><<<grid, 32, 0, st>>>(c, iwb, qidx, chi0_all, nnu_all); break;
-    case 2: k_chi0<2><<<grid, 64, 0, st>>>(c, iwb, qidx, chi0_all, nnu_all); break;
-    case 3: k_chi0<3><<<grid, 96, 0, st>>>(c, iwb, qidx, chi0_all, nnu_all); break;
-    case 4: k_chi0<4><<<grid, 512, 0, st>>>(c, iwb, qidx, chi0_all, nnu_all); break;
-    case 5: k_chi0<5><<<grid, 800, 0, st>>>(c, iwb, qidx, chi0_all, nnu_all); break;
+    case 1: CHI0(1, 128); break;
+    case 2: CHI0(2, 32); break;
+    case 3: CHI0(3, 16); break;
+    case 4: CHI0(4, 8); break;
+    case 5: CHI0(5, 8); break;
     default: return cudaErrorInvalidValue;
   }
+#undef CHI0
   return ADGA_LAUNCH_CHECK();
 }
 

@@ -299,13 +299,13 @@ k_triinv(const T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T
 // U12 = L11^-1 A12 on the right columns (a jb x jb x TW product).
 // ---------------------------------------------------------------------------
 #define TW 32
+#define SWAP_VMAX 16     // gather items per thread: 2*MAXNB rows x TW columns / 256 threads
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps,
             const int *rmap_all, const T *Linv, int nleft_tiles) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  T *Ls = reinterpret_cast<T *>(smraw);
-  T *Xs = Ls + NB * NB;          // [TW][NB]; first reused as the gather buffer [TW][2*NB]
+  T *Xs = reinterpret_cast<T *>(smraw);          // [TW][NB]
   __shared__ int s_map[2 * 2 * MAXNB];
   __shared__ int s_cnt;
   const int tile = blockIdx.x, b = blockIdx.y, t = threadIdx.x, nt = blockDim.x;
@@ -318,21 +318,26 @@ k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int n
   const int *rm = rmap_all + (size_t)b * RMAP_STRIDE;
   if (t == 0) s_cnt = rm[0];
   for (int i = t; i < 2 * rm[0]; i += nt) s_map[i] = rm[1 + i];
-  if (right) {
-    const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
-    for (int e = t; e < NB * jb; e += nt) Ls[e] = L[e];
+  __syncthreads();
+  // row interchanges: every load of the tile, a barrier, then every store
+  const int cnt = s_cnt, items = cnt * nc;
+  T v[SWAP_VMAX];
+#pragma unroll
+  for (int q = 0; q < SWAP_VMAX; ++q) {
+    const int e = t + q * 256;
+    if (e < items) {
+      const int k = e % cnt, c = e / cnt;
+      v[q] = A[(size_t)s_map[2 * k + 1] + (size_t)(cs + c) * N];
+    }
   }
   __syncthreads();
-  // row interchanges as one gather (all loads) then one scatter (all stores)
-  const int cnt = s_cnt;
-  for (int e = t; e < cnt * nc; e += nt) {
-    const int k = e % cnt, c = e / cnt;
-    Xs[c * 2 * NB + k] = A[(size_t)s_map[2 * k + 1] + (size_t)(cs + c) * N];
-  }
-  __syncthreads();
-  for (int e = t; e < cnt * nc; e += nt) {
-    const int k = e % cnt, c = e / cnt;
-    A[(size_t)s_map[2 * k] + (size_t)(cs + c) * N] = Xs[c * 2 * NB + k];
+#pragma unroll
+  for (int q = 0; q < SWAP_VMAX; ++q) {
+    const int e = t + q * 256;
+    if (e < items) {
+      const int k = e % cnt, c = e / cnt;
+      A[(size_t)s_map[2 * k] + (size_t)(cs + c) * N] = v[q];
+    }
   }
   if (!right) return;
   __syncthreads();
@@ -341,10 +346,12 @@ k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int n
     Xs[k + c * NB] = A[(size_t)(J + k) + (size_t)(cs + c) * N];
   }
   __syncthreads();
+  // U12 = L11^-1 A12 with L11^-1 read through L1 (shared by all column tiles)
+  const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
   for (int e = t; e < jb * nc; e += nt) {
     int i = e % jb, c = e / jb;
     T s = czero<T>();
-    for (int k = 0; k <= i; ++k) cfma(s, Ls[i + k * NB], Xs[k + c * NB]);
+    for (int k = 0; k <= i; ++k) cfma(s, __ldg(L + i + k * NB), Xs[k + c * NB]);
     A[(size_t)(J + i) + (size_t)(cs + c) * N] = s;
   }
 }
@@ -496,7 +503,7 @@ k_trisolve(const T *M, size_t strideM, int N, int NB, int nsteps, const T *Dinv,
 // from HBM exactly once with coalesced column accesses.  The forward solve
 // applies the row interchanges P while loading the right-hand sides.
 // ---------------------------------------------------------------------------
-template <typename T, bool UPPER, int RMAX>
+template <typename T, bool UPPER, int RMAX, int RPT>
 __global__ void __launch_bounds__(512)
 k_trisolve_smem(const T *M, size_t strideM, int N, int NB, int nsteps, const T *Dinv, T *C,
                 size_t strideC, int ldc, int R, const int *ipiv_all) {
@@ -531,7 +538,7 @@ k_trisolve_smem(const T *M, size_t strideM, int N, int NB, int nsteps, const T *
       const int i = e % jb, r = e / jb;
       T v = czero<T>();
       const int kb = UPPER ? i : 0, ke = UPPER ? jb : i + 1;
-      for (int k = kb; k < ke; ++k) cfma(v, Di[i + k * NB], Cs[(size_t)r * N + J + k]);
+      for (int k = kb; k < ke; ++k) cfma(v, __ldg(Di + i + k * NB), Cs[(size_t)r * N + J + k]);
       Yt[(size_t)r * NB + i] = v;
     }
     __syncthreads();
@@ -539,22 +546,37 @@ k_trisolve_smem(const T *M, size_t strideM, int N, int NB, int nsteps, const T *
       const int i = e % jb, r = e / jb;
       Cs[(size_t)r * N + J + i] = Yt[(size_t)r * NB + i];
     }
+    // rows still to solve: each thread owns RPT of them, so every Yt value
+    // read from shared memory feeds RPT rows
     const int rb = UPPER ? 0 : J + jb, re = UPPER ? J : N;
-    for (int i = rb + t; i < re; i += nt) {
-      T acc[RMAX];
+    for (int base = rb + t; base < re; base += nt * RPT) {
+      T acc[RPT][RMAX];
 #pragma unroll
-      for (int r = 0; r < RMAX; ++r) acc[r] = czero<T>();
-      const T *col = A + i + (size_t)J * N;
+      for (int q = 0; q < RPT; ++q)
+#pragma unroll
+        for (int r = 0; r < RMAX; ++r) acc[q][r] = czero<T>();
 #pragma unroll 8
       for (int k = 0; k < jb; ++k) {
-        const T u = col[(size_t)k * N];
+        T y[RMAX];
 #pragma unroll
-        for (int r = 0; r < RMAX; ++r)
-          if (r < R) cfma(acc[r], u, Yt[(size_t)r * NB + k]);
+        for (int r = 0; r < RMAX; ++r) y[r] = r < R ? Yt[(size_t)r * NB + k] : czero<T>();
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          const int i = base + q * nt;
+          const T u = i < re ? A[(size_t)i + (size_t)(J + k) * N] : czero<T>();
+#pragma unroll
+          for (int r = 0; r < RMAX; ++r)
+            if (r < R) cfma(acc[q][r], u, y[r]);
+        }
       }
 #pragma unroll
-      for (int r = 0; r < RMAX; ++r)
-        if (r < R) Cs[(size_t)r * N + i] = csub(Cs[(size_t)r * N + i], acc[r]);
+      for (int q = 0; q < RPT; ++q) {
+        const int i = base + q * nt;
+        if (i < re)
+#pragma unroll
+          for (int r = 0; r < RMAX; ++r)
+            if (r < R) Cs[(size_t)r * N + i] = csub(Cs[(size_t)r * N + i], acc[q][r]);
+      }
     }
     __syncthreads();
   }
@@ -574,7 +596,7 @@ static cudaError_t launch_panel(T *M, const LUBatch &lb, int J, int jb, cudaStre
   // fewer, fuller threads per CTA: more matrices resident per SM and cheaper
   // block-wide pivot reductions (FP32 rows cost half the registers of FP64)
   const bool f32 = sizeof(T) == sizeof(z32);
-  if (rows <= (f32 ? 0 : 640)) {
+  if (rows <= (f32 ? 0 : 1024)) {
     k_panel<T, 1><<<lb.batch, nthreads(1), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
   } else if (rows <= (f32 ? 0 : 1280)) {
     k_panel<T, 2><<<lb.batch, nthreads(2), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
@@ -601,13 +623,13 @@ cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t s
 }
 
 template <typename T>
-cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
-                      cudaStream_t st, TrailTiming *tt) {
+cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
+                    cudaStream_t st, TrailTiming *tt) {
   if (lb.NB > MAXNB || lb.NB % SWD) return cudaErrorInvalidValue;
   const int nsteps = lb.nsteps();
   cudaError_t e;
   const size_t sm_tri = sizeof(T) * ((size_t)lb.NB * lb.NB + lb.NB);
-  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * lb.NB + (size_t)2 * lb.NB * TW);
+  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * TW);
   static bool attr_done[2] = {false, false};
   const int ti = sizeof(T) == sizeof(z64) ? 0 : 1;
   if (!attr_done[ti]) {
@@ -615,30 +637,38 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
     cudaFuncSetAttribute(k_swap_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_done[ti] = true;
   }
-  for (int s = 0; s < nsteps; ++s) {
-    const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
-    if ((e = launch_panel<T>(M, lb, J, jb, st)) != cudaSuccess) return e;
-    k_triinv<T><<<lb.batch, 256, sm_tri, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps,
-                                               (T *)lb.Linv, (T *)lb.Uinv, lb.ipiv, lb.rmap);
+  const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
+  if ((e = launch_panel<T>(M, lb, J, jb, st)) != cudaSuccess) return e;
+  k_triinv<T><<<lb.batch, 256, sm_tri, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps,
+                                             (T *)lb.Linv, (T *)lb.Uinv, lb.ipiv, lb.rmap);
+  if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  const int nleft = apply_left ? (J + TW - 1) / TW : 0;
+  const int nright = (lb.ncols - J - jb + TW - 1) / TW;
+  if (nleft + nright > 0) {
+    dim3 g(nleft + nright, lb.batch);
+    k_swap_trsm<T><<<g, 256, sm_trsm, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps,
+                                            lb.rmap, (const T *)lb.Linv, nleft);
     if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-    const int nleft = apply_left ? (J + TW - 1) / TW : 0;
-    const int nright = (lb.ncols - J - jb + TW - 1) / TW;
-    if (nleft + nright > 0) {
-      dim3 g(nleft + nright, lb.batch);
-      k_swap_trsm<T><<<g, 256, sm_trsm, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps,
-                                              lb.rmap, (const T *)lb.Linv, nleft);
-      if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  }
+  if (J + jb < lb.N) {
+    if (tt && tt->ev) cudaEventRecord(tt->ev[2 * tt->n], st);
+    e = trail ? trail(trail_ctx, J, jb, st) : lu_trail_cuda<T>(M, lb, J, jb, st);
+    if (e != cudaSuccess) return e;
+    if (tt && tt->ev) {
+      cudaEventRecord(tt->ev[2 * tt->n + 1], st);
+      tt->gflop += 8.0 * (lb.N - J - jb) * (double)(lb.ncols - J - jb) * jb * lb.batch * 1e-9;
+      tt->n++;
     }
-    if (J + jb < lb.N) {
-      if (tt && tt->ev) cudaEventRecord(tt->ev[2 * tt->n], st);
-      e = trail ? trail(trail_ctx, J, jb, st) : lu_trail_cuda<T>(M, lb, J, jb, st);
-      if (e != cudaSuccess) return e;
-      if (tt && tt->ev) {
-        cudaEventRecord(tt->ev[2 * tt->n + 1], st);
-        tt->gflop += 8.0 * (lb.N - J - jb) * (double)(lb.ncols - J - jb) * jb * lb.batch * 1e-9;
-        tt->n++;
-      }
-    }
+  }
+  return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
+                      cudaStream_t st, TrailTiming *tt) {
+  for (int s = 0; s < lb.nsteps(); ++s) {
+    cudaError_t e = lu_step<T>(M, lb, s, apply_left, trail, trail_ctx, st, tt);
+    if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -656,11 +686,11 @@ static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC,
 #define TS_LAUNCH(UP, RM)                                                                            \
     do {                                                                                             \
       if (!attr_small[ti]) {                                                                         \
-        cudaFuncSetAttribute(k_trisolve_smem<T, UP, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                             200 * 1024);                                                            \
+        cudaFuncSetAttribute(k_trisolve_smem<T, UP, RM, 1>,                                          \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);               \
         attr_small[ti] = true;                                                                       \
       }                                                                                              \
-      k_trisolve_smem<T, UP, RM><<<lb.batch, 512, sm_small, st>>>(                                   \
+      k_trisolve_smem<T, UP, RM, 1><<<lb.batch, 512, sm_small, st>>>(                                \
           M, lb.strideM, lb.N, lb.NB, np, (const T *)(UP ? lb.Uinv : lb.Linv), C, strideC, ldc, R,   \
           lb.ipiv);                                                                                  \
     } while (0)
@@ -710,6 +740,8 @@ cudaError_t lu_fwdsolve_ws(const T *M, const LUBatch &lb, T *V, size_t strideV, 
 }
 
 template cudaError_t lu_factor<z64>(z64 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t, TrailTiming *);
+template cudaError_t lu_step<z64>(z64 *, const LUBatch &, int, bool, trail_fn, void *, cudaStream_t, TrailTiming *);
+template cudaError_t lu_step<z32>(z32 *, const LUBatch &, int, bool, trail_fn, void *, cudaStream_t, TrailTiming *);
 template cudaError_t lu_factor<z32>(z32 *, const LUBatch &, bool, trail_fn, void *, cudaStream_t, TrailTiming *);
 template cudaError_t lu_trail_cuda<z64>(z64 *, const LUBatch &, int, int, cudaStream_t);
 template cudaError_t lu_trail_cuda<z32>(z32 *, const LUBatch &, int, int, cudaStream_t);

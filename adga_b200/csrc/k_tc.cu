@@ -122,7 +122,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 __global__ void __launch_bounds__(192, 2)
 k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int Ncols, int Ncap, int nkb,
-            int *err) {
+            int b0, int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
@@ -131,7 +131,7 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   const uint32_t bar_full = smem_u32(bars), bar_empty = bar_full + 8 * STAGES,
                  bar_acc = bar_full + 16 * STAGES;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM, b = blockIdx.z;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM, b = b0 + blockIdx.z;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -238,9 +238,10 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
 
 // A[b][m][6*NB]: rows m = 0..Mrows-1 are matrix rows J+jb+m, k = 0..NB-1 (zero for k >= jb)
 __global__ void __launch_bounds__(256)
-k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB, __nv_bfloat16 *A) {
+k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB, __nv_bfloat16 *A,
+          int b0) {
   __shared__ z32 tile[64][65];
-  const int b = blockIdx.y, m0 = blockIdx.x * 64;
+  const int b = b0 + blockIdx.y, m0 = blockIdx.x * 64;
   const z32 *L = M + (size_t)b * strideM;
   for (int kc = 0; kc < NB; kc += 64) {
     for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
@@ -272,8 +273,8 @@ k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB,
 // for U rows J..J+jb-1 and columns n = 0..Ncols-1 (matrix columns J+jb+n)
 __global__ void __launch_bounds__(256)
 k_split_b(const z32 *M, size_t strideM, int N, int J, int jb, int Ncols, int Ncap, int NB,
-          __nv_bfloat16 *B) {
-  const int b = blockIdx.y;
+          __nv_bfloat16 *B, int b0) {
+  const int b = b0 + blockIdx.y;
   const z32 *U = M + (size_t)b * strideM;
   const int n = blockIdx.x * (blockDim.x / NB) + threadIdx.x / NB;
   const int k = threadIdx.x % NB;
@@ -365,23 +366,29 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   return cudaSuccess;
 }
 
-cudaError_t tc_trail_run(void *ctxp, int J, int jb, cudaStream_t st) {
+cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, cudaStream_t st) {
   TcCtx *c = (TcCtx *)ctxp;
   const LUBatch &lb = c->lb;
   const int Mrows = lb.N - J - jb, Ncols = lb.ncols - J - jb;
-  if (Mrows <= 0 || Ncols <= 0) return cudaSuccess;
+  if (Mrows <= 0 || Ncols <= 0 || count <= 0) return cudaSuccess;
   const int NB = lb.NB;
-  k_split_a<<<dim3(cdiv_u(Mrows, 64), lb.batch), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Mrows, NB, c->A);
+  k_split_a<<<dim3(cdiv_u(Mrows, 64), count), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Mrows, NB, c->A,
+                                                            first);
   cudaError_t e = ADGA_LAUNCH_CHECK();
   if (e != cudaSuccess) return e;
   const int per = 256 / NB;
-  k_split_b<<<dim3(cdiv_u(Ncols, per), lb.batch), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Ncols,
-                                                                 c->Ncap, NB, c->B);
+  k_split_b<<<dim3(cdiv_u(Ncols, per), count), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Ncols,
+                                                             c->Ncap, NB, c->B, first);
   if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-  dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), lb.batch);
+  dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), count);
   k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA, c->mapB, c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
-                                             c->Ncap, 6 * NB / BK, c->err);
+                                             c->Ncap, 6 * NB / BK, first, c->err);
   return ADGA_LAUNCH_CHECK();
+}
+
+cudaError_t tc_trail_run(void *ctxp, int J, int jb, cudaStream_t st) {
+  TcCtx *c = (TcCtx *)ctxp;
+  return tc_trail_run_range(ctxp, 0, c->lb.batch, J, jb, st);
 }
 
 int tc_trail_error(void *ctxp) {

@@ -43,6 +43,23 @@ struct TrailTiming {
 template <typename T>
 cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
                       cudaStream_t st, TrailTiming *tt = nullptr);
+// one step s (panel, block inverses, interchanges + U12, trailing update)
+template <typename T>
+cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
+                    cudaStream_t st, TrailTiming *tt = nullptr);
+// the matrices [first, first + count) of a batch as a batch of their own
+template <typename T>
+inline LUBatch lu_sub(const LUBatch &lb, int first, int count) {
+  LUBatch r = lb;
+  const size_t blk = (size_t)lb.nsteps() * lb.NB * lb.NB;
+  r.batch = count;
+  r.ipiv = lb.ipiv + (size_t)first * lb.N;
+  r.info = lb.info + first;
+  r.Linv = (T *)lb.Linv + (size_t)first * blk;
+  r.Uinv = (T *)lb.Uinv + (size_t)first * blk;
+  r.rmap = lb.rmap + (size_t)first * RMAP_STRIDE;
+  return r;
+}
 template <typename T>
 cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st);
 // U Y = C in place (C: N x R columns at C + b*strideC, ld ldc)

@@ -100,9 +100,9 @@ typedef struct adga_run_stats {
   double ms_total;             /* device time of the run (CUDA events)         */
   double ms_chi0, ms_bse, ms_lu, ms_post, ms_eom;   /* per-stage device time   */
   long long kernel_launches;   /* kernels this run launched                      */
-  double ms_trail;             /* device time of the LU trailing updates         */
+  double ms_trail;             /* device time of the timed LU trailing updates   */
   double trail_gflop;          /* their algorithmic flops (8 m n k per complex)  */
-  int trail_launches;          /* number of trailing-update launches             */
+  int trail_launches;          /* number of timed trailing-update launches       */
 } adga_run_stats;
 
 /*
