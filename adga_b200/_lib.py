@@ -39,7 +39,8 @@ class RunStats(C.Structure):
                 ("ms_total", C.c_double), ("ms_chi0", C.c_double), ("ms_bse", C.c_double),
                 ("ms_lu", C.c_double), ("ms_post", C.c_double), ("ms_eom", C.c_double),
                 ("kernel_launches", C.c_longlong), ("ms_trail", C.c_double),
-                ("trail_gflop", C.c_double), ("trail_launches", C.c_int)]
+                ("trail_gflop", C.c_double), ("trail_launches", C.c_int),
+                ("trail_gbytes", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -505,6 +505,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   for (int i = 0; i < tt.n; ++i) stage_ms(h, &h->stats.ms_trail, tev[2 * i], tev[2 * i + 1]);
   h->stats.trail_launches += tt.n;
   h->stats.trail_gflop += tt.gflop;
+  h->stats.trail_gbytes += tt.gbytes;
   for (auto &x : tev) cudaEventDestroy(x);
   for (int p = 0; p < np; ++p) {
     int a = info[2 * p], b = info[2 * p + 1];

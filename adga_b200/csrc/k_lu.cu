@@ -305,7 +305,8 @@ __global__ void __launch_bounds__(256)
 k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps,
             const int *rmap_all, const T *Linv, int nleft_tiles) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  T *Xs = reinterpret_cast<T *>(smraw);          // [TW][NB]
+  T *Ls = reinterpret_cast<T *>(smraw);          // [NB][NB]  L11^-1 of this step
+  T *Xs = Ls + NB * NB;                          // [TW][NB]
   __shared__ int s_map[2 * 2 * MAXNB];
   __shared__ int s_cnt;
   const int tile = blockIdx.x, b = blockIdx.y, t = threadIdx.x, nt = blockDim.x;
@@ -318,6 +319,10 @@ k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int n
   const int *rm = rmap_all + (size_t)b * RMAP_STRIDE;
   if (t == 0) s_cnt = rm[0];
   for (int i = t; i < 2 * rm[0]; i += nt) s_map[i] = rm[1 + i];
+  if (right) {
+    const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
+    for (int e = t; e < NB * jb; e += nt) Ls[e] = L[e];
+  }
   __syncthreads();
   // row interchanges: every load of the tile, a barrier, then every store
   const int cnt = s_cnt, items = cnt * nc;
@@ -346,12 +351,11 @@ k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int n
     Xs[k + c * NB] = A[(size_t)(J + k) + (size_t)(cs + c) * N];
   }
   __syncthreads();
-  // U12 = L11^-1 A12 with L11^-1 read through L1 (shared by all column tiles)
-  const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
+  // U12 = L11^-1 A12
   for (int e = t; e < jb * nc; e += nt) {
     int i = e % jb, c = e / jb;
     T s = czero<T>();
-    for (int k = 0; k <= i; ++k) cfma(s, __ldg(L + i + k * NB), Xs[k + c * NB]);
+    for (int k = 0; k <= i; ++k) cfma(s, Ls[i + k * NB], Xs[k + c * NB]);
     A[(size_t)(J + i) + (size_t)(cs + c) * N] = s;
   }
 }
@@ -629,7 +633,7 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
   const int nsteps = lb.nsteps();
   cudaError_t e;
   const size_t sm_tri = sizeof(T) * ((size_t)lb.NB * lb.NB + lb.NB);
-  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * TW);
+  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * lb.NB + (size_t)lb.NB * TW);
   static bool attr_done[2] = {false, false};
   const int ti = sizeof(T) == sizeof(z64) ? 0 : 1;
   if (!attr_done[ti]) {
@@ -656,7 +660,9 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
     if (e != cudaSuccess) return e;
     if (tt && tt->ev) {
       cudaEventRecord(tt->ev[2 * tt->n + 1], st);
-      tt->gflop += 8.0 * (lb.N - J - jb) * (double)(lb.ncols - J - jb) * jb * lb.batch * 1e-9;
+      const double m = lb.N - J - jb, n = lb.ncols - J - jb;
+      tt->gflop += 8.0 * m * n * jb * lb.batch * 1e-9;
+      tt->gbytes += (2.0 * sizeof(T) * m * n + sizeof(T) * (double)jb * (m + n)) * lb.batch * 1e-9;
       tt->n++;
     }
   }

@@ -39,6 +39,7 @@ struct TrailTiming {
   cudaEvent_t *ev = nullptr;   // 2 * nsteps events, created by the caller
   int n = 0;                   // number of pairs recorded
   double gflop = 0.0;          // algorithmic flops of the recorded updates
+  double gbytes = 0.0;         // algorithmic HBM bytes: C read+write, L21 and U12 read once
 };
 template <typename T>
 cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,

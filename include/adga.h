@@ -103,6 +103,7 @@ typedef struct adga_run_stats {
   double ms_trail;             /* device time of the timed LU trailing updates   */
   double trail_gflop;          /* their algorithmic flops (8 m n k per complex)  */
   int trail_launches;          /* number of timed trailing-update launches       */
+  double trail_gbytes;         /* their algorithmic HBM bytes (C r+w, L21, U12)  */
 } adga_run_stats;
 
 /*
