@@ -27,6 +27,8 @@ template <typename T> struct PanelShared {
   int s_p;
   int s_info;
   int s_piv[SWD];
+  int mdst[2 * SWD], msrc[2 * SWD];
+  int mcnt;
   T bufP[SWD], bufC[SWD];
   T Lss[SWD * SWD];
   T Us[SWD * MAXNB];
@@ -117,13 +119,15 @@ __device__ __forceinline__ void panel_column(T (&a)[RPT][SWD], PanelShared<T> &S
 }
 
 template <typename T, int RPT>
-__global__ void __launch_bounds__(PanelThreads<RPT>::v)
+__global__ void __launch_bounds__(PanelThreads<RPT>::v, 1)
 k_panel(T *M, size_t strideM, int N, int J, int jb, int *ipiv_all, int *info_all) {
   const int b = blockIdx.x;
   T *A = M + (size_t)b * strideM;
   int *ipiv = ipiv_all + (size_t)b * N;
   const int nt = blockDim.x, t = threadIdx.x;
   __shared__ PanelShared<T> S;
+  extern __shared__ __align__(16) unsigned char panel_dyn[];
+  T *Gs = reinterpret_cast<T *>(panel_dyn);        // [MAXNB][2*SWD] interchange buffer
   if (t == 0) S.s_info = info_all[b];
   T a[RPT][SWD];
 
@@ -158,17 +162,42 @@ k_panel(T *M, size_t strideM, int N, int J, int jb, int *ipiv_all, int *info_all
           for (int cc = 0; cc < SWD; ++cc) S.Lss[i + cc * SWD] = a[q][cc];
       }
     }
+    if (t == 0) {
+      // compose the sub-panel's interchanges into a (dst <- src) row map
+      int keys[2 * SWD], cont[2 * SWD], nk = sw;
+      for (int i = 0; i < sw; ++i) { keys[i] = c0 + i; cont[i] = c0 + i; }
+      for (int i = 0; i < sw; ++i) {
+        const int p = S.s_piv[i];
+        if (p == c0 + i) continue;
+        int k = -1;
+        if (p < c0 + sw) k = p - c0;
+        else {
+          for (int q = sw; q < nk; ++q)
+            if (keys[q] == p) { k = q; break; }
+          if (k < 0) { k = nk++; keys[k] = p; cont[k] = p; }
+        }
+        const int x = cont[i]; cont[i] = cont[k]; cont[k] = x;
+      }
+      int cnt = 0;
+      for (int k = 0; k < nk; ++k)
+        if (cont[k] != keys[k]) { S.mdst[cnt] = keys[k]; S.msrc[cnt] = cont[k]; ++cnt; }
+      S.mcnt = cnt;
+    }
     __syncthreads();
     if (t < sw) ipiv[c0 + t] = S.s_piv[t];
-    // ---- apply the sub-panel's interchanges to the other panel columns
-    const int nother = jb - sw;
-    for (int u = t; u < nother; u += nt) {
+    // ---- apply the sub-panel's interchanges to the other panel columns:
+    //      every (row, column) load into shared memory, a barrier, every store
+    const int nother = jb - sw, mc = S.mcnt;
+    for (int e = t; e < nother * mc; e += nt) {
+      const int u = e / mc, k = e % mc;
       const int col = (u < s) ? J + u : c0 + sw + (u - s);
-      T *Ac = A + (size_t)col * N;
-      for (int i = 0; i < sw; ++i) {
-        const int pr = S.s_piv[i], r = c0 + i;
-        if (pr != r) { T x = Ac[r]; Ac[r] = Ac[pr]; Ac[pr] = x; }
-      }
+      Gs[u * 2 * SWD + k] = A[(size_t)S.msrc[k] + (size_t)col * N];
+    }
+    __syncthreads();
+    for (int e = t; e < nother * mc; e += nt) {
+      const int u = e / mc, k = e % mc;
+      const int col = (u < s) ? J + u : c0 + sw + (u - s);
+      A[(size_t)S.mdst[k] + (size_t)col * N] = Gs[u * 2 * SWD + k];
     }
     __syncthreads();
     // ---- U rows of the right panel columns: unit-lower solve with Lss
@@ -188,19 +217,29 @@ k_panel(T *M, size_t strideM, int N, int J, int jb, int *ipiv_all, int *info_all
         if (i < sw) { Ac[c0 + i] = x[i]; S.Us[i * MAXNB + u] = x[i]; }
     }
     __syncthreads();
-    // ---- rank-sw update of the rows below, right panel columns
+    // ---- rank-sw update of the rows below, right panel columns, in chunks of
+    //      CW columns whose loads are all issued before their stores (CW
+    //      keeps the chunk beside a[][] inside the register budget)
     if (nright > 0) {
 #pragma unroll
       for (int q = 0; q < RPT; ++q) {
         const int r = J + t + q * nt;
         if (r >= c0 + sw && r < N) {
-          for (int u = 0; u < nright; ++u) {
-            T *ap = A + r + (size_t)(c0 + sw + u) * N;
-            T v = *ap;
+          T *arow = A + r + (size_t)(c0 + sw) * N;
+          constexpr int CW = sizeof(T) == 8 ? 4 : 2;
+          for (int u0 = 0; u0 < nright; u0 += CW) {
+            T v[CW];
 #pragma unroll
-            for (int i = 0; i < SWD; ++i)
-              if (i < sw) cfms(v, a[q][i], S.Us[i * MAXNB + u]);
-            *ap = v;
+            for (int j = 0; j < CW; ++j)
+              if (u0 + j < nright) v[j] = arow[(size_t)(u0 + j) * N];
+#pragma unroll
+            for (int j = 0; j < CW; ++j)
+#pragma unroll
+              for (int i = 0; i < SWD; ++i)
+                if (i < sw) cfms(v[j], a[q][i], S.Us[i * MAXNB + u0 + j]);
+#pragma unroll
+            for (int j = 0; j < CW; ++j)
+              if (u0 + j < nright) arow[(size_t)(u0 + j) * N] = v[j];
           }
         }
       }
@@ -510,11 +549,13 @@ k_trisolve(const T *M, size_t strideM, int N, int NB, int nsteps, const T *Dinv,
 template <typename T, bool UPPER, int RMAX, int RPT>
 __global__ void __launch_bounds__(512)
 k_trisolve_smem(const T *M, size_t strideM, int N, int NB, int nsteps, const T *Dinv, T *C,
-                size_t strideC, int ldc, int R, const int *ipiv_all) {
+                size_t strideC, int ldc, int R, const int *ipiv_all, size_t stage_d) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T *Cs = reinterpret_cast<T *>(smraw);            // [R][N]
   T *Yt = Cs + (size_t)N * R;                        // [R][NB]
   int *perm = reinterpret_cast<int *>(Yt + (size_t)NB * R);
+  // the diagonal-block inverse of the current step, staged when it fits
+  T *Ds = stage_d ? reinterpret_cast<T *>(smraw + stage_d) : nullptr;
   const int b = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
   const T *A = M + (size_t)b * strideM;
   T *Cb = C + (size_t)b * strideC;
@@ -538,12 +579,24 @@ k_trisolve_smem(const T *M, size_t strideM, int N, int NB, int nsteps, const T *
     const int blk = UPPER ? nsteps - 1 - s : s;
     const int J = blk * NB, jb = min(NB, N - J);
     const T *Di = Dinv + ((size_t)b * nsteps + blk) * NB * NB;
+    if (Ds) {
+      for (int e = t; e < NB * jb; e += nt) Ds[e] = Di[e];
+      __syncthreads();
+    }
+    const T *D = Ds ? Ds : Di;
     for (int e = t; e < jb * R; e += nt) {
       const int i = e % jb, r = e / jb;
-      T v = czero<T>();
       const int kb = UPPER ? i : 0, ke = UPPER ? jb : i + 1;
-      for (int k = kb; k < ke; ++k) cfma(v, __ldg(Di + i + k * NB), Cs[(size_t)r * N + J + k]);
-      Yt[(size_t)r * NB + i] = v;
+      T v0 = czero<T>(), v1 = czero<T>(), v2 = czero<T>(), v3 = czero<T>();
+      int k = kb;
+      for (; k + 3 < ke; k += 4) {
+        cfma(v0, D[i + k * NB], Cs[(size_t)r * N + J + k]);
+        cfma(v1, D[i + (k + 1) * NB], Cs[(size_t)r * N + J + k + 1]);
+        cfma(v2, D[i + (k + 2) * NB], Cs[(size_t)r * N + J + k + 2]);
+        cfma(v3, D[i + (k + 3) * NB], Cs[(size_t)r * N + J + k + 3]);
+      }
+      for (; k < ke; ++k) cfma(v0, D[i + k * NB], Cs[(size_t)r * N + J + k]);
+      Yt[(size_t)r * NB + i] = cadd(cadd(v0, v1), cadd(v2, v3));
     }
     __syncthreads();
     for (int e = t; e < jb * R; e += nt) {
@@ -597,17 +650,26 @@ template <typename T>
 static cudaError_t launch_panel(T *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
   const int rows = lb.N - J;
   auto nthreads = [&](int rpt) { int n = ((rows + rpt - 1) / rpt + 31) / 32 * 32; return n < 32 ? 32 : n; };
+  const size_t dyn = sizeof(T) * (size_t)MAXNB * 2 * SWD;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_panel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_panel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_panel<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_panel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    attr = true;
+  }
   // fewer, fuller threads per CTA: more matrices resident per SM and cheaper
   // block-wide pivot reductions (FP32 rows cost half the registers of FP64)
   const bool f32 = sizeof(T) == sizeof(z32);
   if (rows <= (f32 ? 0 : 1024)) {
-    k_panel<T, 1><<<lb.batch, nthreads(1), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+    k_panel<T, 1><<<lb.batch, nthreads(1), dyn, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
   } else if (rows <= (f32 ? 0 : 1280)) {
-    k_panel<T, 2><<<lb.batch, nthreads(2), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+    k_panel<T, 2><<<lb.batch, nthreads(2), dyn, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
   } else if (rows <= 2048) {
-    k_panel<T, 4><<<lb.batch, nthreads(4), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+    k_panel<T, 4><<<lb.batch, nthreads(4), dyn, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
   } else if (rows <= 4096) {
-    k_panel<T, 8><<<lb.batch, nthreads(8), 0, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
+    k_panel<T, 8><<<lb.batch, nthreads(8), dyn, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.info);
   } else {
     return cudaErrorInvalidValue;   // N > 4096 is not supported
   }
@@ -683,7 +745,13 @@ template <typename T>
 static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
                             bool upper, T *work, cudaStream_t st) {
   // few right-hand sides that fit in shared memory: the resident-RHS kernel
-  const size_t sm_small = sizeof(T) * ((size_t)lb.N * R + (size_t)lb.NB * R) + sizeof(int) * lb.N;
+  size_t sm_small = sizeof(T) * ((size_t)lb.N * R + (size_t)lb.NB * R) + sizeof(int) * lb.N;
+  size_t stage_d = 0;
+  const size_t dbytes = sizeof(T) * (size_t)lb.NB * lb.NB;
+  if (sm_small + 16 + dbytes <= 112 * 1024) {       // keep two CTAs per SM
+    stage_d = (sm_small + 15) / 16 * 16;
+    sm_small = stage_d + dbytes;
+  }
   if (R <= 25 && sm_small <= 200 * 1024) {
     static bool attr_small[16] = {false};
     const int ti = (sizeof(T) == sizeof(z64) ? 0 : 1) * 8 + (upper ? 4 : 0) +
@@ -698,7 +766,7 @@ static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC,
       }                                                                                              \
       k_trisolve_smem<T, UP, RM, 1><<<lb.batch, 512, sm_small, st>>>(                                \
           M, lb.strideM, lb.N, lb.NB, np, (const T *)(UP ? lb.Uinv : lb.Linv), C, strideC, ldc, R,   \
-          lb.ipiv);                                                                                  \
+          lb.ipiv, stage_d);                                                                         \
     } while (0)
     if (upper) {
       if (R == 9) TS_LAUNCH(true, 9); else if (R <= 4) TS_LAUNCH(true, 4);

@@ -191,16 +191,21 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
       z32 *Cb = M + (size_t)b * strideM + (size_t)(J + jb + m);
       const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16);
       const bool rowok = m < Mrows;
-#pragma unroll 1
-      for (int c = 0; c < BN; c += 16) {
-        // all loads of the chunk are issued before any store, so the 16
-        // read-modify-writes of this thread overlap in the memory system
-        z32 cv[16];
+      // Each C element is read once and then written by this thread only, so
+      // the loads go through the read-only path and are issued a chunk ahead
+      // of the stores (software pipelining over 16-column chunks).
+      auto ldc = [&](int c, z32 (&cv)[16]) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int n = n0 + c + j;
-          cv[j] = (rowok && n < Ncols) ? Cb[(size_t)(J + jb + n) * N] : make_float2(0.f, 0.f);
+          cv[j] = (rowok && n < Ncols) ? __ldg(Cb + (size_t)(J + jb + n) * N) : make_float2(0.f, 0.f);
         }
+      };
+      z32 cur[16], nxt[16];
+      ldc(0, cur);
+#pragma unroll 1
+      for (int c = 0; c < BN; c += 16) {
+        if (c + 16 < BN) ldc(c + 16, nxt);
         float re[16], im[16];
         tmem_ld16(tl + c, re);
         tmem_ld16(tl + BN + c, im);
@@ -209,12 +214,14 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         for (int j = 0; j < 16; ++j) {
           const int n = n0 + c + j;
           if (rowok && n < Ncols) {
-            z32 v = cv[j];
+            z32 v = cur[j];
             v.x -= re[j];
             v.y -= im[j];
             Cb[(size_t)(J + jb + n) * N] = v;
           }
         }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) cur[j] = nxt[j];
       }
     }
   }
