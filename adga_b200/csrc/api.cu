@@ -56,7 +56,7 @@ struct adga_handle {
   z64 *etad = nullptr, *etam = nullptr;
   int *qidx_d = nullptr, *qidx_h = nullptr;
   void *Tm = nullptr, *Linv = nullptr, *Uinv = nullptr;
-  int *ipiv = nullptr, *info = nullptr, *rmap = nullptr;
+  int *ipiv = nullptr, *info = nullptr, *rmap = nullptr, *perm = nullptr;
   int NB = 64;
   z64 *X64 = nullptr, *XD = nullptr;
   z32 *V32 = nullptr, *work32 = nullptr;
@@ -300,7 +300,7 @@ static size_t bytes_per_point(const adga_handle *h, int prec, int NB) {
     b += 2 * N * (N + R) * 16 + 2 * 2 * nsteps * NB * NB * 16;
   } else {
     b += 2 * N * (N + R) * 8 + 2 * 2 * nsteps * NB * NB * 8;
-    b += 2 * 2 * R * N * 16 + 2 * R * N * 8 + 2 * ((R + 15) / 16) * 16 * N * 8 + 64;
+    b += 2 * 2 * R * N * 16 + 2 * R * N * 8 + 2 * ((R + 15) / 16) * 16 * N * 8 + 2 * N * 4 + 64;
   }
   return b;
 }
@@ -347,6 +347,7 @@ static int ensure_work(adga_handle *h, int prec, int want) {
          alloc_into(h, h->XD, (size_t)2 * cap * R * N, W) &&
          alloc_into(h, h->V32, (size_t)2 * cap * R * N, W) &&
          alloc_into(h, h->work32, (size_t)2 * cap * ((R + 15) / 16) * 16 * N, W) &&
+         alloc_into(h, h->perm, (size_t)2 * cap * N, W) &&
          alloc_into(h, h->norms, (size_t)4 * cap, W);
   }
   if (!ok) {
@@ -448,6 +449,8 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     CK(factor_batch<z32>(h, T, lb, true, h->tc != nullptr, &tt));
     CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     CK(launch_init_x(T, strideM, (int)N, (int)R, 2 * np, h->X64, st));
+    CK(lu_build_perm(lb, h->perm, st));
+    lb.perm = h->perm;
     const int nmat = 2 * np;
     const size_t per = N * R;
     std::vector<unsigned long long> nh(2 * nmat);

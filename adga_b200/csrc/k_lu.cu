@@ -744,6 +744,9 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
 template <typename T>
 static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
                             bool upper, T *work, cudaStream_t st) {
+  // few right-hand sides and NB = 64: the streaming solve (k_trsv.cu)
+  if (trsv_stream_supported<T>(lb, strideC, R, upper, lb.perm, work))
+    return launch_trsv_stream<T>(M, lb, C, strideC, ldc, R, upper, lb.perm, work, st);
   // few right-hand sides that fit in shared memory: the resident-RHS kernel
   size_t sm_small = sizeof(T) * ((size_t)lb.N * R + (size_t)lb.NB * R) + sizeof(int) * lb.N;
   size_t stage_d = 0;

@@ -26,6 +26,7 @@ struct LUBatch {
   int *ipiv, *info;
   void *Linv, *Uinv;        // [batch][nsteps][NB*NB] of the element type
   int *rmap;                // [batch][RMAP_STRIDE]
+  int *perm = nullptr;      // [batch][N] row i of P B = row perm[i] of B (lu_build_perm); optional
   int nsteps() const { return (N + NB - 1) / NB; }
 };
 
@@ -59,6 +60,7 @@ inline LUBatch lu_sub(const LUBatch &lb, int first, int count) {
   r.Linv = (T *)lb.Linv + (size_t)first * blk;
   r.Uinv = (T *)lb.Uinv + (size_t)first * blk;
   r.rmap = lb.rmap + (size_t)first * RMAP_STRIDE;
+  r.perm = lb.perm ? lb.perm + (size_t)first * lb.N : nullptr;
   return r;
 }
 template <typename T>
@@ -73,3 +75,12 @@ cudaError_t lu_backsolve(const T *M, const LUBatch &lb, T *C, size_t strideC, in
 template <typename T>
 cudaError_t lu_fwdsolve_ws(const T *M, const LUBatch &lb, T *V, size_t strideV, int ldv, int R,
                            T *work, cudaStream_t st);
+// the factorization's row permutation, from ipiv, into perm[batch][N]
+cudaError_t lu_build_perm(const LUBatch &lb, int *perm, cudaStream_t st);
+// streaming solves (k_trsv.cu): NB = 64, R <= 25; the forward one needs lb.perm and work
+template <typename T>
+bool trsv_stream_supported(const LUBatch &lb, size_t strideC, int R, bool upper, const int *perm,
+                           const T *work);
+template <typename T>
+cudaError_t launch_trsv_stream(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
+                               bool upper, const int *perm, T *work, cudaStream_t st);

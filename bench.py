@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 arm")
     ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--points", type=int, default=0,
+                    help="q points per step (0 = the whole slice); smaller cases are for profiling")
     return ap.parse_args()
 
 
@@ -184,10 +186,10 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def config(args, spec):
+def config(args, spec, npts=None):
     return {"workload": f"{args.workload}: SrVO3-like t2g, ndim={spec.ndim}, k={spec.nk}, q={spec.nq}, "
                         f"2x{spec.iwf} fermionic x {2 * spec.iwb + 1} bosonic, BSE N={spec.maxdim} complex",
-            "points_per_step": spec.nqp, "step": "one omega slice (all q at one bosonic frequency)",
+            "points_per_step": npts or spec.nqp, "step": "one omega slice (all q at one bosonic frequency)",
             "l2": "inputs larger than L2 (BSE matrices of one slice: ~19 GB FP32 / ~38 GB FP64)",
             "parallelism": f"replicas x{args.gpus} (independent omega slices per GPU)"}
 
@@ -237,6 +239,7 @@ def main():
         return float(t.item())
 
     p = synth.make_problem(args.workload)
+    npts = min(args.points, spec.nqp) if args.points > 0 else spec.nqp
     nw = 2 * spec.iwb + 1
     nsteps = args.warmup + args.steps
     omegas = [(-spec.iwb + (rank * nsteps + s) % nw) for s in range(nsteps)]
@@ -256,7 +259,7 @@ def main():
 
     def slice_range(iwb):
         q0 = (iwb + spec.iwb) * spec.nqp + 1
-        return q0, q0 + spec.nqp - 1
+        return q0, q0 + npts - 1
 
     def timed(prec):
         for s in range(args.warmup):
@@ -272,11 +275,11 @@ def main():
         return allmax(ms), stats, clk.summary()
 
     ms_mixed, st_mixed, clk = timed("mixed")
-    v_mixed = world * spec.nqp * args.steps / (ms_mixed * 1e-3)
+    v_mixed = world * npts * args.steps / (ms_mixed * 1e-3)
     res = {}
     if not args.no_fp64:
         ms64, st64, clk64 = timed("fp64")
-        res["fp64"] = world * spec.nqp * args.steps / (ms64 * 1e-3)
+        res["fp64"] = world * npts * args.steps / (ms64 * 1e-3)
 
     # accuracy: mixed vs FP64 on the same slice, and vs the oracle on sampled points
     iwb_chk = omegas[-1]
@@ -309,14 +312,14 @@ def main():
         h2d = sum(x.nbytes for x in pinned[iwb])
         d2h = sum(v.nbytes for v in out.values())
     e2e_t = allmax(e2e_t)
-    e2e = {"value": world * spec.nqp * args.steps / e2e_t, "unit": UNIT,
+    e2e = {"value": world * npts * args.steps / e2e_t, "unit": UNIT,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     # CPU baseline + oracle check on sampled points (rank 0)
     cpu_line = None
     if cpu is not None:
         rng = np.random.default_rng(1)
-        iqs = [int(x) for x in rng.integers(0, spec.nqp, cpu.n)]
+        iqs = [int(x) for x in rng.integers(0, npts, cpu.n)]
         dt, pts = cpu.step(iqs)
         cpu.close()
         cpu_line = {"value": len(iqs) / dt, "unit": UNIT, "cores": cpu.n, "kind": "port",
@@ -360,7 +363,7 @@ def main():
             "dtype": "mixed: c64 LU (bf16x3 tensor-core updates, f32 accumulate) + c128 refinement; "
                      "chi0/EOM c128",
             "data": "synthetic (seeded SrVO3-like t2g model, chi_loc = (chi0_loc^-1 + Gamma)^-1)",
-            "config": config(args, spec), "fp64_value": res.get("fp64"),
+            "config": config(args, spec, npts), "fp64_value": res.get("fp64"),
             "mixed_over_fp64": (v_mixed / res["fp64"]) if res.get("fp64") else None,
             "accuracy": acc, "stage_ms_per_step": stage,
             "refine": {"max_iters": max(s["max_refine_iters"] for s in st_mixed),
