@@ -15,14 +15,15 @@
 
 // tensor-core trailing update of the mixed path (k_tc.cu)
 cudaError_t tc_trail_setup(void **ctx, z32 *M, const LUBatch &lb, cudaStream_t st);
-cudaError_t tc_trail_run(void *ctx, int J, int jb, cudaStream_t st);
-cudaError_t tc_trail_run_range(void *ctx, int first, int count, int J, int jb, cudaStream_t st);
+cudaError_t tc_trail_run_range(void *ctx, int first, int count, int J, int jb, cudaStream_t st,
+                               cudaEvent_t ev0, cudaEvent_t ev1);
 
 // a matrix range of the tensor-core trailing-update context
 struct TcRange { void *ctx; int first, count; };
-static cudaError_t tc_trail_range_fn(void *r, int J, int jb, cudaStream_t st) {
+static cudaError_t tc_trail_range_fn(void *r, int J, int jb, cudaStream_t st, cudaEvent_t ev0,
+                                     cudaEvent_t ev1) {
   TcRange *x = (TcRange *)r;
-  return tc_trail_run_range(x->ctx, x->first, x->count, J, jb, st);
+  return tc_trail_run_range(x->ctx, x->first, x->count, J, jb, st, ev0, ev1);
 }
 void tc_trail_free(void *ctx);
 int tc_available();

@@ -717,11 +717,17 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
     if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
   }
   if (J + jb < lb.N) {
-    if (tt && tt->ev) cudaEventRecord(tt->ev[2 * tt->n], st);
-    e = trail ? trail(trail_ctx, J, jb, st) : lu_trail_cuda<T>(M, lb, J, jb, st);
+    cudaEvent_t ev0 = (tt && tt->ev) ? tt->ev[2 * tt->n] : nullptr;
+    cudaEvent_t ev1 = (tt && tt->ev) ? tt->ev[2 * tt->n + 1] : nullptr;
+    if (trail) {
+      e = trail(trail_ctx, J, jb, st, ev0, ev1);
+    } else {
+      if (ev0) cudaEventRecord(ev0, st);
+      e = lu_trail_cuda<T>(M, lb, J, jb, st);
+      if (ev1) cudaEventRecord(ev1, st);
+    }
     if (e != cudaSuccess) return e;
     if (tt && tt->ev) {
-      cudaEventRecord(tt->ev[2 * tt->n + 1], st);
       const double m = lb.N - J - jb, n = lb.ncols - J - jb;
       tt->gflop += 8.0 * m * n * jb * lb.batch * 1e-9;
       tt->gbytes += (2.0 * sizeof(T) * m * n + sizeof(T) * (double)jb * (m + n)) * lb.batch * 1e-9;

@@ -11,15 +11,20 @@
 //     A[m]     = [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo]
 //     Bre[n]   = [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo, Ur_hi, -Ui_hi]
 //     Bim[n]   = [Ui_hi,  Ur_hi, Ui_lo,  Ur_lo, Ui_hi,  Ur_hi]
-// (K = 6*NB).  The GEMM kernel: warp 0 issues TMA loads (128B swizzle) into
-// a ring of shared-memory stages, warp 1 allocates TMEM and issues
-// tcgen05.mma (M=128, N=256, K=16) from one thread, warps 2-5 read the
-// accumulator with tcgen05.ld and apply C -= acc with coalesced FP32 stores.
+// (K = 6*NB).  Two GEMM kernels share the operand path (TMA loads with
+// 128B swizzle into a ring of shared-memory stages, tcgen05.mma M=128,
+// N=256, K=16 issued by one thread, FP32 accumulators in TMEM):
+//   k_tc_persist  (used when the C strides are 16-byte multiples) one CTA per
+//                 SM loops over the tiles; C tiles arrive in shared memory by
+//                 TMA during the MMAs and the accumulator is double-buffered,
+//                 so the C read-modify-write overlaps the next tile;
+//   k_tc_update   one CTA per tile, C read and written by the epilogue warps.
 // Every mbarrier wait is bounded; on timeout the kernel records an error and
 // leaves.  Loads use no cluster multicast.
 #include "lu.cuh"
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <algorithm>
 #include <cstdio>
 
 namespace {
@@ -184,7 +189,7 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     // epilogue: warp w reads TMEM lanes 32*(w%4).. (= tile rows)
     const int quad = warp & 3;
     const int row = quad * 32 + lane;
-    ok = mbar_wait(bar_acc, 0, err, 3);
+    ok = __all_sync(0xffffffffu, mbar_wait(bar_acc, 0, err, 3));
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (ok) {
       const int m = m0 + row;
@@ -232,6 +237,191 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
     // thread issued no further work after its last commit
     asm volatile("tcgen05.fence::after_thread_sync;");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent variant: one CTA per SM loops over the (column tile, row tile,
+// matrix) tiles of the launch.  The C tile of each output tile is brought
+// into shared memory by TMA (two 64-column halves) while the MMAs of that
+// tile run, and the accumulator is double-buffered in TMEM (2 x 256
+// columns), so the epilogue of one tile overlaps the loads and MMAs of the
+// next and the C read-modify-write no longer waits on DRAM latency.
+//   warp 0        TMA loads of the A/B k-blocks (ring of P_STAGES)
+//   warp 1        TMEM allocation (512 columns) and tcgen05.mma issue
+//   warp 2        TMA loads of the C halves
+//   warps 4..11   epilogue: group h = 0, 1 owns C half h, warp w reads TMEM
+//                 lanes 32*(w%4)..; C - acc is stored straight to global
+// Every wait is bounded (WAIT_NS); on a timeout a role records an error and
+// stops issuing work.
+// ---------------------------------------------------------------------------
+constexpr int P_STAGES = 2;
+constexpr int P_CH_COLS = 64;                         // columns per C half
+constexpr int P_CH_BYTES = BM * 8 * P_CH_COLS;        // 64 KB of complex FP32
+constexpr int P_TMEM_COLS = 2 * TMEM_COLS;            // two accumulators
+constexpr int P_THREADS = 384;
+constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + 2 * P_CH_BYTES + 1024 + 256;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(P_THREADS, 1)
+k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+             const __grid_constant__ CUtensorMap mapC, z32 *M, size_t strideM, int N, int J, int jb,
+             int Mrows, int Ncols, int Ncap, int nkb, int b0, int count, int *err) {
+  extern __shared__ unsigned char smraw[];
+  const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
+  unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
+  const uint32_t scbase = sbase + P_STAGES * STAGE_BYTES;           // the two C halves
+  const unsigned char *gc = gbase + P_STAGES * STAGE_BYTES;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + P_STAGES * STAGE_BYTES + 2 * P_CH_BYTES);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * P_STAGES + 8);
+  const uint32_t bar_full = smem_u32(bars), bar_empty = bar_full + 8 * P_STAGES;
+  const uint32_t bar_accf = bar_empty + 8 * P_STAGES;   // [2]
+  const uint32_t bar_acce = bar_accf + 16;              // [2]
+  const uint32_t bar_cfull = bar_acce + 16;             // [2]
+  const uint32_t bar_cempty = bar_cfull + 16;           // [2]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntn = (Ncols + BN - 1) / BN, ntm = (Mrows + BM - 1) / BM;
+  const int ntiles = ntn * ntm * count;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P_STAGES; ++s) {
+      mbar_init(bar_full + 8 * s, 1);
+      mbar_init(bar_empty + 8 * s, 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(bar_accf + 8 * a, 1);
+      mbar_init(bar_acce + 8 * a, 8);      // one arrival per epilogue warp
+      mbar_init(bar_cfull + 8 * a, 1);
+      mbar_init(bar_cempty + 8 * a, 4);    // one arrival per warp of the group
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(P_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int kbt = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
+        bool ok = true;
+        for (int kb = 0; kb < nkb; ++kb, ++kbt) {
+          const int s = kbt % P_STAGES;
+          if (kbt >= P_STAGES && !(ok = mbar_wait(bar_empty + 8 * s, ((kbt / P_STAGES) - 1) & 1, err, 11)))
+            break;
+          const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
+          mbar_expect_tx(bar_full + 8 * s, STAGE_BYTES);
+          tma_load_3d(sa, &mapA, bar_full + 8 * s, kb * BK, tm * BM, b);
+          tma_load_3d(sb, &mapB, bar_full + 8 * s, kb * BK, tn * BN, b);
+          tma_load_3d(sb + B_BYTES / 2, &mapB, bar_full + 8 * s, kb * BK, Ncap + tn * BN, b);
+        }
+        if (!ok) break;
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int kbt = 0, it = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int a = it & 1, use = it >> 1;
+        bool ok = true;
+        if (use > 0) ok = mbar_wait(bar_acce + 8 * a, (use - 1) & 1, err, 12);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t dacc = tmem + (uint32_t)(a * TMEM_COLS);
+        for (int kb = 0; kb < nkb; ++kb, ++kbt) {
+          const int s = kbt % P_STAGES;
+          if (!(ok = mbar_wait(bar_full + 8 * s, (kbt / P_STAGES) & 1, err, 13))) break;
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
+#pragma unroll
+          for (int k = 0; k < BK / 16; ++k)
+            mma_bf16(dacc, smem_desc(sa + 32 * k), smem_desc(sb + 32 * k), (kb > 0 || k > 0) ? 1u : 0u);
+          mma_commit(bar_empty + 8 * s);
+        }
+        if (!ok) break;
+        mma_commit(bar_accf + 8 * a);
+      }
+    }
+  } else if (warp == 2) {
+    if (lane == 0) {
+      int it = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
+        bool ok = true;
+        for (int h = 0; h < 2 && ok; ++h) {
+          if (it > 0) ok = mbar_wait(bar_cempty + 8 * h, (it - 1) & 1, err, 14);
+          if (!ok) break;
+          mbar_expect_tx(bar_cfull + 8 * h, P_CH_BYTES);
+          // x counts floats: rows J+jb+m0.. as (re, im) pairs
+          tma_load_3d(scbase + h * P_CH_BYTES, &mapC, bar_cfull + 8 * h, 2 * (J + jb + tm * BM),
+                      J + jb + tn * BN + h * P_CH_COLS, b);
+        }
+        if (!ok) break;
+      }
+    }
+  } else if (warp >= 4) {
+    const int e = warp - 4, h = e >> 2, quad = warp & 3;
+    const int row = quad * 32 + lane;
+    const z32 *cs = reinterpret_cast<const z32 *>(gc + h * P_CH_BYTES);   // [col][128 rows]
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+      const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
+      const int a = it & 1;
+      // every lane waits (and so observes the TMA-written C half); the warp
+      // leaves together if any lane gave up, so tcgen05.ld stays warp-wide
+      bool ok = mbar_wait(bar_accf + 8 * a, (it >> 1) & 1, err, 15);
+      ok = ok && mbar_wait(bar_cfull + 8 * h, it & 1, err, 16);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const int m = tm * BM + row;
+      const bool rowok = m < Mrows;
+      z32 *Cb = M + (size_t)b * strideM + (size_t)(J + jb + m);
+      const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * TMEM_COLS + h * P_CH_COLS);
+      const int nbase = tn * BN + h * P_CH_COLS;
+#pragma unroll 1
+      for (int c = 0; c < P_CH_COLS; c += 16) {
+        float re[16], im[16];
+        tmem_ld16(tl + c, re);
+        tmem_ld16(tl + BN + c, im);
+        z32 cv[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) cv[j] = cs[(c + j) * BM + row];
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = nbase + c + j;
+          if (rowok && n < Ncols) {
+            z32 v = cv[j];
+            v.x -= re[j];
+            v.y -= im[j];
+            Cb[(size_t)(J + jb + n) * N] = v;
+          }
+        }
+      }
+      // this warp is done with the C half and with the accumulator
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(bar_cempty + 8 * h);
+        mbar_arrive(bar_acce + 8 * a);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P_TMEM_COLS));
   }
 }
 
@@ -304,7 +494,9 @@ struct TcCtx {
   __nv_bfloat16 *A = nullptr, *B = nullptr;
   int *err = nullptr;
   int Ncap = 0;
-  CUtensorMap mapA, mapB;
+  int nsm = 0;
+  bool persist = false;        // C tiles by TMA: needs 16-byte column and matrix strides
+  CUtensorMap mapA, mapB, mapC;
 };
 
 typedef CUresult (*encode_fn_t)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -337,6 +529,20 @@ bool make_map(CUtensorMap *map, void *base, uint64_t inner, uint64_t rows, uint6
   return r == CUDA_SUCCESS;
 }
 
+// C as FP32: dims (2N floats per column, columns, matrices), box 128 rows x 64 columns
+bool make_map_c(CUtensorMap *map, void *base, uint64_t N, uint64_t ncols, uint64_t strideM, uint64_t batch) {
+  encode_fn_t enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[3] = {2 * N, ncols, batch};
+  cuuint64_t strides[2] = {N * 8, strideM * 8};
+  cuuint32_t box[3] = {2 * BM, P_CH_COLS, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 int tc_available() {
@@ -364,6 +570,16 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
     e = cudaErrorInvalidValue;
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  // the persistent kernel: C column stride (N * 8 B) and matrix stride on 16 bytes
+  if (e == cudaSuccess && lb.N % 2 == 0 && lb.strideM % 2 == 0 &&
+      make_map_c(&c->mapC, M, lb.N, lb.ncols, lb.strideM, lb.batch) &&
+      cudaFuncSetAttribute(k_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES) ==
+          cudaSuccess) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
+    c->persist = c->nsm > 0;
+  }
   if (e != cudaSuccess) {
     cudaFree(c->A); cudaFree(c->B); cudaFree(c->err);
     delete c;
@@ -373,7 +589,8 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   return cudaSuccess;
 }
 
-cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, cudaStream_t st) {
+cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, cudaStream_t st,
+                               cudaEvent_t ev0, cudaEvent_t ev1) {
   TcCtx *c = (TcCtx *)ctxp;
   const LUBatch &lb = c->lb;
   const int Mrows = lb.N - J - jb, Ncols = lb.ncols - J - jb;
@@ -387,15 +604,21 @@ cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, 
   k_split_b<<<dim3(cdiv_u(Ncols, per), count), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Ncols,
                                                              c->Ncap, NB, c->B, first);
   if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-  dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), count);
-  k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA, c->mapB, c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
-                                             c->Ncap, 6 * NB / BK, first, c->err);
-  return ADGA_LAUNCH_CHECK();
-}
-
-cudaError_t tc_trail_run(void *ctxp, int J, int jb, cudaStream_t st) {
-  TcCtx *c = (TcCtx *)ctxp;
-  return tc_trail_run_range(ctxp, 0, c->lb.batch, J, jb, st);
+  if (ev0) cudaEventRecord(ev0, st);
+  if (c->persist) {
+    const long long ntiles = (long long)cdiv_u(Ncols, BN) * cdiv_u(Mrows, BM) * count;
+    const int grid = (int)std::min<long long>(ntiles, c->nsm);
+    k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapC, c->M, lb.strideM, lb.N, J,
+                                                         jb, Mrows, Ncols, c->Ncap, 6 * NB / BK, first, count,
+                                                         c->err);
+  } else {
+    dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), count);
+    k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA, c->mapB, c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
+                                               c->Ncap, 6 * NB / BK, first, c->err);
+  }
+  e = ADGA_LAUNCH_CHECK();
+  if (ev1) cudaEventRecord(ev1, st);
+  return e;
 }
 
 int tc_trail_error(void *ctxp) {

@@ -31,8 +31,9 @@ struct LUBatch {
 };
 
 // Trailing update C -= A B of one step (rows r0.., cols c0..), pluggable so
-// that the mixed path can route it to the tensor cores.
-typedef cudaError_t (*trail_fn)(void *ctx, int J, int jb, cudaStream_t st);
+// that the mixed path can route it to the tensor cores.  ev0 / ev1 (may be
+// null) are recorded around the GEMM launch itself, operand staging excluded.
+typedef cudaError_t (*trail_fn)(void *ctx, int J, int jb, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
 
 // Optional timing of the trailing updates: events[2*s], events[2*s+1]
 // bracket the update of step s (pass nullptr to skip).

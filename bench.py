@@ -30,8 +30,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "BSE q·ω pts/s at 1e-8 rel err vs FP64 oracle: mixed-prec vs plain FP64 on B200"
-# DRAM bytes / algorithmic bytes of one k_tc_update launch measured with ncu
-# (64-point t2g case, LU step 3, 128 matrices: 1.627 GB over 1.51 GB)
+# DRAM bytes / algorithmic bytes of one k_tc_persist launch measured with ncu
+# (64-point t2g case, LU step 3, 128 matrices); profiles/k_tc_persist_t2g.md
 TRAFFIC_OVER_ALG = 1.08
 UNIT = "qw_points/s"
 WORKLOAD = "c1"
@@ -347,7 +347,7 @@ def main():
     nlaunch = max(sum(s["trail_launches"] for s in st_mixed), 1)
     achieved = gbytes / mst * 1e3 if mst else 0.0          # GB/s
     peak = pk.get("hbm_gbs")
-    roof = {"kernel": "k_tc_update (+ operand split): LU trailing update of the mixed path",
+    roof = {"kernel": "k_tc_persist: tensor-core LU trailing update of the mixed path (GEMM launch only)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if peak else None,
             "traffic": TRAFFIC_OVER_ALG * gbytes * 1e9 / nlaunch,
