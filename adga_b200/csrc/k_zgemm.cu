@@ -10,8 +10,8 @@ using namespace zg;
 
 __global__ void __launch_bounds__(NT)
 k_trail_z64(z64 *M, size_t strideM, int N, int ncols, int J, int jb) {
-  __shared__ __align__(16) z64 As[2 * BK * BM];
-  __shared__ __align__(16) z64 Bs[2 * BK * BN];
+  extern __shared__ __align__(16) z64 zg_smem[];
+  z64 *As = zg_smem, *Bs = zg_smem + STAGES * BK * BM;
   const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
   z64 *A = M + (size_t)blockIdx.z * strideM;
   const int r0 = J + jb + blockIdx.y * BM, c0 = J + jb + blockIdx.x * BN;
@@ -45,8 +45,13 @@ k_trail_z64(z64 *M, size_t strideM, int N, int ncols, int J, int jb) {
 cudaError_t lu_trail_z64(z64 *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
   const int m = lb.N - J - jb, n = lb.ncols - J - jb;
   if (m <= 0 || n <= 0) return cudaSuccess;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_trail_z64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
   dim3 grid(cdiv_u(n, BN), cdiv_u(m, BM), lb.batch);
-  k_trail_z64<<<grid, NT, 0, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb);
+  k_trail_z64<<<grid, NT, SMEM_BYTES, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb);
   return ADGA_LAUNCH_CHECK();
 }
 
@@ -55,8 +60,8 @@ cudaError_t lu_trail_z64(z64 *M, const LUBatch &lb, int J, int jb, cudaStream_t 
 __global__ void __launch_bounds__(NT)
 k_resid_z64(int N, int R, int npts, int ch, const z64 *__restrict__ XD, const z64 *__restrict__ X,
             const z64 *__restrict__ Frow, const z64 *__restrict__ opg, z32 *V) {
-  __shared__ __align__(16) z64 As[2 * BK * BM];
-  __shared__ __align__(16) z64 Bs[2 * BK * BN];
+  extern __shared__ __align__(16) z64 zg_smem[];
+  z64 *As = zg_smem, *Bs = zg_smem + STAGES * BK * BM;
   const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
   const int rows = npts * R;
   const int r0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
@@ -94,10 +99,15 @@ k_resid_z64(int N, int R, int npts, int ch, const z64 *__restrict__ XD, const z6
 cudaError_t launch_resid_z64(const DevCtx &c, int npts, const z64 *XD, const z64 *X,
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, z32 *V, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_resid_z64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
   dim3 g(cdiv_u(c.N, BN), cdiv_u((size_t)npts * c.R, BM));
-  k_resid_z64<<<g, NT, 0, st>>>(c.N, c.R, npts, 0, XD, X, Frow_d, opg_d, V);
+  k_resid_z64<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, 0, XD, X, Frow_d, opg_d, V);
   cudaError_t e = ADGA_LAUNCH_CHECK();
   if (e != cudaSuccess) return e;
-  k_resid_z64<<<g, NT, 0, st>>>(c.N, c.R, npts, 1, XD, X, Frow_m, opg_m, V);
+  k_resid_z64<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, 1, XD, X, Frow_m, opg_m, V);
   return ADGA_LAUNCH_CHECK();
 }
