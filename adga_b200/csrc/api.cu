@@ -143,7 +143,7 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   h->bigbox = h->nnu_all != 2 * c.iwf;
   h->nd4 = c.nd2 * c.nd2;
   const char *ev = getenv("ADGA_NB");
-  if (ev) h->NB = std::max(16, std::min(128, atoi(ev) / 8 * 8));
+  if (ev) h->NB = std::max(16, std::min(64, atoi(ev) / 8 * 8));   // the LU kernels assume NB <= 64
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
     return ADGA_ECUDA;

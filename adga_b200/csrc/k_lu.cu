@@ -336,66 +336,147 @@ k_triinv(const T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T
 // ---------------------------------------------------------------------------
 // Row interchanges of one step on the columns outside the panel, then
 // U12 = L11^-1 A12 on the right columns (a jb x jb x TW product).
+//
+// The interchange map of the step (at most 2*NB <= 128 rows for NB <= 64) is
+// applied to a TW-column tile with every load issued before a barrier and
+// every store after it; thread (t % 64, t / 64) moves rows t%64 and t%64 + 64
+// of columns t/64 + 4v.  Left tiles (columns left of the panel, needed by the
+// forward solves) only swap rows and run in k_swap_left, which holds no
+// dynamic shared memory.  A k_swap_trsm CTA stages L11^-1 (lower triangle,
+// zero above) once and walks TPC column tiles: swap, stage the A12 tile,
+// multiply.  Both operands are arranged so that the FP32 path uses packed
+// two-lane FMAs (L as (re, re, -im, im), A12 as (re, im, im, re)).  Warp w
+// owns row blocks w and 15 - w (4 rows each), so every warp does the same
+// triangular k work; lane (r, cq) owns row r of each block and columns
+// cq + 8n (n < 4).
 // ---------------------------------------------------------------------------
 #define TW 32
-#define SWAP_VMAX 16     // gather items per thread: 2*MAXNB rows x TW columns / 256 threads
+constexpr int TS_LD = 65;        // A12 tile column stride (elements) in shared memory
+constexpr int TPC = 4;           // column tiles per k_swap_trsm CTA (L11^-1 staged once)
+
+template <typename T>
+__device__ __forceinline__ int load_map(const int *rm, int *s_map) {
+  const int cnt = min(rm[0], 128);
+  for (int i = threadIdx.x; i < 2 * cnt; i += 256) s_map[i] = rm[1 + i];
+  return cnt;
+}
+// every load of the tile before a barrier, every store after it (s_map loaded and synced)
+template <typename T>
+__device__ __forceinline__ void swap_tile(T *A, int N, int cnt, int cs, int nc, const int *s_map) {
+  const int t = threadIdx.x, kk = t & 63, cc = t >> 6;
+  T v[2][8];
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      const int k = kk + 64 * u, c = cc + 4 * w;
+      if (k < cnt && c < nc) v[u][w] = A[(size_t)s_map[2 * k + 1] + (size_t)(cs + c) * N];
+    }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      const int k = kk + 64 * u, c = cc + 4 * w;
+      if (k < cnt && c < nc) A[(size_t)s_map[2 * k] + (size_t)(cs + c) * N] = v[u][w];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_swap_left(T *M, size_t strideM, int N, int J, const int *rmap_all) {
+  __shared__ int s_map[4 * 64];
+  const int cs = blockIdx.x * TW, b = blockIdx.y;
+  const int cnt = load_map<T>(rmap_all + (size_t)b * RMAP_STRIDE, s_map);
+  __syncthreads();
+  swap_tile<T>(M + (size_t)b * strideM, N, cnt, cs, min(J, cs + TW) - cs, s_map);
+}
+
+template <typename T> struct TrsmOp;
+template <> struct TrsmOp<z32> {
+  typedef float4 L;
+  typedef float4 X;
+  static __device__ __forceinline__ L packL(z32 l) { return make_float4(l.x, l.x, -l.y, l.y); }
+  static __device__ __forceinline__ X packX(z32 x) { return make_float4(x.x, x.y, x.y, x.x); }
+  static __device__ __forceinline__ void fma(z32 &acc, const L &l, const X &x) {
+    acc = __ffma2_rn(make_float2(l.x, l.y), make_float2(x.x, x.y), acc);
+    acc = __ffma2_rn(make_float2(l.z, l.w), make_float2(x.z, x.w), acc);
+  }
+};
+template <> struct TrsmOp<z64> {
+  typedef z64 L;
+  typedef z64 X;
+  static __device__ __forceinline__ L packL(z64 l) { return l; }
+  static __device__ __forceinline__ X packX(z64 x) { return x; }
+  static __device__ __forceinline__ void fma(z64 &acc, const L &l, const X &x) { cfma(acc, l, x); }
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps,
-            const int *rmap_all, const T *Linv, int nleft_tiles) {
+            const int *rmap_all, const T *Linv) {
+  typedef TrsmOp<T> Op;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T *Ls = reinterpret_cast<T *>(smraw);          // [NB][NB]  L11^-1 of this step
-  T *Xs = Ls + NB * NB;                          // [TW][NB]
-  __shared__ int s_map[2 * 2 * MAXNB];
-  __shared__ int s_cnt;
-  const int tile = blockIdx.x, b = blockIdx.y, t = threadIdx.x, nt = blockDim.x;
+  typename Op::L *Ls = reinterpret_cast<typename Op::L *>(smraw);           // [64 k][64 i]
+  typename Op::X *Xs = reinterpret_cast<typename Op::X *>(Ls + 64 * 64);    // [TW c][TS_LD k]
+  __shared__ int s_map[4 * 64];
+  const int b = blockIdx.y, t = threadIdx.x;
   T *A = M + (size_t)b * strideM;
-  const bool right = tile >= nleft_tiles;
-  int cs, ce;
-  if (!right) { cs = tile * TW; ce = min(J, cs + TW); }
-  else { cs = J + jb + (tile - nleft_tiles) * TW; ce = min(ncols, cs + TW); }
-  const int nc = ce - cs;
-  const int *rm = rmap_all + (size_t)b * RMAP_STRIDE;
-  if (t == 0) s_cnt = rm[0];
-  for (int i = t; i < 2 * rm[0]; i += nt) s_map[i] = rm[1 + i];
-  if (right) {
-    const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
-    for (int e = t; e < NB * jb; e += nt) Ls[e] = L[e];
+  const T *L = Linv + ((size_t)b * nsteps + J / NB) * NB * NB;
+  for (int e = t; e < 64 * 64; e += 256) {
+    const int i = e & 63, k = e >> 6;
+    Ls[e] = Op::packL((i < jb && k <= i) ? L[i + k * NB] : czero<T>());
   }
-  __syncthreads();
-  // row interchanges: every load of the tile, a barrier, then every store
-  const int cnt = s_cnt, items = cnt * nc;
-  T v[SWAP_VMAX];
-#pragma unroll
-  for (int q = 0; q < SWAP_VMAX; ++q) {
-    const int e = t + q * 256;
-    if (e < items) {
-      const int k = e % cnt, c = e / cnt;
-      v[q] = A[(size_t)s_map[2 * k + 1] + (size_t)(cs + c) * N];
+  const int cnt = load_map<T>(rmap_all + (size_t)b * RMAP_STRIDE, s_map);
+  // warp w owns row blocks w and 15-w (4 rows each): equal k work per warp
+  const int warp = t >> 5, lane = t & 31, r = lane & 3, cq = lane >> 2;
+  const int ia = 4 * warp + r, ib = 4 * (15 - warp) + r;
+  const int ka = min(4 * warp + 4, jb), kb = min(4 * (16 - warp), jb);
+  for (int tile = 0; tile < TPC; ++tile) {
+    const int cs = J + jb + (blockIdx.x * TPC + tile) * TW;
+    if (cs >= ncols) break;
+    const int nc = min(ncols, cs + TW) - cs;
+    __syncthreads();               // map and L staged; the previous tile's Xs reads are done
+    swap_tile<T>(A, N, cnt, cs, nc, s_map);
+    __syncthreads();
+    for (int e = t; e < 64 * TW; e += 256) {
+      const int k = e & 63, c = e >> 6;
+      Xs[k + c * TS_LD] =
+          Op::packX((k < jb && c < nc) ? A[(size_t)(J + k) + (size_t)(cs + c) * N] : czero<T>());
     }
-  }
-  __syncthreads();
+    __syncthreads();
+    T acc[2][4];
 #pragma unroll
-  for (int q = 0; q < SWAP_VMAX; ++q) {
-    const int e = t + q * 256;
-    if (e < items) {
-      const int k = e % cnt, c = e / cnt;
-      A[(size_t)s_map[2 * k] + (size_t)(cs + c) * N] = v[q];
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int n = 0; n < 4; ++n) acc[m][n] = czero<T>();
+    int k = 0;
+#pragma unroll 2
+    for (; k < ka; ++k) {
+      const typename Op::L la = Ls[ia + k * 64], lb = Ls[ib + k * 64];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const typename Op::X x = Xs[k + (cq + 8 * n) * TS_LD];
+        Op::fma(acc[0][n], la, x);
+        Op::fma(acc[1][n], lb, x);
+      }
     }
-  }
-  if (!right) return;
-  __syncthreads();
-  for (int e = t; e < jb * nc; e += nt) {
-    int k = e % jb, c = e / jb;
-    Xs[k + c * NB] = A[(size_t)(J + k) + (size_t)(cs + c) * N];
-  }
-  __syncthreads();
-  // U12 = L11^-1 A12
-  for (int e = t; e < jb * nc; e += nt) {
-    int i = e % jb, c = e / jb;
-    T s = czero<T>();
-    for (int k = 0; k <= i; ++k) cfma(s, Ls[i + k * NB], Xs[k + c * NB]);
-    A[(size_t)(J + i) + (size_t)(cs + c) * N] = s;
+#pragma unroll 2
+    for (; k < kb; ++k) {
+      const typename Op::L lb = Ls[ib + k * 64];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) Op::fma(acc[1][n], lb, Xs[k + (cq + 8 * n) * TS_LD]);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int i = m ? ib : ia;
+      if (i < jb)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          const int c = cq + 8 * n;
+          if (c < nc) A[(size_t)(J + i) + (size_t)(cs + c) * N] = acc[m][n];
+        }
+    }
   }
 }
 
@@ -691,11 +772,11 @@ cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t s
 template <typename T>
 cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
                     cudaStream_t st, TrailTiming *tt) {
-  if (lb.NB > MAXNB || lb.NB % SWD) return cudaErrorInvalidValue;
+  if (lb.NB > 64 || lb.NB % SWD) return cudaErrorInvalidValue;   // k_swap_trsm covers NB <= 64
   const int nsteps = lb.nsteps();
   cudaError_t e;
   const size_t sm_tri = sizeof(T) * ((size_t)lb.NB * lb.NB + lb.NB);
-  const size_t sm_trsm = sizeof(T) * ((size_t)lb.NB * lb.NB + (size_t)lb.NB * TW);
+  const size_t sm_trsm = sizeof(typename TrsmOp<T>::L) * 64 * 64 + sizeof(typename TrsmOp<T>::X) * TW * TS_LD;
   static bool attr_done[2] = {false, false};
   const int ti = sizeof(T) == sizeof(z64) ? 0 : 1;
   if (!attr_done[ti]) {
@@ -710,10 +791,13 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
   if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
   const int nleft = apply_left ? (J + TW - 1) / TW : 0;
   const int nright = (lb.ncols - J - jb + TW - 1) / TW;
-  if (nleft + nright > 0) {
-    dim3 g(nleft + nright, lb.batch);
-    k_swap_trsm<T><<<g, 256, sm_trsm, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps,
-                                            lb.rmap, (const T *)lb.Linv, nleft);
+  if (nleft > 0) {
+    k_swap_left<T><<<dim3(nleft, lb.batch), 256, 0, st>>>(M, lb.strideM, lb.N, J, lb.rmap);
+    if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  }
+  if (nright > 0) {
+    k_swap_trsm<T><<<dim3((nright + TPC - 1) / TPC, lb.batch), 256, sm_trsm, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB,
+                                                                 nsteps, lb.rmap, (const T *)lb.Linv);
     if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
   }
   if (J + jb < lb.N) {
