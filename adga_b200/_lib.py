@@ -21,7 +21,8 @@ EXPORTS = [
     "adga_get_chi0_loc_inv", "adga_chi0_q", "adga_bse_point", "adga_get_gamma_w",
     "adga_calc_chi_qw", "adga_calc_eom_dynamic", "adga_calc_eom_dmft", "adga_calc_eom_static",
     "adga_inverse_matrix_z", "adga_index_kq", "adga_generate_q_vol", "adga_create_u",
-    "adga_inverse_matrix_z_noalloc",
+    "adga_inverse_matrix_z_noalloc", "adga_set_vertex_g4", "adga_vertex_transform",
+    "adga_index2component_band",
 ]
 
 
@@ -87,6 +88,9 @@ def load():
         "adga_index_kq": [i, i, i, vp, i, vp, i, vp],
         "adga_generate_q_vol": [i, i, i, i, i, i, vp],
         "adga_create_u": [i, d, d, d, vp, vp, vp],
+        "adga_set_vertex_g4": [vp, i, i, i, i, vp, vp, vp],
+        "adga_vertex_transform": [vp, i, i, i, i, vp, vp, vp, vp, vp],
+        "adga_index2component_band": [i, i, vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

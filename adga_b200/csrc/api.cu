@@ -40,6 +40,8 @@ struct adga_handle {
   std::vector<void *> owned;
   // vertex store, one pair per omega
   std::vector<z64 *> vd, vm;
+  z64 *g4buf = nullptr;        // g4 staging of adga_set_vertex_g4 (both channels)
+  size_t g4cap = 0;
   // local block
   int diag_iwb = INT_MIN, loc_iwb = INT_MIN;
   z64 *c0inv = nullptr, *c0w = nullptr, *bubtmp = nullptr;
@@ -217,6 +219,7 @@ extern "C" int adga_destroy(adga_handle *h) {
   free_list(h->owned);
   for (auto p : h->vd) if (p) cudaFree(p);
   for (auto p : h->vm) if (p) cudaFree(p);
+  if (h->g4buf) cudaFree(h->g4buf);
   if (h->qidx_h) cudaFreeHost(h->qidx_h);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
@@ -263,6 +266,86 @@ extern "C" int adga_set_vertex(adga_handle *h, int iwb, const adga_z *chi_d, con
   CK(cudaMemcpyAsync(h->vm[w], chi_m, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
   if (h->loc_iwb == iwb) h->loc_iwb = INT_MIN;
   CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// vertex ingest (read_vertex's transform, k_vertex.cu)
+static int vertex_g4(adga_handle *h, int iwb, int vtype, int W, int nineq, const int *ndims,
+                     const adga_z *g4d, const adga_z *g4m, z64 *outd, z64 *outm) {
+  const DevCtx &c = h->c;
+  if (!g4d || !g4m || !ndims || nineq < 1) return fail(h, ADGA_EINVAL, "vertex_g4: missing argument");
+  if (vtype < ADGA_VERTEX_FULL_G4 || vtype > ADGA_VERTEX_CHI_G4)
+    return fail(h, ADGA_EINVAL, "vertex_g4: unknown vertex type");
+  if (iwb < -c.iwb || iwb > c.iwb) return fail(h, ADGA_EINVAL, "vertex_g4: iwb out of range");
+  if (W < c.iwf) return fail(h, ADGA_EINVAL, "vertex_g4: iwfmax_g4 smaller than iwfmax_small");
+  if (c.nd > ADGA_MAX_BANDS) return fail(h, ADGA_EINVAL, "vertex_g4: more than ADGA_MAX_BANDS bands");
+  // index2cor (src/aux.f90:190-221): correlated bands of atom ineq start after
+  // all bands of the atoms before it
+  VertexAtoms atoms{};
+  int start = 0;
+  for (int q = 0; q < nineq; ++q) {
+    const int ncor = ndims[q], nunc = ndims[nineq + q];
+    if (ncor < 0 || nunc < 0) return fail(h, ADGA_EINVAL, "vertex_g4: negative band count");
+    for (int b = start; b < start + ncor && b < c.nd; ++b) atoms.a[b] = q + 1;
+    start += ncor + nunc;
+  }
+  if (start != c.nd) return fail(h, ADGA_EINVAL, "vertex_g4: ndims do not add up to ndim");
+  const size_t n = (size_t)c.nd2 * c.nd2 * (2 * (size_t)W) * (2 * (size_t)W);
+  if (h->g4cap < n) {
+    if (h->g4buf) cudaFree(h->g4buf);
+    h->g4buf = nullptr;
+    h->g4cap = 0;
+    if (cudaMalloc(&h->g4buf, 2 * n * sizeof(z64)) != cudaSuccess)
+      return fail(h, ADGA_ENOMEM, "vertex_g4: staging buffer");
+    h->g4cap = n;
+  }
+  CK(cudaMemcpyAsync(h->g4buf, g4d, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->g4buf + n, g4m, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  CK(launch_vertex_g4(c, iwb, vtype, W, atoms, h->g4buf, h->g4buf + n, outd, outm, h->st));
+  return 0;
+}
+
+extern "C" int adga_set_vertex_g4(adga_handle *h, int iwb, int vertex_type, int iwfmax_g4, int nineq,
+                                  const int *ndims, const adga_z *g4_dens, const adga_z *g4_magn) {
+  if (!h) return ADGA_EINVAL;
+  if (iwb < -h->c.iwb || iwb > h->c.iwb) return fail(h, ADGA_EINVAL, "iwb out of range");
+  const int w = iwb + h->c.iwb;
+  const size_t n = (size_t)h->c.N * h->c.N;
+  if (!h->vd[w]) {
+    if (cudaMalloc(&h->vd[w], n * sizeof(z64)) != cudaSuccess) return fail(h, ADGA_ENOMEM, "vertex alloc");
+    if (cudaMalloc(&h->vm[w], n * sizeof(z64)) != cudaSuccess) return fail(h, ADGA_ENOMEM, "vertex alloc");
+  }
+  int r = vertex_g4(h, iwb, vertex_type, iwfmax_g4, nineq, ndims, g4_dens, g4_magn, h->vd[w], h->vm[w]);
+  if (r) return r;
+  if (h->loc_iwb == iwb) h->loc_iwb = INT_MIN;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+extern "C" int adga_vertex_transform(adga_handle *h, int iwb, int vertex_type, int iwfmax_g4, int nineq,
+                                     const int *ndims, const adga_z *g4_dens, const adga_z *g4_magn,
+                                     adga_z *chi_loc_dens, adga_z *chi_loc_magn) {
+  if (!h || !chi_loc_dens || !chi_loc_magn) return ADGA_EINVAL;
+  const size_t n = (size_t)h->c.N * h->c.N;
+  z64 *tmp = nullptr;
+  if (cudaMalloc(&tmp, 2 * n * sizeof(z64)) != cudaSuccess) return fail(h, ADGA_ENOMEM, "transform output");
+  int r = vertex_g4(h, iwb, vertex_type, iwfmax_g4, nineq, ndims, g4_dens, g4_magn, tmp, tmp + n);
+  if (!r && (cudaMemcpyAsync(chi_loc_dens, tmp, n * sizeof(z64), cudaMemcpyDeviceToHost, h->st) != cudaSuccess ||
+             cudaMemcpyAsync(chi_loc_magn, tmp + n, n * sizeof(z64), cudaMemcpyDeviceToHost, h->st) != cudaSuccess ||
+             cudaStreamSynchronize(h->st) != cudaSuccess))
+    r = fail(h, ADGA_ECUDA, "transform download");
+  cudaFree(tmp);
+  return r;
+}
+
+extern "C" int adga_index2component_band(int nbands, int ind, int *b) {
+  if (!b || nbands < 1 || ind < 1 || ind > nbands * nbands * nbands * nbands) return ADGA_EINVAL;
+  const int i = ind - 1, n3 = nbands * nbands * nbands, n2 = nbands * nbands;
+  b[0] = i / n3 + 1;
+  b[1] = (i % n3) / n2 + 1;
+  b[2] = (i % n2) / nbands + 1;
+  b[3] = i % nbands + 1;
   return 0;
 }
 

@@ -2,6 +2,7 @@
 // one-particle data.  Passed by value to the kernels.
 #pragma once
 #include "common.cuh"
+#include "adga.h"
 
 struct DevCtx {
   int nd, nd2, nkp, nqp, nkp_eom;
@@ -20,6 +21,11 @@ struct DevCtx {
   const int *kq;                 // k-q index, 0-based, (nkp, nqp)
   const int *kqe;                // EOM k-q index, 0-based, (nkp_eom, nqp)
   const z64 *gtab;               // G(k, nu): [(nu - nu_lo)*nkp + k][nd2], column-major nd x nd
+};
+
+// correlated-subspace atom (1-based) of every band, 0 for uncorrelated bands
+struct VertexAtoms {
+  int a[ADGA_MAX_BANDS];
 };
 
 // Kernel launchers (host functions), grouped by source file.
@@ -41,6 +47,10 @@ cudaError_t launch_eom_dmft(const DevCtx &c, int iwb, const z64 *gam_d, z64 *sig
 cudaError_t launch_mirror_sigma(const DevCtx &c, z64 *sigma, int nk, cudaStream_t st);
 cudaError_t launch_calc_chi_qw(const DevCtx &c, z64 *chi_qw, const z64 *interm3,
                                const z64 *chi0_sum, cudaStream_t st);
+
+// k_vertex.cu: read_vertex's transform of g4 (one omega) into chi_loc (device buffers)
+cudaError_t launch_vertex_g4(const DevCtx &c, int iwb, int vtype, int W, const VertexAtoms &atoms,
+                             const z64 *g4d, const z64 *g4m, z64 *chid, z64 *chim, cudaStream_t st);
 
 // k_chi0.cu: chi0q[p] (nd2, nd2, nnu_out) for a batch of points at one omega
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,

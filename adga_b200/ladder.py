@@ -125,6 +125,39 @@ class Ladder:
         d, m = _z(chi_loc_dens, (N, N)), _z(chi_loc_magn, (N, N))
         self._check(self._lib.adga_set_vertex(self._h, int(iwb), ptr(d), ptr(m)), "set_vertex")
 
+    VERTEX_TYPES = {"full_g4": 0, "connected_g4": 1, "chi_g4": 2}
+
+    def _g4_args(self, vertex_type, g4_dens, g4_magn, ndims):
+        vt = self.VERTEX_TYPES[vertex_type] if isinstance(vertex_type, str) else int(vertex_type)
+        nd = self.ndim
+        W = g4_dens.shape[2] // 2
+        shape = (nd, nd, 2 * W, nd, nd, 2 * W)
+        d, m = _z(g4_dens, shape), _z(g4_magn, shape)
+        nd_arr = np.asfortranarray(np.asarray(ndims if ndims is not None else [[nd, 0]], dtype=np.int32))
+        return vt, W, nd_arr, d, m
+
+    def set_vertex_g4(self, iwb, g4_dens, g4_magn, vertex_type="connected_g4", ndims=None):
+        """read_vertex (src/hdf5_module.f90:629-773) from the two-particle Green's
+        functions g4(ndim, ndim, 2W, ndim, ndim, 2W) as w2dynamics stores them
+        (before the beta factor): beta scaling, compound index of the small box
+        and the disconnected terms of vertex_type are applied on the GPU, and the
+        result is staged like set_vertex.  ndims(nineq, 2): correlated and
+        uncorrelated band counts per inequivalent atom (default: one atom, all
+        bands correlated)."""
+        vt, W, nd_arr, d, m = self._g4_args(vertex_type, g4_dens, g4_magn, ndims)
+        self._check(self._lib.adga_set_vertex_g4(self._h, int(iwb), vt, W, nd_arr.shape[0], ptr(nd_arr),
+                                                 ptr(d), ptr(m)), "set_vertex_g4")
+
+    def vertex_transform(self, iwb, g4_dens, g4_magn, vertex_type="connected_g4", ndims=None):
+        """The same transform, returning (chi_loc_dens, chi_loc_magn), maxdim x maxdim."""
+        vt, W, nd_arr, d, m = self._g4_args(vertex_type, g4_dens, g4_magn, ndims)
+        N = self.maxdim
+        od = np.zeros((N, N), dtype=np.complex128, order="F")
+        om = np.zeros((N, N), dtype=np.complex128, order="F")
+        self._check(self._lib.adga_vertex_transform(self._h, int(iwb), vt, W, nd_arr.shape[0], ptr(nd_arr),
+                                                    ptr(d), ptr(m), ptr(od), ptr(om)), "vertex_transform")
+        return od, om
+
     def reset_outputs(self):
         self._check(self._lib.adga_reset_outputs(self._h), "reset_outputs")
 
@@ -255,6 +288,17 @@ def inverse_matrix(M):
     if rc < 0:
         raise AdgaError(rc, "inverse_matrix_z")
     return A, ierr.value, buf.value.decode()
+
+
+def index2component_band(nbands, ind):
+    """index2component_band (src/aux.f90:169-186): 1-based band pattern of a
+    1-based vertex group index."""
+    lib = _lib.load()
+    b = np.zeros(4, dtype=np.int32)
+    rc = lib.adga_index2component_band(int(nbands), int(ind), ptr(b))
+    if rc:
+        raise AdgaError(rc, "index2component_band: index out of range")
+    return tuple(int(x) for x in b)
 
 
 def generate_q_vol(nk, nq):

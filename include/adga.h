@@ -87,6 +87,40 @@ int adga_device_bytes(const adga_handle *h, long long *bytes);
 int adga_set_vertex(adga_handle *h, int iwb, const adga_z *chi_loc_dens,
                     const adga_z *chi_loc_magn);
 
+/* Vertex types of the two-particle input (vertex_type, src/parameters_module.f90:74). */
+#define ADGA_VERTEX_FULL_G4      0   /* full two-particle Green's function      */
+#define ADGA_VERTEX_CONNECTED_G4 1   /* connected part                          */
+#define ADGA_VERTEX_CHI_G4       2   /* generalised susceptibility chi          */
+#define ADGA_MAX_BANDS 32
+
+/*
+ * Vertex ingest: read_vertex's transform (src/hdf5_module.f90:629-773) on
+ * the device.  g4_dens / g4_magn hold the local two-particle Green's
+ * function of omega = iwb as w2dynamics stores it and read_vertex places it
+ * (before its beta factor, :700,711): Fortran order
+ * g4(ndim, ndim, -iwfmax_g4:iwfmax_g4-1, ndim, ndim, -iwfmax_g4:iwfmax_g4-1),
+ * iwfmax_g4 >= iwfmax_small.  The library applies the beta factor, the
+ * compound index of the small box and the disconnected terms of vertex_type
+ * (ADGA_VERTEX_*), and stages the result as adga_set_vertex would.
+ * nineq and ndims(nineq, 2) (Fortran order: correlated, then uncorrelated
+ * band counts per inequivalent atom) decide which legs share a correlated
+ * subspace (index2cor, src/aux.f90:190-221); their band counts must sum to
+ * ndim.  Replaces read_vertex's loop at src/hdf5_module.f90:718-770.
+ */
+int adga_set_vertex_g4(adga_handle *h, int iwb, int vertex_type, int iwfmax_g4, int nineq,
+                       const int *ndims, const adga_z *g4_dens, const adga_z *g4_magn);
+
+/* The same transform, returning chi_loc^{dens,magn} (maxdim x maxdim,
+ * column-major) to host memory instead of staging it. */
+int adga_vertex_transform(adga_handle *h, int iwb, int vertex_type, int iwfmax_g4, int nineq,
+                          const int *ndims, const adga_z *g4_dens, const adga_z *g4_magn,
+                          adga_z *chi_loc_dens, adga_z *chi_loc_magn);
+
+/* index2component_band (src/aux.f90:169-186): the 1-based band pattern
+ * b[0..3] of a 1-based vertex group index ind over nbands bands (the group
+ * names of the w2dynamics vertex file).  Host only; returns 0 or ADGA_EINVAL. */
+int adga_index2component_band(int nbands, int ind, int *b);
+
 /* Zero the device accumulators (chi, bubble, Sigma) before a run. */
 int adga_reset_outputs(adga_handle *h);
 

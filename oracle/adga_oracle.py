@@ -128,6 +128,80 @@ def _index2ineq(ndims, m, n, o, p):
     return a if (a == b and c == d and a == d) else 0
 
 
+def component2index_band(nbands, b1, b2, b3, b4):
+    """src/aux.f90:157-164 (1-based bands and group index)."""
+    return nbands ** 3 * (b1 - 1) + nbands ** 2 * (b2 - 1) + nbands * (b3 - 1) + b4
+
+
+def index2component_band(nbands, ind):
+    """src/aux.f90:169-186 (1-based group index -> 1-based bands)."""
+    it = ind - 1
+    n3, n2 = nbands ** 3, nbands ** 2
+    b1 = it // n3 + 1
+    b2 = (it - n3 * (b1 - 1)) // n2 + 1
+    b3 = (it - n3 * (b1 - 1) - n2 * (b2 - 1)) // nbands + 1
+    b4 = it - n3 * (b1 - 1) - n2 * (b2 - 1) - nbands * (b3 - 1) + 1
+    return b1, b2, b3, b4
+
+
+FULL_G4, CONNECTED_G4, CHI_G4 = 0, 1, 2   # src/parameters_module.f90:74
+
+
+def read_vertex_transform(g4_dens, g4_magn, iwb, vertex_type, ndims, giw, beta, iwf, iwmax):
+    """The compound-index part of read_vertex (src/hdf5_module.f90:700,711 and
+    :718-770): g4(ndim, ndim, 2W, ndim, ndim, 2W) as w2dynamics stores it
+    (index n + W holds Matsubara n, before the beta factor) -> chi_loc of the
+    small box (maxdim x maxdim) with the disconnected terms of vertex_type.
+    giw[n + iwmax, i] is the local Green's function."""
+    nd = g4_dens.shape[0]
+    W = g4_dens.shape[2] // 2
+    nd2 = nd * nd
+    N = nd2 * 2 * iwf
+    g4d = np.asarray(g4_dens) * beta
+    g4m = np.asarray(g4_magn) * beta
+    cd = np.zeros((N, N), complex)
+    cm = np.zeros((N, N), complex)
+    cor = {}
+    for i in range(nd):
+        for j in range(nd):
+            for k in range(nd):
+                for l in range(nd):
+                    cor[i, j, k, l] = _index2cor(ndims, i + 1, j + 1, k + 1, l + 1)
+    g = lambda n, b: giw[n + iwmax, b]
+    i2 = 0
+    for w2 in range(-iwf, iwf):
+        for l in range(nd):
+            for k in range(nd):
+                i1 = 0
+                for w1 in range(-iwf, iwf):
+                    for i in range(nd):
+                        for j in range(nd):
+                            cm[i1, i2] = g4m[i, j, w1 + W, k, l, w2 + W]
+                            cd[i1, i2] = g4d[i, j, w1 + W, k, l, w2 + W]
+                            c4 = cor[i, j, k, l]
+                            bub = w2 == w1 and i == l and j == k
+                            if vertex_type == FULL_G4:
+                                if iwb == 0 and i == j and k == l and c4:
+                                    cd[i1, i2] -= 2.0 * beta * g(w1, i) * g(w2, l)
+                                if bub and not c4:
+                                    t = beta * g(w1, i) * g(w2 - iwb, j)
+                                    cd[i1, i2] -= t
+                                    cm[i1, i2] -= t
+                            elif vertex_type == CONNECTED_G4:
+                                if bub:
+                                    t = beta * g(w1, i) * g(w2 - iwb, j)
+                                    cd[i1, i2] -= t
+                                    cm[i1, i2] -= t
+                            elif vertex_type == CHI_G4:
+                                if bub and not c4:
+                                    t = beta * g(w1, i) * g(w2 - iwb, j)
+                                    cd[i1, i2] -= t
+                                    cm[i1, i2] -= t
+                            i1 += 1
+                i2 += 1
+    return np.asfortranarray(cd), np.asfortranarray(cm)
+
+
 def create_u(ndims, Udd, Vdd, Jdd, Upp=None, Vpp=None, Jpp=None,
              Udp=None, Vdp=None, Jdp=None, interaction_mode=None):
     """Kanamori/density-density U tensor and its compound forms.
