@@ -4,6 +4,7 @@
 #include "adga.h"
 #include "ctx.cuh"
 #include "lu.cuh"
+#define GINV_MAXND_HOST 8   // ndim limit of the small inverses (ginv.cuh)
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -183,7 +184,7 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   if (kde) UP(kde, k_data_eom, sizeof(int) * c.nkp_eom);
 #undef UP
   c.iw = iw; c.hk = hk_d; c.siw = siw_d; c.giw = giw_d; c.dc = dc_d;
-  c.u = u_d; c.ut = ut_d; c.ndmft = nd_d; c.kq = kq; c.kqe = kqe; c.gtab = gt;
+  c.u = u_d; c.ut = ut_d; c.ndmft = nd_d; c.kq = kq; c.kqe = kqe; c.gtab = gt; c.keom = kde;
   CK(launch_kq_index(c.nkpx, c.nkpy, c.nkpz, nullptr, c.nkp, qd, c.nqp, 0, kq, st));
   if (c.nkp_eom == c.nkp && !kde)
     CK(cudaMemcpyAsync(kqe, kq, sizeof(int) * c.nkp * c.nqp, cudaMemcpyDeviceToDevice, st));
@@ -695,6 +696,46 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   h->stats.kernel_launches = g_adga_launches.load() - launches0;
   h->last_npts = npts;
   if (stats) *stats = h->stats;
+  return 0;
+}
+
+extern "C" int adga_post_loop(adga_handle *h, adga_z *sigma_sum, adga_z *sigma_loc, adga_z *gloc,
+                              adga_z *n_dga_k, adga_z *n_dga) {
+  if (!h) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  cudaStream_t st = h->st;
+  const bool full_mesh = c.nkp_eom == c.nkp && !c.keom;
+  if ((sigma_loc || gloc) && !full_mesh)
+    return fail(h, ADGA_EINVAL, "post_loop: sigma_loc / gloc need the EOM on the full k mesh");
+  if (c.nd > GINV_MAXND_HOST) return fail(h, ADGA_EINVAL, "post_loop: ndim above 8");
+  const size_t ns = (size_t)c.nd2 * 2 * c.iwf * c.nkp_eom, ngl = (size_t)2 * c.iwmax * c.nd2;
+  const size_t nsl = (size_t)c.nd2 * 2 * c.iwf, nnk = (size_t)c.nkp_eom * c.nd2;
+  z64 *buf = nullptr;
+  const size_t total = ns + nsl + ngl + nnk + c.nd;
+  if (cudaMalloc(&buf, total * sizeof(z64)) != cudaSuccess) return fail(h, ADGA_ENOMEM, "post_loop buffers");
+  z64 *sig = buf, *sl = sig + ns, *gl = sl + nsl, *nk = gl + ngl, *n = nk + nnk;
+  cudaError_t e;
+  if (sigma_sum) {
+    e = cudaMemcpyAsync(sig, sigma_sum, ns * sizeof(z64), cudaMemcpyHostToDevice, st);
+  } else {
+    // this handle's own non-local Sigma, mirrored (src/eom_module.f90:228)
+    e = launch_mirror_sigma(c, h->sigma_nl, c.nkp_eom, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sig, h->sigma_nl, ns * sizeof(z64), cudaMemcpyDeviceToDevice, st);
+  }
+  if (e == cudaSuccess)
+    e = launch_post_loop(c, c.keom, sig, sigma_loc ? sl : nullptr, gloc ? gl : nullptr,
+                         (n_dga_k || n_dga) ? nk : nullptr, n_dga ? n : nullptr, st);
+#define PDN(dst, src, cnt) \
+  if (e == cudaSuccess && dst) e = cudaMemcpyAsync(dst, src, (cnt) * sizeof(z64), cudaMemcpyDeviceToHost, st)
+  PDN(sigma_sum, sig, ns);
+  PDN(sigma_loc, sl, nsl);
+  PDN(gloc, gl, ngl);
+  PDN(n_dga_k, nk, nnk);
+  PDN(n_dga, n, (size_t)c.nd);
+#undef PDN
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(h, ADGA_ECUDA, std::string("post_loop: ") + cudaGetErrorString(e));
   return 0;
 }
 

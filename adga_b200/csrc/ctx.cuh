@@ -20,6 +20,7 @@ struct DevCtx {
   const z64 *ndmft;              // nd
   const int *kq;                 // k-q index, 0-based, (nkp, nqp)
   const int *kqe;                // EOM k-q index, 0-based, (nkp_eom, nqp)
+  const int *keom;               // EOM k-points (k_data_eom, 1-based), null for the full mesh
   const z64 *gtab;               // G(k, nu): [(nu - nu_lo)*nkp + k][nd2], column-major nd x nd
 };
 
@@ -51,6 +52,11 @@ cudaError_t launch_calc_chi_qw(const DevCtx &c, z64 *chi_qw, const z64 *interm3,
 // k_vertex.cu: read_vertex's transform of g4 (one omega) into chi_loc (device buffers)
 cudaError_t launch_vertex_g4(const DevCtx &c, int iwb, int vtype, int W, const VertexAtoms &atoms,
                              const z64 *g4d, const z64 *g4m, z64 *chid, z64 *chim, cudaStream_t st);
+
+// k_postloop.cu: add_siw_dmft on sig (in place), then get_sigma_g_loc (sig_loc, gloc; full
+// k mesh) and get_ndga (n_dga_k, n_dga); null outputs are skipped
+cudaError_t launch_post_loop(const DevCtx &c, const int *keom, z64 *sig, z64 *sig_loc, z64 *gloc,
+                             z64 *n_dga_k, z64 *n_dga, cudaStream_t st);
 
 // k_chi0.cu: chi0q[p] (nd2, nd2, nnu_out) for a batch of points at one omega
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,

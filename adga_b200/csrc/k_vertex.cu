@@ -19,6 +19,7 @@
 // One thread per chi_loc element; the result lands in the handle's vertex
 // store or in a caller buffer.
 #include "ctx.cuh"
+#include <algorithm>
 
 __global__ void __launch_bounds__(256)
 k_vertex_g4(DevCtx c, int iwb, int vtype, int W, VertexAtoms atoms, const z64 *__restrict__ g4d,

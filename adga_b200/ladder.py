@@ -208,6 +208,26 @@ class Ladder:
             sig[b, b] += np.asarray(siw)[nu, b][:, None]
         return dict(chi_dens=chi_d, chi_magn=chi_m, chi_loc_dens=cld, chi_loc_magn=clm, sigma=sig)
 
+    def post_loop(self, sigma_sum=None, want=("sigma_loc", "gloc", "n_dga_k", "n_dga")):
+        """Post-loop assembly of src/main.F90:869-890 on the GPU: add_siw_dmft,
+        get_sigma_g_loc (full k mesh only) and get_ndga.  sigma_sum: the reduced
+        non-local self-energy (ndim, ndim, 2*iwf, nkp_eom); None uses this
+        handle's own accumulated Sigma_nl.  Returns a dict with 'sigma_sum'
+        (Sigma_nl + siw) and the requested outputs."""
+        nd, iwf = self.ndim, self.iwf
+        nke = self.nkp_eom
+        sig = (np.zeros((nd, nd, 2 * iwf, nke), dtype=np.complex128, order="F") if sigma_sum is None
+               else _z(sigma_sum, (nd, nd, 2 * iwf, nke)).copy(order="F"))
+        bufs = {"sigma_loc": (nd, nd, 2 * iwf), "gloc": (2 * self.iwmax, nd, nd),
+                "n_dga_k": (nke, nd, nd), "n_dga": (nd,)}
+        out = {k: np.zeros(v, dtype=np.complex128, order="F") for k, v in bufs.items() if k in want}
+        self._check(self._lib.adga_post_loop(self._h, ptr(sig) if sigma_sum is not None else None,
+                                             ptr(out.get("sigma_loc")), ptr(out.get("gloc")),
+                                             ptr(out.get("n_dga_k")), ptr(out.get("n_dga"))), "post_loop")
+        if sigma_sum is not None:
+            out["sigma_sum"] = sig
+        return out
+
     # ---- per-routine entry points -------------------------------------
     def get_chi0_loc(self, iwf, iwb):
         out = np.zeros((self.ndim2, self.ndim2), dtype=np.complex128, order="F")

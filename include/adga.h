@@ -121,6 +121,25 @@ int adga_vertex_transform(adga_handle *h, int iwb, int vertex_type, int iwfmax_g
  * names of the w2dynamics vertex file).  Host only; returns 0 or ADGA_EINVAL. */
 int adga_index2component_band(int nbands, int ind, int *b);
 
+/*
+ * Post-loop assembly of the self-energy (src/main.F90:869-890) on the GPU:
+ *   add_siw_dmft     (src/eom_module.f90:237-251): sigma_sum(i,i,nu,k) += siw(nu,i);
+ *   get_sigma_g_loc  (src/one_particle_quant_module.f90:129-187): the k-summed DGA
+ *                    self-energy sigma_loc(ndim,ndim,-iwfmax_small:iwfmax_small-1) and
+ *                    Green's function gloc(-iwmax:iwmax-1,ndim,ndim) (DGA Sigma inside
+ *                    the vertex box, siw outside, gloc(-nu-1) = gloc(nu)^dagger);
+ *                    needs the EOM on the full k mesh;
+ *   get_ndga         (src/one_particle_quant_module.f90:344-394): n_dga_k(nkp_eom,ndim,ndim)
+ *                    and n_dga(ndim) (complex, zero imaginary part, as declared at
+ *                    src/parameters_module.f90:61).
+ * sigma_sum (ndim,ndim,-iwfmax_small:iwfmax_small-1,nkp_eom) holds the reduced non-local
+ * self-energy (src/main.F90:845-852) on entry and sigma_sum + siw on exit; NULL uses
+ * this handle's own accumulated (mirrored) Sigma_nl and leaves it unchanged.  Any
+ * output may be NULL to skip it.
+ */
+int adga_post_loop(adga_handle *h, adga_z *sigma_sum, adga_z *sigma_loc, adga_z *gloc,
+                   adga_z *n_dga_k, adga_z *n_dga);
+
 /* Zero the device accumulators (chi, bubble, Sigma) before a run. */
 int adga_reset_outputs(adga_handle *h);
 

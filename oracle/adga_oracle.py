@@ -701,3 +701,57 @@ def assemble(inp: LadderInputs, out):
         sig[b, b, :, :] += inp.siw[np.arange(-iwfs, iwfs) + inp.iwmax, b][:, None]
     return dict(chi_dens=chi_d, chi_magn=chi_m, chi_loc_dens=chi_loc_d,
                 chi_loc_magn=chi_loc_m, sigma=sig)
+
+
+def _gkiw_dga(inp: LadderInputs, ik, n, skiw):
+    """get_gkiw_dga (src/one_particle_quant_module.f90:106-126): lattice G at k-point
+    ik (0-based, full mesh), Matsubara n, with any self-energy skiw (ndim x ndim)."""
+    nd = inp.ndim
+    g = -inp.hk[:, :, ik] - skiw
+    for i in range(nd):
+        g[i, i] = 1j * inp.iw_data[n + inp.iwmax] + inp.mu - inp.hk[i, i, ik] - inp.dc[0, i] - skiw[i, i]
+    return inverse_matrix(g)[0]
+
+
+def post_loop(inp: LadderInputs, sigma_sum, k_data_eom=None):
+    """src/main.F90:869-890 on the reduced non-local self-energy
+    sigma_sum(ndim, ndim, 2*iwf, nkp_eom):
+      add_siw_dmft    (src/eom_module.f90:237-251),
+      get_sigma_g_loc (src/one_particle_quant_module.f90:129-187; full k mesh only),
+      get_ndga        (src/one_particle_quant_module.f90:344-394).
+    k_data_eom: 1-based full-mesh k indices of the EOM k-points (None = full mesh)."""
+    nd, iwf, iwmax, beta = inp.ndim, inp.iwfmax_small, inp.iwmax, inp.beta
+    sig = np.array(sigma_sum, dtype=complex, order="F")
+    nk_eom = sig.shape[3]
+    for ik in range(nk_eom):                       # add_siw_dmft
+        for w in range(-iwf, iwf):
+            for b in range(nd):
+                sig[b, b, w + iwf, ik] += inp.siw[w + iwmax, b]
+    out = {"sigma_sum": sig}
+    diag_siw = lambda n: np.diag(inp.siw[n + iwmax, :])
+    if k_data_eom is None and nk_eom == inp.nkp:   # get_sigma_g_loc
+        nkp = inp.nkp
+        sloc = sig.sum(axis=3) / nkp
+        gloc = np.zeros((2 * iwmax, nd, nd), complex)
+        for ik in range(nkp):
+            for n in range(0, iwf):
+                gloc[n + iwmax] += _gkiw_dga(inp, ik, n, sig[:, :, n + iwf, ik])
+            for n in range(iwf, iwmax):
+                gloc[n + iwmax] += _gkiw_dga(inp, ik, n, diag_siw(n))
+        for n in range(0, iwmax):
+            gloc[-n - 1 + iwmax] = gloc[n + iwmax].conj().T
+        out["sigma_loc"] = np.asfortranarray(sloc)
+        out["gloc"] = np.asfortranarray(gloc / nkp)
+    kmap = (np.arange(nk_eom) if k_data_eom is None else np.asarray(k_data_eom) - 1)
+    nk = np.zeros((nk_eom, nd, nd), complex)
+    for ik in range(nk_eom):                       # get_ndga
+        for n in range(0, iwf):
+            nk[ik] += _gkiw_dga(inp, kmap[ik], n, sig[:, :, n + iwf, ik]).real
+        for n in range(iwf, iwmax):
+            nk[ik] += _gkiw_dga(inp, kmap[ik], n, diag_siw(n)).real
+        nk[ik] = 2.0 * nk[ik] / beta
+        for i in range(nd):
+            nk[ik, i, i] += 0.5
+    out["n_dga_k"] = np.asfortranarray(nk)
+    out["n_dga"] = np.array([nk[:, i, i].sum() for i in range(nd)]) / nk_eom
+    return out
