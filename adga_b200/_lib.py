@@ -22,7 +22,7 @@ EXPORTS = [
     "adga_calc_chi_qw", "adga_calc_eom_dynamic", "adga_calc_eom_dmft", "adga_calc_eom_static",
     "adga_inverse_matrix_z", "adga_index_kq", "adga_generate_q_vol", "adga_create_u",
     "adga_inverse_matrix_z_noalloc", "adga_set_vertex_g4", "adga_vertex_transform",
-    "adga_index2component_band", "adga_post_loop",
+    "adga_index2component_band", "adga_post_loop", "adga_set_threeleg", "adga_set_chi_loc_ext",
 ]
 
 
@@ -92,6 +92,8 @@ def load():
         "adga_vertex_transform": [vp, i, i, i, i, vp, vp, vp, vp, vp],
         "adga_index2component_band": [i, i, vp],
         "adga_post_loop": [vp, vp, vp, vp, vp, vp],
+        "adga_set_threeleg": [vp, i, i, i, vp, vp, vp],
+        "adga_set_chi_loc_ext": [vp, i, i, vp, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

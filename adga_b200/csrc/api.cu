@@ -41,8 +41,10 @@ struct adga_handle {
   std::vector<void *> owned;
   // vertex store, one pair per omega
   std::vector<z64 *> vd, vm;
-  z64 *g4buf = nullptr;        // g4 staging of adga_set_vertex_g4 (both channels)
+  z64 *g4buf = nullptr;        // staging of the raw vertex / three-leg / chi_loc inputs
   size_t g4cap = 0;
+  std::vector<z64 *> tl_d, tl_m;   // external three-leg gamma^w per omega (nd2 x N), or null
+  z64 *ext_cld = nullptr, *ext_clm = nullptr;   // external chi_loc (nd2, nd2, nw), or null
   // local block
   int diag_iwb = INT_MIN, loc_iwb = INT_MIN;
   z64 *c0inv = nullptr, *c0w = nullptr, *bubtmp = nullptr;
@@ -207,6 +209,8 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   if (!ok) { adga_destroy(h); return ADGA_ENOMEM; }
   h->vd.assign(h->nw, nullptr);
   h->vm.assign(h->nw, nullptr);
+  h->tl_d.assign(h->nw, nullptr);
+  h->tl_m.assign(h->nw, nullptr);
   CK(cudaStreamSynchronize(st));
   *out = h;
   return adga_reset_outputs(h);
@@ -221,6 +225,10 @@ extern "C" int adga_destroy(adga_handle *h) {
   for (auto p : h->vd) if (p) cudaFree(p);
   for (auto p : h->vm) if (p) cudaFree(p);
   if (h->g4buf) cudaFree(h->g4buf);
+  for (auto p : h->tl_d) if (p) cudaFree(p);
+  for (auto p : h->tl_m) if (p) cudaFree(p);
+  if (h->ext_cld) cudaFree(h->ext_cld);
+  if (h->ext_clm) cudaFree(h->ext_clm);
   if (h->qidx_h) cudaFreeHost(h->qidx_h);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
@@ -271,38 +279,52 @@ extern "C" int adga_set_vertex(adga_handle *h, int iwb, const adga_z *chi_d, con
 }
 
 // ---------------------------------------------------------------------------
-// vertex ingest (read_vertex's transform, k_vertex.cu)
-static int vertex_g4(adga_handle *h, int iwb, int vtype, int W, int nineq, const int *ndims,
-                     const adga_z *g4d, const adga_z *g4m, z64 *outd, z64 *outm) {
-  const DevCtx &c = h->c;
-  if (!g4d || !g4m || !ndims || nineq < 1) return fail(h, ADGA_EINVAL, "vertex_g4: missing argument");
-  if (vtype < ADGA_VERTEX_FULL_G4 || vtype > ADGA_VERTEX_CHI_G4)
-    return fail(h, ADGA_EINVAL, "vertex_g4: unknown vertex type");
-  if (iwb < -c.iwb || iwb > c.iwb) return fail(h, ADGA_EINVAL, "vertex_g4: iwb out of range");
-  if (W < c.iwf) return fail(h, ADGA_EINVAL, "vertex_g4: iwfmax_g4 smaller than iwfmax_small");
-  if (c.nd > ADGA_MAX_BANDS) return fail(h, ADGA_EINVAL, "vertex_g4: more than ADGA_MAX_BANDS bands");
-  // index2cor (src/aux.f90:190-221): correlated bands of atom ineq start after
-  // all bands of the atoms before it
-  VertexAtoms atoms{};
+// index2cor (src/aux.f90:190-221): the correlated bands of atom ineq start
+// after all bands of the atoms before it; ndims(nineq, 2) in Fortran order
+static int make_atoms(adga_handle *h, int nineq, const int *ndims, VertexAtoms *atoms, const char *who) {
+  if (!ndims || nineq < 1) return fail(h, ADGA_EINVAL, std::string(who) + ": missing ndims");
+  if (h->c.nd > ADGA_MAX_BANDS) return fail(h, ADGA_EINVAL, std::string(who) + ": more than ADGA_MAX_BANDS bands");
+  *atoms = VertexAtoms{};
   int start = 0;
   for (int q = 0; q < nineq; ++q) {
     const int ncor = ndims[q], nunc = ndims[nineq + q];
-    if (ncor < 0 || nunc < 0) return fail(h, ADGA_EINVAL, "vertex_g4: negative band count");
-    for (int b = start; b < start + ncor && b < c.nd; ++b) atoms.a[b] = q + 1;
+    if (ncor < 0 || nunc < 0) return fail(h, ADGA_EINVAL, std::string(who) + ": negative band count");
+    for (int b = start; b < start + ncor && b < h->c.nd; ++b) atoms->a[b] = q + 1;
     start += ncor + nunc;
   }
-  if (start != c.nd) return fail(h, ADGA_EINVAL, "vertex_g4: ndims do not add up to ndim");
-  const size_t n = (size_t)c.nd2 * c.nd2 * (2 * (size_t)W) * (2 * (size_t)W);
+  if (start != h->c.nd) return fail(h, ADGA_EINVAL, std::string(who) + ": ndims do not add up to ndim");
+  return 0;
+}
+
+// upload two host arrays of n elements into the staging buffer (grown on demand)
+static int stage_pair(adga_handle *h, const adga_z *a, const adga_z *b, size_t n, const char *who) {
   if (h->g4cap < n) {
     if (h->g4buf) cudaFree(h->g4buf);
     h->g4buf = nullptr;
     h->g4cap = 0;
     if (cudaMalloc(&h->g4buf, 2 * n * sizeof(z64)) != cudaSuccess)
-      return fail(h, ADGA_ENOMEM, "vertex_g4: staging buffer");
+      return fail(h, ADGA_ENOMEM, std::string(who) + ": staging buffer");
     h->g4cap = n;
   }
-  CK(cudaMemcpyAsync(h->g4buf, g4d, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(h->g4buf + n, g4m, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->g4buf, a, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->g4buf + n, b, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  return 0;
+}
+
+// vertex ingest (read_vertex's transform, k_vertex.cu)
+static int vertex_g4(adga_handle *h, int iwb, int vtype, int W, int nineq, const int *ndims,
+                     const adga_z *g4d, const adga_z *g4m, z64 *outd, z64 *outm) {
+  const DevCtx &c = h->c;
+  if (!g4d || !g4m) return fail(h, ADGA_EINVAL, "vertex_g4: missing argument");
+  if (vtype < ADGA_VERTEX_FULL_G4 || vtype > ADGA_VERTEX_CHI_G4)
+    return fail(h, ADGA_EINVAL, "vertex_g4: unknown vertex type");
+  if (iwb < -c.iwb || iwb > c.iwb) return fail(h, ADGA_EINVAL, "vertex_g4: iwb out of range");
+  if (W < c.iwf) return fail(h, ADGA_EINVAL, "vertex_g4: iwfmax_g4 smaller than iwfmax_small");
+  VertexAtoms atoms{};
+  int r = make_atoms(h, nineq, ndims, &atoms, "vertex_g4");
+  if (r) return r;
+  const size_t n = (size_t)c.nd2 * c.nd2 * (2 * (size_t)W) * (2 * (size_t)W);
+  if ((r = stage_pair(h, g4d, g4m, n, "vertex_g4"))) return r;
   CK(launch_vertex_g4(c, iwb, vtype, W, atoms, h->g4buf, h->g4buf + n, outd, outm, h->st));
   return 0;
 }
@@ -350,6 +372,53 @@ extern "C" int adga_index2component_band(int nbands, int ind, int *b) {
   return 0;
 }
 
+extern "C" int adga_set_threeleg(adga_handle *h, int iwb, int n3iwf, int nineq, const int *ndims,
+                                 const adga_z *g3_dens, const adga_z *g3_magn) {
+  if (!h || !g3_dens || !g3_magn) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  if (iwb < -c.iwb || iwb > c.iwb) return fail(h, ADGA_EINVAL, "set_threeleg: iwb out of range");
+  if (n3iwf < c.iwf) return fail(h, ADGA_EINVAL, "set_threeleg: n3iwf smaller than iwfmax_small");
+  VertexAtoms atoms{};
+  int r = make_atoms(h, nineq, ndims, &atoms, "set_threeleg");
+  if (r) return r;
+  const int w = iwb + c.iwb;
+  const size_t ng = (size_t)c.nd2 * c.N;
+  if (!h->tl_d[w]) {
+    if (cudaMalloc(&h->tl_d[w], ng * sizeof(z64)) != cudaSuccess ||
+        cudaMalloc(&h->tl_m[w], ng * sizeof(z64)) != cudaSuccess)
+      return fail(h, ADGA_ENOMEM, "set_threeleg: gamma storage");
+  }
+  const size_t n = (size_t)c.nd2 * c.nd2 * 2 * (size_t)n3iwf;
+  if ((r = stage_pair(h, g3_dens, g3_magn, n, "set_threeleg"))) return r;
+  CK(launch_threeleg(c, iwb, n3iwf, atoms, h->g4buf, h->g4buf + n, h->tl_d[w], h->tl_m[w], h->st));
+  if (h->loc_iwb == iwb) h->loc_iwb = INT_MIN;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+extern "C" int adga_set_chi_loc_ext(adga_handle *h, int n2iwb, int nineq, const int *ndims,
+                                    const adga_z *chi_dens, const adga_z *chi_magn) {
+  if (!h || !chi_dens || !chi_magn) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  if (n2iwb < c.iwb) return fail(h, ADGA_EINVAL, "set_chi_loc_ext: n2iwb smaller than iwbmax_small");
+  VertexAtoms atoms{};
+  int r = make_atoms(h, nineq, ndims, &atoms, "set_chi_loc_ext");
+  if (r) return r;
+  const size_t nc = (size_t)h->nd4 * h->nw;
+  if (!h->ext_cld) {
+    if (cudaMalloc(&h->ext_cld, nc * sizeof(z64)) != cudaSuccess ||
+        cudaMalloc(&h->ext_clm, nc * sizeof(z64)) != cudaSuccess)
+      return fail(h, ADGA_ENOMEM, "set_chi_loc_ext: storage");
+  }
+  const size_t n = (size_t)h->nd4 * (2 * (size_t)n2iwb + 1);
+  if ((r = stage_pair(h, chi_dens, chi_magn, n, "set_chi_loc_ext"))) return r;
+  // read_chi_loc extends the bubble unless one impurity holds every band as correlated
+  const int extend = !(ndims[0] == c.nd);
+  CK(launch_chi_loc_ext(c, n2iwb, atoms, extend, h->g4buf, h->g4buf + n, h->ext_cld, h->ext_clm, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 static int ensure_diag(adga_handle *h, int iwb) {
   if (h->diag_iwb == iwb) return 0;
@@ -368,8 +437,17 @@ static int ensure_local(adga_handle *h, int iwb) {
   if (r) return r;
   CK(launch_local_F(h->c, h->vd[w], h->c0inv, h->Frow_d, h->st));
   CK(launch_local_F(h->c, h->vm[w], h->c0inv, h->Frow_m, h->st));
-  CK(launch_local_gamma(h->c, h->Frow_d, h->gam_d, h->opg_d, h->st));
-  CK(launch_local_gamma(h->c, h->Frow_m, h->gam_m, h->opg_m, h->st));
+  if (h->tl_d[w]) {
+    // external three-leg vertex (src/main.F90:560-561), then 1 + gamma^w
+    const size_t ng = (size_t)h->c.nd2 * h->c.N;
+    CK(cudaMemcpyAsync(h->gam_d, h->tl_d[w], ng * sizeof(z64), cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(h->gam_m, h->tl_m[w], ng * sizeof(z64), cudaMemcpyDeviceToDevice, h->st));
+    CK(launch_one_plus_gamma(h->c, h->gam_d, h->opg_d, h->st));
+    CK(launch_one_plus_gamma(h->c, h->gam_m, h->opg_m, h->st));
+  } else {
+    CK(launch_local_gamma(h->c, h->Frow_d, h->gam_d, h->opg_d, h->st));
+    CK(launch_local_gamma(h->c, h->Frow_m, h->gam_m, h->opg_m, h->st));
+  }
   h->loc_iwb = iwb;
   return 0;
 }
@@ -671,8 +749,8 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
     if (iq0 == 0) {
       if (do_chi)
         CK(launch_chi_loc_update(c, h->gam_d, h->gam_m, h->c0w, h->bubtmp,
-                                 h->chi_loc_d + (size_t)(iwb + c.iwb) * h->nd4,
-                                 h->chi_loc_m + (size_t)(iwb + c.iwb) * h->nd4,
+                                 h->ext_cld ? nullptr : h->chi_loc_d + (size_t)(iwb + c.iwb) * h->nd4,
+                                 h->ext_cld ? nullptr : h->chi_loc_m + (size_t)(iwb + c.iwb) * h->nd4,
                                  h->bubble_loc + (size_t)(iwb + c.iwb) * h->nd4, h->st));
       if (do_eom) {
         if (iwb == 0) CK(launch_eom_static(c, h->sigma_dmft, h->st));
@@ -754,8 +832,9 @@ extern "C" int adga_get_outputs(adga_handle *h, const adga_outputs *o) {
     DN(o->bubble_nl, h->bubble_nl, np * h->nd4);
   }
   DN(o->bubble_loc, h->bubble_loc, (size_t)h->nd4 * h->nw);
-  DN(o->chi_loc_dens, h->chi_loc_d, (size_t)h->nd4 * h->nw);
-  DN(o->chi_loc_magn, h->chi_loc_m, (size_t)h->nd4 * h->nw);
+  // an external chi_loc (read_chi_loc) replaces the one built from gamma^w
+  DN(o->chi_loc_dens, h->ext_cld ? h->ext_cld : h->chi_loc_d, (size_t)h->nd4 * h->nw);
+  DN(o->chi_loc_magn, h->ext_clm ? h->ext_clm : h->chi_loc_m, (size_t)h->nd4 * h->nw);
   DN(o->sigma_nl, h->sigma_nl, (size_t)c.nd2 * 2 * c.iwf * c.nkp_eom);
   DN(o->sigma_dmft, h->sigma_dmft, (size_t)c.nd2 * 2 * c.iwf);
   DN(o->sigma_hf, h->sigma_hf, (size_t)c.nd2 * c.nkp_eom);

@@ -53,6 +53,14 @@ cudaError_t launch_calc_chi_qw(const DevCtx &c, z64 *chi_qw, const z64 *interm3,
 cudaError_t launch_vertex_g4(const DevCtx &c, int iwb, int vtype, int W, const VertexAtoms &atoms,
                              const z64 *g4d, const z64 *g4m, z64 *chid, z64 *chim, cudaStream_t st);
 
+// k_vertex.cu: read_threeleg's transform into gamma^w (nd2 x N); 1 + gamma^w; read_chi_loc's
+// transform into chi_loc (nd2, nd2, 2 iwb + 1) per channel
+cudaError_t launch_threeleg(const DevCtx &c, int iwb, int n3iwf, const VertexAtoms &atoms, const z64 *g3d,
+                            const z64 *g3m, z64 *gd, z64 *gm, cudaStream_t st);
+cudaError_t launch_one_plus_gamma(const DevCtx &c, const z64 *gam, z64 *opg, cudaStream_t st);
+cudaError_t launch_chi_loc_ext(const DevCtx &c, int n2iwb, const VertexAtoms &atoms, int extend, const z64 *rd,
+                               const z64 *rm, z64 *od, z64 *om, cudaStream_t st);
+
 // k_postloop.cu: add_siw_dmft on sig (in place), then get_sigma_g_loc (sig_loc, gloc; full
 // k mesh) and get_ndga (n_dga_k, n_dga); null outputs are skipped
 cudaError_t launch_post_loop(const DevCtx &c, const int *keom, z64 *sig, z64 *sig_loc, z64 *gloc,

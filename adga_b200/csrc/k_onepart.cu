@@ -176,8 +176,10 @@ __global__ void k_chi_loc_update(DevCtx c, const z64 *gd, const z64 *gm, const z
     cfma(sm, gm[i1 + col], w);
   }
   double b2 = c.beta * c.beta;
-  cld[idx] = cadd(cld[idx], make_double2(sd.x / b2, sd.y / b2));
-  clm[idx] = cadd(clm[idx], make_double2(sm.x / b2, sm.y / b2));
+  if (cld) {   // null with an external chi_loc: only the bubble accumulates (src/main.F90:573)
+    cld[idx] = cadd(cld[idx], make_double2(sd.x / b2, sd.y / b2));
+    clm[idx] = cadd(clm[idx], make_double2(sm.x / b2, sm.y / b2));
+  }
   bub_loc[idx] = cadd(bub_loc[idx], bub_tmp[idx]);
 }
 

@@ -158,6 +158,34 @@ class Ladder:
                                                     ptr(d), ptr(m), ptr(od), ptr(om)), "vertex_transform")
         return od, om
 
+    def _ndims(self, ndims):
+        return np.asfortranarray(np.asarray(ndims if ndims is not None else [[self.ndim, 0]], dtype=np.int32))
+
+    def set_threeleg(self, iwb, g3_dens, g3_magn, ndims=None):
+        """external_threelegs (src/main.F90:560-561): read_threeleg's transform
+        (src/hdf5_module.f90:860-880) of g3(ndim, ndim, ndim, ndim, 2*n3iwf) on
+        the GPU; the result replaces gamma^w of omega = iwb."""
+        nd = self.ndim
+        n3 = np.asarray(g3_dens).shape[4] // 2
+        shape = (nd, nd, nd, nd, 2 * n3)
+        d, m = _z(g3_dens, shape), _z(g3_magn, shape)
+        nd_arr = self._ndims(ndims)
+        self._check(self._lib.adga_set_threeleg(self._h, int(iwb), n3, nd_arr.shape[0], ptr(nd_arr),
+                                                ptr(d), ptr(m)), "set_threeleg")
+
+    def set_chi_loc_ext(self, chi_dens, chi_magn, ndims=None):
+        """external_chi_loc (src/main.F90:407-411): read_chi_loc's transform
+        (src/hdf5_module.f90:958-993) of chi(ndim, ndim, ndim, ndim, 2*n2iwb+1)
+        on the GPU; the chi_loc outputs are these from now on."""
+        nd = self.ndim
+        n2 = (np.asarray(chi_dens).shape[4] - 1) // 2
+        shape = (nd, nd, nd, nd, 2 * n2 + 1)
+        d, m = _z(chi_dens, shape), _z(chi_magn, shape)
+        nd_arr = self._ndims(ndims)
+        self._check(self._lib.adga_set_chi_loc_ext(self._h, n2, nd_arr.shape[0], ptr(nd_arr), ptr(d), ptr(m)),
+                    "set_chi_loc_ext")
+        self.ext_chi_loc = True
+
     def reset_outputs(self):
         self._check(self._lib.adga_reset_outputs(self._h), "reset_outputs")
 
@@ -198,8 +226,11 @@ class Ladder:
         add_siw_dmft, src/eom_module.f90:237-251)."""
         qs, _ = self.last_range
         widx = (np.arange(qs, qs + self.last_npts) - 1) // self.nqp
-        cld = out["chi_loc_dens"] + out["bubble_loc"]
-        clm = out["chi_loc_magn"] + out["bubble_loc"]
+        if getattr(self, "ext_chi_loc", False):     # external chi_loc holds the bubble already
+            cld, clm = out["chi_loc_dens"], out["chi_loc_magn"]
+        else:
+            cld = out["chi_loc_dens"] + out["bubble_loc"]
+            clm = out["chi_loc_magn"] + out["bubble_loc"]
         chi_d = out["chi_qw_dens"] + out["bubble_nl"] + cld[:, :, widx]
         chi_m = out["chi_qw_magn"] + out["bubble_nl"] + clm[:, :, widx]
         sig = out["sigma_nl"].copy(order="F")

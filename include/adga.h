@@ -116,6 +116,29 @@ int adga_vertex_transform(adga_handle *h, int iwb, int vertex_type, int iwfmax_g
                           const int *ndims, const adga_z *g4_dens, const adga_z *g4_magn,
                           adga_z *chi_loc_dens, adga_z *chi_loc_magn);
 
+/*
+ * External three-leg vertex (external_threelegs, src/main.F90:560-561):
+ * read_threeleg's transform (src/hdf5_module.f90:860-880) on the device.
+ * g3_dens / g3_magn: g3(ndim, ndim, ndim, ndim, 2*n3iwf) as w2dynamics stores
+ * it for omega = iwb (Matsubara -n3iwf..n3iwf-1, before the beta factor of
+ * :829,838), n3iwf >= iwfmax_small.  The resulting gamma^w(ndim2, maxdim)
+ * replaces the sum over the F~ rows for that omega (1+gamma^w follows);
+ * adga_get_gamma_w returns it.  nineq / ndims as for adga_set_vertex_g4.
+ */
+int adga_set_threeleg(adga_handle *h, int iwb, int n3iwf, int nineq, const int *ndims,
+                      const adga_z *g3_dens, const adga_z *g3_magn);
+
+/*
+ * External local susceptibility (external_chi_loc, src/main.F90:407-411):
+ * read_chi_loc's transform (src/hdf5_module.f90:958-993) on the device.
+ * chi_dens / chi_magn: chi(ndim, ndim, ndim, ndim, 2*n2iwb+1) (bosonic
+ * -n2iwb..n2iwb, n2iwb >= iwbmax_small).  From then on the handle's chi_loc
+ * outputs are these (the loop no longer builds them from gamma^w, and the
+ * local bubble is not added at assembly, src/main.F90:933-936).
+ */
+int adga_set_chi_loc_ext(adga_handle *h, int n2iwb, int nineq, const int *ndims,
+                         const adga_z *chi_dens, const adga_z *chi_magn);
+
 /* index2component_band (src/aux.f90:169-186): the 1-based band pattern
  * b[0..3] of a 1-based vertex group index ind over nbands bands (the group
  * names of the w2dynamics vertex file).  Host only; returns 0 or ADGA_EINVAL. */

@@ -365,6 +365,12 @@ class LadderInputs:
     do_eom: bool = True
     bubble_big_box: bool = False  # "[Debug] Bubble" (src/config_module.f90:467-477)
     iw_data: Optional[np.ndarray] = None
+    # external_threelegs: iwb -> (gamma_d, gamma_m) (ndim2, maxdim) as read_threeleg
+    # returns them (src/main.F90:560-561); None = gamma^w from F~ (:563-570)
+    threeleg: Optional[Callable[[int], Tuple[np.ndarray, np.ndarray]]] = None
+    # external_chi_loc: (chi_loc_dens, chi_loc_magn) (ndim2, ndim2, 2*iwb+1) as
+    # read_chi_loc returns them (src/main.F90:407-411); None = built from gamma^w
+    chi_loc_ext: Optional[Tuple[np.ndarray, np.ndarray]] = None
 
     def __post_init__(self):
         if self.iw_data is None:
@@ -613,13 +619,16 @@ class Oracle:
         Fm *= scale[None, :]
         Fd[np.arange(N), np.arange(N)] -= 1.0
         Fm[np.arange(N), np.arange(N)] -= 1.0
-        # gamma^w (main.F90:564-570)
-        gd = np.zeros((nd2, N), complex, order="F")
-        gm = np.zeros((nd2, N), complex, order="F")
-        for dum in range(2 * iwfs):
-            gd += Fd[dum * nd2:(dum + 1) * nd2, :]
-            gm += Fm[dum * nd2:(dum + 1) * nd2, :]
-        if iq == 0 and inp.do_chi:
+        # gamma^w (main.F90:559-571): external three-leg vertex or the F~ row sums
+        if inp.threeleg is not None:
+            gd, gm = (np.array(x, dtype=complex, order="F") for x in inp.threeleg(iwb))
+        else:
+            gd = np.zeros((nd2, N), complex, order="F")
+            gm = np.zeros((nd2, N), complex, order="F")
+            for dum in range(2 * iwfs):
+                gd += Fd[dum * nd2:(dum + 1) * nd2, :]
+                gm += Fm[dum * nd2:(dum + 1) * nd2, :]
+        if iq == 0 and inp.do_chi and inp.chi_loc_ext is None:
             self.calc_chi_qw(out["chi_loc_dens"][:, :, iwb + iwbs], gd, chi0w)
             self.calc_chi_qw(out["chi_loc_magn"][:, :, iwb + iwbs], gm, chi0w)
         opgd = gd.copy(order="F")
@@ -690,8 +699,12 @@ def assemble(inp: LadderInputs, out):
     chi(q,w) = chi_nl + bubble_nl + chi_loc(w) (main.F90:1050,1059-1063,1127,1136-1140);
     Sigma = Sigma_nl + siw on the diagonal (add_siw_dmft, src/eom_module.f90:237-251)."""
     iwbs, iwfs, nd = inp.iwbmax_small, inp.iwfmax_small, inp.ndim
-    chi_loc_d = out["chi_loc_dens"] + out["bubble_loc"]
-    chi_loc_m = out["chi_loc_magn"] + out["bubble_loc"]
+    if inp.chi_loc_ext is not None:   # read from file: already contains the bubble (main.F90:933-936)
+        chi_loc_d = np.asarray(inp.chi_loc_ext[0])
+        chi_loc_m = np.asarray(inp.chi_loc_ext[1])
+    else:
+        chi_loc_d = out["chi_loc_dens"] + out["bubble_loc"]
+        chi_loc_m = out["chi_loc_magn"] + out["bubble_loc"]
     qw = out["qw"]
     widx = qw[:, 0] + iwbs
     chi_d = out["chi_qw_dens"] + out["bubble_nl"] + chi_loc_d[:, :, widx]
@@ -755,3 +768,78 @@ def post_loop(inp: LadderInputs, sigma_sum, k_data_eom=None):
     out["n_dga_k"] = np.asfortranarray(nk)
     out["n_dga"] = np.array([nk[:, i, i].sum() for i in range(nd)]) / nk_eom
     return out
+
+
+def read_threeleg_transform(g3_dens, g3_magn, iwb, ndims, giw, n_dmft, beta, iwf, iwmax):
+    """The transform part of read_threeleg (src/hdf5_module.f90:820-880): the
+    three-leg vertex g3(ndim, ndim, ndim, ndim, 2*n3iwf) as w2dynamics stores it
+    (index m + n3iwf holds Matsubara m, before the beta factor of :829,838) ->
+    gamma^w(ndim2, maxdim) with the disconnected parts and the division by
+    -G G in the correlated subspace."""
+    nd = g3_dens.shape[0]
+    n3iwf = g3_dens.shape[4] // 2
+    nd2 = nd * nd
+    gtd = np.asarray(g3_dens) * beta
+    gtm = np.asarray(g3_magn) * beta
+    gd = np.zeros((nd2, nd2 * 2 * iwf), complex)
+    gm = np.zeros((nd2, nd2 * 2 * iwf), complex)
+    g = lambda n, b: giw[n + iwmax, b]
+    i1 = 0
+    for i in range(nd):
+        for j in range(nd):
+            i2 = 0
+            for w in range(2 * iwf):
+                nu = w - iwf
+                for k in range(nd):
+                    for l in range(nd):
+                        c4 = _index2cor(ndims, i + 1, j + 1, k + 1, l + 1)
+                        vd = gtd[k, l, j, i, n3iwf + w - iwf]
+                        vm = gtm[k, l, j, i, n3iwf + w - iwf]
+                        if i == j and k == l and iwb == 0 and c4:
+                            vd = vd + 2.0 * beta * (1.0 - n_dmft[i]) * g(nu, k)
+                        if i == k and j == l and c4:
+                            t = g(nu, k) * g(nu - iwb, l)
+                            vd = vd + t
+                            vm = vm + t
+                        if c4:
+                            den = -1.0 * g(nu, k) * g(nu - iwb, l)
+                            vd = vd / den
+                            vm = vm / den
+                        gd[i1, i2] = vd
+                        gm[i1, i2] = vm
+                        i2 += 1
+            i1 += 1
+    return np.asfortranarray(gd), np.asfortranarray(gm)
+
+
+def read_chi_loc_transform(chi_raw, channel, ndims, giw, n_dmft, beta, iwbs, iwmax):
+    """The transform part of read_chi_loc (src/hdf5_module.f90:958-993): the
+    frequency-summed local susceptibility chi(ndim, ndim, ndim, ndim, 2*n2iwb+1)
+    as w2dynamics stores it (index m + n2iwb holds bosonic m) -> chi_loc(ndim2,
+    ndim2, -iwbs:iwbs) with the dens-channel omega = 0 term and, when the model
+    has more than one impurity or uncorrelated bands, the lattice bubble of the
+    uncorrelated legs."""
+    nd = chi_raw.shape[0]
+    n2iwb = chi_raw.shape[4] // 2
+    nd2 = nd * nd
+    extend = not (len(ndims) >= 1 and ndims[0][0] == nd)
+    sl = np.asarray(chi_raw)[..., n2iwb - iwbs:n2iwb + iwbs + 1]
+    out = np.zeros((nd2, nd2, 2 * iwbs + 1), complex)
+    g = lambda n, b: giw[n + iwmax, b]
+    i1 = 0
+    for i in range(nd):
+        for j in range(nd):
+            i2 = 0
+            for k in range(nd):
+                for l in range(nd):
+                    out[i1, i2, :] = sl[i, j, l, k, :]
+                    c4 = _index2cor(ndims, i + 1, j + 1, k + 1, l + 1)
+                    if c4 and i == j and k == l and channel == "dens":
+                        out[i1, i2, iwbs] -= 2.0 * beta * (1.0 - n_dmft[i]) * (1.0 - n_dmft[k])
+                    if extend and not c4 and i == k and j == l:
+                        for w in range(-iwbs, iwbs + 1):
+                            for n in range(-iwmax + iwbs, iwmax - iwbs):
+                                out[i1, i2, w + iwbs] -= g(n, i) * g(n - w, j) / beta
+                    i2 += 1
+            i1 += 1
+    return np.asfortranarray(out)
