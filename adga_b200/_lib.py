@@ -23,6 +23,7 @@ EXPORTS = [
     "adga_inverse_matrix_z", "adga_index_kq", "adga_generate_q_vol", "adga_create_u",
     "adga_inverse_matrix_z_noalloc", "adga_set_vertex_g4", "adga_vertex_transform",
     "adga_index2component_band", "adga_post_loop", "adga_set_threeleg", "adga_set_chi_loc_ext",
+    "adga_set_vq",
 ]
 
 
@@ -94,6 +95,7 @@ def load():
         "adga_post_loop": [vp, vp, vp, vp, vp, vp],
         "adga_set_threeleg": [vp, i, i, i, vp, vp, vp],
         "adga_set_chi_loc_ext": [vp, i, i, vp, vp, vp],
+        "adga_set_vq": [vp, vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -45,6 +45,9 @@ struct adga_handle {
   size_t g4cap = 0;
   std::vector<z64 *> tl_d, tl_m;   // external three-leg gamma^w per omega (nd2 x N), or null
   z64 *ext_cld = nullptr, *ext_clm = nullptr;   // external chi_loc (nd2, nd2, nw), or null
+  z64 *vq_d = nullptr, *nfock_d = nullptr;       // V(q) and n_fock (do_vq), or null
+  z64 *vq_extra = nullptr;                        // density-channel V(q) residual term (mixed)
+  size_t vq_extra_cap = 0;
   // local block
   int diag_iwb = INT_MIN, loc_iwb = INT_MIN;
   z64 *c0inv = nullptr, *c0w = nullptr, *bubtmp = nullptr;
@@ -229,6 +232,9 @@ extern "C" int adga_destroy(adga_handle *h) {
   for (auto p : h->tl_m) if (p) cudaFree(p);
   if (h->ext_cld) cudaFree(h->ext_cld);
   if (h->ext_clm) cudaFree(h->ext_clm);
+  if (h->vq_d) cudaFree(h->vq_d);
+  if (h->nfock_d) cudaFree(h->nfock_d);
+  if (h->vq_extra) cudaFree(h->vq_extra);
   if (h->qidx_h) cudaFreeHost(h->qidx_h);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
@@ -419,6 +425,36 @@ extern "C" int adga_set_chi_loc_ext(adga_handle *h, int n2iwb, int nineq, const 
   return 0;
 }
 
+extern "C" int adga_set_vq(adga_handle *h, const adga_z *vq) {
+  if (!h) return ADGA_EINVAL;
+  DevCtx &c = h->c;
+  if (!vq) {                    // switch the non-local interaction off
+    c.vq = nullptr;
+    c.nfock = nullptr;
+    h->loc_iwb = INT_MIN;
+    return 0;
+  }
+  if (c.nd > GINV_MAXND_HOST) return fail(h, ADGA_EINVAL, "set_vq: ndim above 8");
+  const size_t nv = (size_t)h->nd4 * c.nqp;
+  if (!h->vq_d) {
+    if (cudaMalloc(&h->vq_d, nv * sizeof(z64)) != cudaSuccess ||
+        cudaMalloc(&h->nfock_d, (size_t)c.nkp * c.nd2 * sizeof(z64)) != cudaSuccess)
+      return fail(h, ADGA_ENOMEM, "set_vq: storage");
+  }
+  z64 *raw = nullptr;
+  if (cudaMalloc(&raw, nv * sizeof(z64)) != cudaSuccess) return fail(h, ADGA_ENOMEM, "set_vq: staging");
+  cudaError_t e = cudaMemcpyAsync(raw, vq, nv * sizeof(z64), cudaMemcpyHostToDevice, h->st);
+  if (e == cudaSuccess) e = launch_vq_permute(c.nd, c.nqp, raw, h->vq_d, h->st);
+  if (e == cudaSuccess) e = launch_nfock(c, h->nfock_d, h->st);      // get_nfock
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(raw);
+  if (e != cudaSuccess) return fail(h, ADGA_ECUDA, std::string("set_vq: ") + cudaGetErrorString(e));
+  c.vq = h->vq_d;
+  c.nfock = h->nfock_d;
+  h->loc_iwb = INT_MIN;
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 static int ensure_diag(adga_handle *h, int iwb) {
   if (h->diag_iwb == iwb) return 0;
@@ -599,7 +635,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   if (prec == ADGA_FP64) {
     z64 *T = (z64 *)h->Tm;
     CK(launch_bse_build<z64>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
-                             strideM, h->gq, st));
+                             strideM, h->gq, h->qidx_d, st));
     cudaEventRecord(ev[2], st);
     CK(factor_batch<z64>(h, T, lb, false, false, &tt));
     CK(lu_backsolve<z64>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
@@ -607,7 +643,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   } else {
     z32 *T = (z32 *)h->Tm;
     CK(launch_bse_build<z32>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
-                             strideM, h->gq, st));
+                             strideM, h->gq, h->qidx_d, st));
     cudaEventRecord(ev[2], st);
     CK(factor_batch<z32>(h, T, lb, true, h->tc != nullptr, &tt));
     CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
@@ -620,8 +656,22 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     std::vector<char> conv(nmat, 0);
     for (int it = 0; it < h->max_iter; ++it) {
       CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
+      z64 *extra = nullptr;
+      if (c.vq) {     // density-channel V(q) term of the residual
+        const size_t ne = (size_t)np * c.nd2 * c.N;
+        if (h->vq_extra_cap < ne) {
+          if (h->vq_extra) cudaFree(h->vq_extra);
+          h->vq_extra = nullptr;
+          h->vq_extra_cap = 0;
+          if (cudaMalloc(&h->vq_extra, ne * sizeof(z64)) != cudaSuccess)
+            return fail(h, ADGA_ENOMEM, "V(q) residual buffer");
+          h->vq_extra_cap = ne;
+        }
+        extra = h->vq_extra;
+        CK(launch_vq_resid_extra(c, np, h->qidx_d, h->X64, chi0q, h->opg_d, extra, st));
+      }
       CK(launch_residual(c, np, h->X64, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m,
-                         h->XD, h->V32, st));
+                         h->XD, h->V32, extra, st));
       CK(lu_fwdsolve_ws<z32>(T, lb, h->V32, per, (int)N, (int)R, h->work32, st));
       CK(lu_backsolve<z32>(T, lb, h->V32, per, (int)N, (int)R, st));
       CK(launch_update((int)per, nmat, h->V32, h->X64, h->norms, nullptr, st));
@@ -650,7 +700,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   cudaEventRecord(ev[3], st);
   CK(launch_post(c, np, X, sp, sc, (int)N, h->opg_d, h->opg_m, h->gam_d, h->gam_m, h->gq, chi0q,
                  h->c0w, chi_qw_d + (size_t)off * h->nd4, chi_qw_m + (size_t)off * h->nd4,
-                 do_eom ? h->mtot : nullptr, h->etad, h->etam, st));
+                 do_eom ? h->mtot : nullptr, h->etad, h->etam, h->qidx_d, st));
   for (int p : fallback)    // their EOM contribution comes from the FP64 re-solve below
     CK(cudaMemsetAsync(h->mtot + (size_t)p * c.nd2 * c.iwf * c.nd2, 0,
                        sizeof(z64) * c.nd2 * c.iwf * c.nd2, st));
@@ -760,6 +810,10 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
     for (int b0 = 0; b0 < seg; b0 += h->cap) {
       const int nb = std::min(h->cap, seg - b0);
       for (int i = 0; i < nb; ++i) h->qidx_h[i] = iq0 + b0 + i;
+      if (do_eom && iwb == 0 && c.vq) {   // calc_eom_static's V(q) terms, every q (src/main.F90:635-637)
+        CK(cudaMemcpyAsync(h->qidx_d, h->qidx_h, sizeof(int) * nb, cudaMemcpyHostToDevice, h->st));
+        CK(launch_eom_static_vq(c, h->qidx_d, nb, h->sigma_hf, h->st));
+      }
       r = run_batch(h, iwb, nb, p + b0, precision, status, h->chi_qw_d, h->chi_qw_m, h->bubble_nl,
                     do_eom, do_chi);
       if (r) return r;
@@ -997,11 +1051,18 @@ extern "C" int adga_calc_eom_dynamic(adga_handle *h, const adga_z *etaqd, const 
   if (e == cudaSuccess) e = cudaMemsetAsync(chi0z, 0, sizeof(z64) * h->nd4 * 2 * c.iwf, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h->gq, gammaqd, sizeof(z64) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sig, sigma_nl, sizeof(z64) * ns, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = launch_post(c, 1, X, 2 * n, n, c.N, opz, opz, opz, opz, h->gq, chi0z, h->c0w, scr, scr + h->nd4,
-                    h->mtot, h->etad, h->etam, st);
   h->qidx_h[0] = iq - 1;
   if (e == cudaSuccess) e = cudaMemcpyAsync(h->qidx_d, h->qidx_h, sizeof(int), cudaMemcpyHostToDevice, st);
+  // with V(q), m_tot also needs gamma^w_d of this omega (src/eom_module.f90:202-205)
+  const z64 *gwd = opz;
+  if (e == cudaSuccess && c.vq) {
+    int rl = ensure_local(h, iwb);
+    if (rl) { free_list(tmp); return rl; }
+    gwd = h->gam_d;
+  }
+  if (e == cudaSuccess)
+    e = launch_post(c, 1, X, 2 * n, n, c.N, opz, opz, gwd, opz, h->gq, chi0z, h->c0w, scr, scr + h->nd4,
+                    h->mtot, h->etad, h->etam, h->qidx_d, st);
   if (e == cudaSuccess) e = launch_eom_dynamic(c, iwb, h->qidx_d, 1, h->mtot, sig, st);
   if (e == cudaSuccess) e = launch_mirror_sigma(c, sig, c.nkp_eom, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sigma_nl, sig, sizeof(z64) * ns, cudaMemcpyDeviceToHost, st);

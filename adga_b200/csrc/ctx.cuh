@@ -21,6 +21,8 @@ struct DevCtx {
   const int *kq;                 // k-q index, 0-based, (nkp, nqp)
   const int *kqe;                // EOM k-q index, 0-based, (nkp_eom, nqp)
   const int *keom;               // EOM k-points (k_data_eom, 1-based), null for the full mesh
+  const z64 *vq;                 // V(q) (nd2, nd2, nqp) in read_vq's layout, null without do_vq
+  const z64 *nfock;              // n_fock(k, i, j) (nkp, nd, nd), with vq
   const z64 *gtab;               // G(k, nu): [(nu - nu_lo)*nkp + k][nd2], column-major nd x nd
 };
 
@@ -66,6 +68,14 @@ cudaError_t launch_chi_loc_ext(const DevCtx &c, int n2iwb, const VertexAtoms &at
 cudaError_t launch_post_loop(const DevCtx &c, const int *keom, z64 *sig, z64 *sig_loc, z64 *gloc,
                              z64 *n_dga_k, z64 *n_dga, cudaStream_t st);
 
+cudaError_t launch_nfock(const DevCtx &c, z64 *nfock, cudaStream_t st);
+
+// k_vq.cu: V(q) (do_vq)
+cudaError_t launch_vq_permute(int nd, int nqp, const z64 *raw, z64 *v, cudaStream_t st);
+cudaError_t launch_eom_static_vq(const DevCtx &c, const int *qidx, int npts, z64 *sigma_hf, cudaStream_t st);
+cudaError_t launch_vq_resid_extra(const DevCtx &c, int npts, const int *qidx, const z64 *X, const z64 *chi0q,
+                                  const z64 *opg_d, z64 *extra, cudaStream_t st);
+
 // k_chi0.cu: chi0q[p] (nd2, nd2, nnu_out) for a batch of points at one omega
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,
                         int nnu_all, cudaStream_t st);
@@ -77,12 +87,12 @@ template <typename T>
 cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const z64 *c0inv,
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, T *Tmat, size_t strideM, z64 *gammaqd,
-                             cudaStream_t st);
+                             const int *qidx, cudaStream_t st);
 // X of point p, channel ch at X + p*sp + ch*sc: N x R column-major (ld ldX)
 cudaError_t launch_post(const DevCtx &c, int npts, const z64 *X, size_t sp, size_t sc, int ldX,
                         const z64 *opg_d, const z64 *opg_m, const z64 *gam_d, const z64 *gam_m,
                         const z64 *gammaqd, const z64 *chi0q, const z64 *c0w, z64 *chi_qw_d,
-                        z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam, cudaStream_t st);
+                        z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam, const int *qidx, cudaStream_t st);
 cudaError_t launch_eom_dynamic(const DevCtx &c, int iwb, const int *qidx, int npts,
                                const z64 *mtot, z64 *sigma_nl, cudaStream_t st);
 
@@ -90,6 +100,7 @@ cudaError_t launch_eom_dynamic(const DevCtx &c, int iwb, const int *qidx, int np
 cudaError_t launch_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X, cudaStream_t st);
 cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q,
                             const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
-                            const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, cudaStream_t st);
+                            const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, const z64 *extra_d,
+                            cudaStream_t st);
 cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,
                           const int *active, cudaStream_t st);

@@ -20,8 +20,9 @@ __global__ void __launch_bounds__(128)
 k_bse_build(DevCtx c, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0inv,
             const z64 *__restrict__ Frow_d, const z64 *__restrict__ Frow_m,
             const z64 *__restrict__ opg_d, const z64 *__restrict__ opg_m, T *Tm, size_t strideM,
-            z64 *gammaqd) {
+            z64 *gammaqd, const int *__restrict__ qidx) {
   __shared__ z64 sw[ND2 * ND2];
+  __shared__ z64 sv[ND2 * ND2];   // 2 beta^-2 chi0^q(nu) v(q), density channel with V(q)
   const int N = c.N;
   const int cc = blockIdx.x * blockDim.x + threadIdx.x;
   const int ch = blockIdx.y, p = blockIdx.z;
@@ -32,6 +33,12 @@ k_bse_build(DevCtx c, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0i
   z64 gq[ND2];
 #pragma unroll
   for (int a = 0; a < ND2; ++a) gq[a] = make_double2(0.0, 0.0);
+  const bool vterm = c.vq && ch == 0;
+  const z64 *vq = vterm ? c.vq + (size_t)qidx[p] * ND2 * ND2 : nullptr;
+  z64 og[ND2];                      // (1 + gamma^w_d)(:, cc)
+  if (vterm && cc < N)
+#pragma unroll
+    for (int i3 = 0; i3 < ND2; ++i3) og[i3] = opg_d[i3 + (size_t)cc * ND2];
   for (int dum = 0; dum < 2 * c.iwf; ++dum) {
     __syncthreads();
     for (int e = threadIdx.x; e < ND2 * ND2; e += blockDim.x) {
@@ -39,6 +46,12 @@ k_bse_build(DevCtx c, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0i
       z64 v = cmul(c0[(size_t)dum * ND2 * ND2 + e], c0inv[dum * ND2 + i3]);
       if (i1 == i3) v.x -= 1.0;
       sw[e] = v;                       // sw(i1, i3) at i1 + i3*nd2
+      if (vterm) {                     // src/main.F90:710-719
+        z64 t = make_double2(0.0, 0.0);
+        for (int m = 0; m < ND2; ++m) cfma(t, c0[(size_t)dum * ND2 * ND2 + i1 + m * ND2], vq[m + i3 * ND2]);
+        const double f = 2.0 / (c.beta * c.beta);
+        sv[e] = make_double2(f * t.x, f * t.y);
+      }
     }
     __syncthreads();
     if (cc < N) {
@@ -52,6 +65,9 @@ k_bse_build(DevCtx c, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0i
         for (int i3 = 0; i3 < ND2; ++i3) cfma(w, sw[i1 + i3 * ND2], f[i3]);
         int r = i1 + dum * ND2;
         z64 t = make_double2(-w.x, -w.y);
+        if (vterm)
+#pragma unroll
+          for (int i3 = 0; i3 < ND2; ++i3) cfms(t, sv[i1 + i3 * ND2], og[i3]);
         if (r == cc) t.x += 1.0;
         Tp[cc + (size_t)r * N] = from64<T>(t);
         if (ch == 0) gq[i1] = cadd(gq[i1], w);
@@ -73,12 +89,12 @@ template <typename T>
 cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const z64 *c0inv,
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, T *Tmat, size_t strideM, z64 *gammaqd,
-                             cudaStream_t st) {
+                             const int *qidx, cudaStream_t st) {
   if (npts <= 0) return cudaSuccess;
   dim3 grid(cdiv_u(c.N, 128), 2, npts);
 #define BUILD(NDD)                                                                            \
   k_bse_build<T, NDD><<<grid, 128, 0, st>>>(c, chi0q, c0inv, Frow_d, Frow_m, opg_d, opg_m,     \
-                                            Tmat, strideM, gammaqd)
+                                            Tmat, strideM, gammaqd, qidx)
   switch (c.nd2) {
     case 1: BUILD(1); break;
     case 4: BUILD(4); break;
@@ -92,10 +108,10 @@ cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const 
 }
 template cudaError_t launch_bse_build<z64>(const DevCtx &, int, const z64 *, const z64 *,
                                            const z64 *, const z64 *, const z64 *, const z64 *,
-                                           z64 *, size_t, z64 *, cudaStream_t);
+                                           z64 *, size_t, z64 *, const int *, cudaStream_t);
 template cudaError_t launch_bse_build<z32>(const DevCtx &, int, const z64 *, const z64 *,
                                            const z64 *, const z64 *, const z64 *, const z64 *,
-                                           z32 *, size_t, z64 *, cudaStream_t);
+                                           z32 *, size_t, z64 *, const int *, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // post: one block per point.
@@ -108,7 +124,7 @@ __global__ void __launch_bounds__(256)
 k_post(DevCtx c, const z64 *__restrict__ X, size_t sp, size_t sc, int ldX, const z64 *__restrict__ opg_d,
        const z64 *__restrict__ opg_m, const z64 *__restrict__ gam_d, const z64 *__restrict__ gam_m,
        const z64 *__restrict__ gammaqd, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0w,
-       z64 *chi_qw_d, z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam) {
+       z64 *chi_qw_d, z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam, const int *__restrict__ qidx) {
   const int p = blockIdx.x;
   const int N = c.N, nd2 = c.nd2, iwf = c.iwf;
   const size_t nd2N = (size_t)nd2 * N;
@@ -149,22 +165,27 @@ k_post(DevCtx c, const z64 *__restrict__ X, size_t sp, size_t sc, int ldX, const
   // 3. m_tot for the nu >= 0 half of the columns
   if (mtot) {
     const double inv = 1.0 / c.beta / (double)c.nqp;
+    // V(q) terms of m_tot (src/eom_module.f90:187-205)
+    const z64 *vq = (c.vq && qidx) ? c.vq + (size_t)qidx[p] * nd2 * nd2 : nullptr;
     const z64 *gq = gammaqd + (size_t)p * nd2N;
     z64 *m = mtot + (size_t)p * nd2 * iwf * nd2;
     for (int t = threadIdx.x; t < nd2 * iwf * nd2; t += blockDim.x) {
       int i1 = t % nd2, cl = t / nd2;          // local column
       size_t col = (size_t)(cl + iwf * nd2) * nd2;
-      z64 a1 = make_double2(0.0, 0.0), a2 = a1, a3 = a1;
+      z64 a1 = make_double2(0.0, 0.0), a2 = a1, a3 = a1, a4 = a1;
       for (int i3 = 0; i3 < nd2; ++i3) {
         z64 uu = c.u[i1 + i3 * nd2], tt = c.ut[i1 + i3 * nd2];
         z64 uw = make_double2(uu.x - 0.5 * tt.x, uu.y - 0.5 * tt.y);
+        if (vq) uw = cadd(vq[i1 + i3 * nd2], uw);       // u_work = v + u - u~/2
         cfma(a1, uw, ed[i3 + col]);
         cfma(a2, tt, em[i3 + col]);
         cfma(a3, uu, gq[i3 + col]);
+        if (vq) cfma(a4, vq[i1 + i3 * nd2], gam_d[i3 + col]);   // v gamma^w_d
       }
       z64 v = cscale(a1, -inv);
       v = cadd(cscale(a2, 1.5 * inv), v);
       v = cadd(cscale(a3, inv), v);
+      if (vq) v = cadd(cscale(a4, -inv), v);
       m[t] = v;
     }
   }
@@ -173,10 +194,10 @@ k_post(DevCtx c, const z64 *__restrict__ X, size_t sp, size_t sc, int ldX, const
 cudaError_t launch_post(const DevCtx &c, int npts, const z64 *X, size_t sp, size_t sc, int ldX,
                         const z64 *opg_d, const z64 *opg_m, const z64 *gam_d, const z64 *gam_m,
                         const z64 *gammaqd, const z64 *chi0q, const z64 *c0w, z64 *chi_qw_d,
-                        z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam, cudaStream_t st) {
+                        z64 *chi_qw_m, z64 *mtot, z64 *etad, z64 *etam, const int *qidx, cudaStream_t st) {
   if (npts <= 0) return cudaSuccess;
   k_post<<<npts, 256, 0, st>>>(c, X, sp, sc, ldX, opg_d, opg_m, gam_d, gam_m, gammaqd, chi0q, c0w,
-                               chi_qw_d, chi_qw_m, mtot, etad, etam);
+                               chi_qw_d, chi_qw_m, mtot, etad, etam, qidx);
   return ADGA_LAUNCH_CHECK();
 }
 

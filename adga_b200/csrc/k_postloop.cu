@@ -97,17 +97,20 @@ __global__ void __launch_bounds__(256) k_gloc(DevCtx c, const z64 *sig, z64 *glo
   }
 }
 
-// n_dga_k(ik, i, j) (Fortran order, complex with zero imaginary part)
-__global__ void __launch_bounds__(128) k_ndga_k(DevCtx c, const int *keom, const z64 *sig, z64 *nk) {
+// occupation n(ik, i, j) = 2/beta sum_{nu>=0} Re G(k, nu) + 1/2 delta_ij over nk k-points
+// (Fortran order, complex with zero imaginary part): n_dga_k with the DGA Sigma inside
+// the box (get_ndga), or n_fock with the DMFT siw everywhere when sig is null (get_nfock,
+// src/one_particle_quant_module.f90:316-342)
+__global__ void __launch_bounds__(128) k_occ(DevCtx c, int nkk, const int *keom, const z64 *sig, z64 *nk) {
   const int ik = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ik >= c.nkp_eom) return;
+  if (ik >= nkk) return;
   const int nd = c.nd, nd2 = c.nd2;
   const int kfull = keom ? keom[ik] - 1 : ik;
   double acc[PL_MAXND * PL_MAXND];
   for (int e = 0; e < nd2; ++e) acc[e] = 0.0;
   for (int nu = 0; nu < c.iwmax; ++nu) {
     z64 a[PL_MAXND * PL_MAXND];
-    const z64 *s = nu < c.iwf ? sig + (size_t)nd2 * ((size_t)(nu + c.iwf) + 2 * (size_t)c.iwf * ik) : nullptr;
+    const z64 *s = (sig && nu < c.iwf) ? sig + (size_t)nd2 * ((size_t)(nu + c.iwf) + 2 * (size_t)c.iwf * ik) : nullptr;
     pl_gk(c, kfull, nu, s, a);
     for (int e = 0; e < nd2; ++e) acc[e] += a[e].x;
   }
@@ -115,7 +118,7 @@ __global__ void __launch_bounds__(128) k_ndga_k(DevCtx c, const int *keom, const
     const int i = e % nd, j = e / nd;
     double v = 2.0 * acc[e] / c.beta;
     if (i == j) v += 0.5;
-    nk[(size_t)ik + (size_t)c.nkp_eom * e] = make_double2(v, 0.0);
+    nk[(size_t)ik + (size_t)nkk * e] = make_double2(v, 0.0);
   }
 }
 
@@ -145,7 +148,7 @@ cudaError_t launch_post_loop(const DevCtx &c, const int *keom, z64 *sig, z64 *si
     e = ADGA_LAUNCH_CHECK();
   }
   if (e == cudaSuccess && n_dga_k) {
-    k_ndga_k<<<cdiv_u(c.nkp_eom, 128), 128, 0, st>>>(c, keom, sig, n_dga_k);
+    k_occ<<<cdiv_u(c.nkp_eom, 128), 128, 0, st>>>(c, c.nkp_eom, keom, sig, n_dga_k);
     e = ADGA_LAUNCH_CHECK();
     if (e == cudaSuccess && n_dga) {
       k_ndga<<<c.nd, 256, 0, st>>>(c, n_dga_k, n_dga);
@@ -153,4 +156,10 @@ cudaError_t launch_post_loop(const DevCtx &c, const int *keom, z64 *sig, z64 *si
     }
   }
   return e;
+}
+
+cudaError_t launch_nfock(const DevCtx &c, z64 *nfock, cudaStream_t st) {
+  if (c.nd > PL_MAXND) return cudaErrorInvalidValue;
+  k_occ<<<cdiv_u(c.nkp, 128), 128, 0, st>>>(c, c.nkp, nullptr, nullptr, nfock);
+  return ADGA_LAUNCH_CHECK();
 }

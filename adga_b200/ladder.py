@@ -186,6 +186,16 @@ class Ladder:
                     "set_chi_loc_ext")
         self.ext_chi_loc = True
 
+    def set_vq(self, vq):
+        """do_vq: V(q)_{ijkl}, shape (ndim, ndim, ndim, ndim, nqp) in q_data order, as
+        read_vq reads it (src/interaction_module.f90:39-123); None switches it off."""
+        if vq is None:
+            self._check(self._lib.adga_set_vq(self._h, None), "set_vq")
+            return
+        nd = self.ndim
+        v = _z(vq, (nd, nd, nd, nd, self.nqp))
+        self._check(self._lib.adga_set_vq(self._h, ptr(v)), "set_vq")
+
     def reset_outputs(self):
         self._check(self._lib.adga_reset_outputs(self._h), "reset_outputs")
 

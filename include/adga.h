@@ -139,6 +139,20 @@ int adga_set_threeleg(adga_handle *h, int iwb, int n3iwf, int nineq, const int *
 int adga_set_chi_loc_ext(adga_handle *h, int n2iwb, int nineq, const int *ndims,
                          const adga_z *chi_dens, const adga_z *chi_magn);
 
+/*
+ * Non-local interaction V(q) (do_vq, read_vq at src/main.F90:497-498).
+ * vq(ndim, ndim, ndim, ndim, nqp): V(q)_{ijkl} for the handle's q points in
+ * q_data order, as read_vq reads it (src/interaction_module.f90:75-104); the
+ * library applies read_vq's index map (:107-119), computes n_fock (get_nfock,
+ * src/one_particle_quant_module.f90:316-342) and from then on adds the V(q)
+ * terms: the density-channel BSE term 2 beta^-2 chi0^q v (1+gamma^w_d)
+ * (src/main.F90:710-719, also in the mixed refinement residual), the m_tot
+ * terms (src/eom_module.f90:187-205) and calc_eom_static's non-local Hartree
+ * and Fock parts into sigma_hf (src/eom_module.f90:70-108).  NULL switches
+ * the interaction off.
+ */
+int adga_set_vq(adga_handle *h, const adga_z *vq);
+
 /* index2component_band (src/aux.f90:169-186): the 1-based band pattern
  * b[0..3] of a 1-based vertex group index ind over nbands bands (the group
  * names of the w2dynamics vertex file).  Host only; returns 0 or ADGA_EINVAL. */

@@ -371,6 +371,9 @@ class LadderInputs:
     # external_chi_loc: (chi_loc_dens, chi_loc_magn) (ndim2, ndim2, 2*iwb+1) as
     # read_chi_loc returns them (src/main.F90:407-411); None = built from gamma^w
     chi_loc_ext: Optional[Tuple[np.ndarray, np.ndarray]] = None
+    # do_vq: V(q) per q point, (ndim2, ndim2, nqp) as read_vq returns it
+    # (src/interaction_module.f90:39-123); None = no non-local interaction
+    vq: Optional[np.ndarray] = None
 
     def __post_init__(self):
         if self.iw_data is None:
@@ -479,10 +482,40 @@ class Oracle:
         chi_qw += tmp / inp.beta ** 2
 
     # ---- EOM (src/eom_module.f90) ----
-    def calc_eom_static(self, iq, sigma_dmft):
-        """Local Hartree term (src/eom_module.f90:52-70); V(q) parts are off."""
+    def n_fock(self):
+        """get_nfock (src/one_particle_quant_module.f90:316-342): n(k, i, j) =
+        2/beta sum_{nu>=0} Re G_DMFT(k, nu) + 1/2 on the diagonal."""
+        if getattr(self, "_n_fock", None) is None:
+            inp = self.inp
+            acc = np.zeros((inp.nkp, inp.ndim, inp.ndim))
+            for n in range(inp.iwmax):
+                acc += self.gk_lapack(n).real
+            nf = (2.0 * acc / inp.beta).astype(complex)
+            for i in range(inp.ndim):
+                nf[:, i, i] += 0.5
+            self._n_fock = nf
+        return self._n_fock
+
+    def calc_eom_static(self, iq, sigma_dmft, sigma_hf=None):
+        """calc_eom_static (src/eom_module.f90:39-111): local Hartree term into
+        sigma_dmft for iq = 0; with V(q) the non-local Hartree 2 v(q=0) n_dmft
+        (iq = 0) and the Fock term -v(q)/nqp n_fock(k-q) into sigma_hf."""
         inp = self.inp
         nd = inp.ndim
+        if inp.vq is not None and sigma_hf is not None:
+            v = inp.vq[:, :, iq]
+            if iq == 0:
+                for i in range(nd):
+                    for j in range(nd):
+                        sigma_hf[i, i, :] += 2.0 * v[i * nd + i, j * nd + j] * inp.n_dmft[j]
+            nf = self.n_fock()
+            ikq = self.kq_ind[:, iq] - 1
+            for l in range(nd):
+                for j in range(nd):
+                    for i in range(nd):
+                        for k in range(nd):
+                            alpha = v[i * nd + k, l * nd + j] / inp.nqp
+                            sigma_hf[i, l, :] -= alpha * nf[ikq, j, k]
         if iq == 0:
             tmp = np.zeros(nd, dtype=complex)
             for i in range(nd):
@@ -508,23 +541,26 @@ class Oracle:
                         sigma_dmft[i, l, iwf + iwfs] += m_tot[i1, i2] * self.giw(iwf - iwb, k)
             sigma_dmft[:, :, -iwf - 1 + iwfs] = np.conj(sigma_dmft[:, :, iwf + iwfs]).T
 
-    def eom_m_tot(self, etaqd, etaqm, gammaqd):
-        """m_tot of calc_eom_dynamic (src/eom_module.f90:184-207), V(q)=0."""
+    def eom_m_tot(self, etaqd, etaqm, gammaqd, iq=None, gammawd=None):
+        """m_tot of calc_eom_dynamic (src/eom_module.f90:184-207)."""
         inp = self.inp
         nqp = float(inp.nqp)
-        u_work = inp.u - 0.5 * inp.u_tilde
+        v = inp.vq[:, :, iq] if inp.vq is not None else 0.0
+        u_work = v + inp.u - 0.5 * inp.u_tilde
         m = (-1.0 / inp.beta / nqp) * (u_work @ etaqd)
         m += (1.5 / inp.beta / nqp) * (inp.u_tilde @ etaqm)
         m += (1.0 / inp.beta / nqp) * (inp.u @ gammaqd)
+        if inp.vq is not None:
+            m += (-1.0 / inp.beta / nqp) * (v @ gammawd)
         return m
 
-    def calc_eom_dynamic(self, etaqd, etaqm, gammaqd, iwb, iq, sigma_nl):
+    def calc_eom_dynamic(self, etaqd, etaqm, gammaqd, iwb, iq, sigma_nl, gammawd=None):
         """Sigma(i,l,nu,k) += m_tot({j,i},{k',l,nu}) G_jk'(k-q, nu-omega) for
         nu >= 0, then the mirror Sigma(-nu-1) = Sigma(nu)^dagger
         (src/eom_module.f90:165-233)."""
         inp = self.inp
         nd, nd2, iwfs = inp.ndim, inp.ndim2, inp.iwfmax_small
-        m_tot = self.eom_m_tot(etaqd, etaqm, gammaqd)
+        m_tot = self.eom_m_tot(etaqd, etaqm, gammaqd, iq, gammawd)
         M = m_tot[:, nd2 * iwfs:].reshape(nd, nd, iwfs, nd, nd)   # [i, j, w, l, k']
         ikq = self.kq_ind[:, iq] - 1
         G = np.stack([self.gk_lapack(iwf - iwb)[ikq] for iwf in range(iwfs)], axis=1)  # [n, w, j, k']
@@ -570,8 +606,8 @@ class Oracle:
                 cur_iwb = iwb
                 loc = self.local_block(iwb, iq, out)
             chi0w_inv, chi0w, bubble_loc_tmp, Fd, Fm, gd, gm, opgd, opgm = loc
-            if inp.do_eom and iwb == 0 and iq == 0:
-                self.calc_eom_static(iq, out["sigma_dmft"])
+            if inp.do_eom and iwb == 0 and (iq == 0 or inp.vq is not None):
+                self.calc_eom_static(iq, out["sigma_dmft"], out["sigma_hf"])
             if inp.do_eom and iq == 0:
                 self.calc_eom_dmft(gd, iwb, out["sigma_dmft"])
             res = self.point(iq, iwb, loc)
@@ -581,7 +617,7 @@ class Oracle:
                 out["chi_qw_magn"][:, :, p] = res["chi_qw_magn"]
             if inp.do_eom:
                 self.calc_eom_dynamic(res["etaqd"], res["etaqm"], res["gammaqd"], iwb, iq,
-                                      out["sigma_nl"])
+                                      out["sigma_nl"], gd)
             out["status"][p] = res["ierr"]
             if p == 0:
                 out["first_point"] = res
@@ -673,6 +709,9 @@ class Oracle:
             gammaqd += rect
             rect = sw @ Fm[off:off + nd2, :]
             bm[off:off + nd2, :] = -rect
+            if inp.vq is not None:     # density channel: 2 beta^-2 chi0^q v^q (1+gamma^w_d) (:710-719)
+                small = (2.0 / beta ** 2) * (chi0q[:, :, dum1] @ inp.vq[:, :, iq])
+                bd[off:off + nd2, :] -= small @ opgd
         bd[np.arange(N), np.arange(N)] += 1.0
         bm[np.arange(N), np.arange(N)] += 1.0
         res["A_dens"] = bd.copy(order="F")
@@ -843,3 +882,17 @@ def read_chi_loc_transform(chi_raw, channel, ndims, giw, n_dmft, beta, iwbs, iwm
                     i2 += 1
             i1 += 1
     return np.asfortranarray(out)
+
+
+def read_vq_transform(vq_raw):
+    """The index map of read_vq (src/interaction_module.f90:107-119):
+    vq(i, j, k, l, q) -> v(i1 = i*ndim + k, i2 = l*ndim + j, q)."""
+    vq_raw = np.asarray(vq_raw)
+    nd, nqp = vq_raw.shape[0], vq_raw.shape[4]
+    v = np.zeros((nd * nd, nd * nd, nqp), complex)
+    for l in range(nd):
+        for j in range(nd):
+            for i in range(nd):
+                for k in range(nd):
+                    v[i * nd + k, l * nd + j, :] = vq_raw[i, j, k, l, :]
+    return np.asfortranarray(v)
