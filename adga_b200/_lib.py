@@ -23,7 +23,8 @@ EXPORTS = [
     "adga_inverse_matrix_z", "adga_index_kq", "adga_generate_q_vol", "adga_create_u",
     "adga_inverse_matrix_z_noalloc", "adga_set_vertex_g4", "adga_vertex_transform",
     "adga_index2component_band", "adga_post_loop", "adga_set_threeleg", "adga_set_chi_loc_ext",
-    "adga_set_vq",
+    "adga_set_vq", "adga_set_tangent", "adga_set_vertex_tangent", "adga_ladder_run_tangent",
+    "adga_get_tangent_outputs", "adga_clear_tangents",
 ]
 
 
@@ -96,6 +97,11 @@ def load():
         "adga_set_threeleg": [vp, i, i, i, vp, vp, vp],
         "adga_set_chi_loc_ext": [vp, i, i, vp, vp, vp],
         "adga_set_vq": [vp, vp],
+        "adga_set_tangent": [vp, i, vp, vp, vp],
+        "adga_set_vertex_tangent": [vp, i, i, vp, vp],
+        "adga_ladder_run_tangent": [vp, i, i, ip, C.POINTER(RunStats)],
+        "adga_get_tangent_outputs": [vp, i, C.POINTER(Outputs)],
+        "adga_clear_tangents": [vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

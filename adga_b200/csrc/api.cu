@@ -30,6 +30,9 @@ void tc_trail_free(void *ctx);
 int tc_available();
 int tc_trail_error(void *ctx);
 
+struct TanState;
+struct TanWork;
+
 struct adga_handle {
   adga_dims d{};
   DevCtx c{};
@@ -47,6 +50,9 @@ struct adga_handle {
   z64 *ext_cld = nullptr, *ext_clm = nullptr;   // external chi_loc (nd2, nd2, nw), or null
   z64 *vq_d = nullptr, *nfock_d = nullptr;       // V(q) and n_fock (do_vq), or null
   z64 *vq_extra = nullptr;                        // density-channel V(q) residual term (mixed)
+  TanState *tan[ADGA_MAX_TANGENTS] = {};         // tangent directions, or null
+  TanWork *tw = nullptr;                          // their shared work
+  bool tan_on = false;                            // inside adga_ladder_run_tangent
   size_t vq_extra_cap = 0;
   // local block
   int diag_iwb = INT_MIN, loc_iwb = INT_MIN;
@@ -77,6 +83,33 @@ struct adga_handle {
   // last-run statistics
   adga_run_stats stats{};
 };
+
+// one tangent direction
+struct TanState {
+  bool has_dhk = false;
+  z64 *gdot = nullptr, *du = nullptr, *dut = nullptr;
+  std::vector<z64 *> vd, vm;               // dchi_loc per omega (N x N), or null
+  z64 *Fd = nullptr, *Fm = nullptr, *gd = nullptr, *gm = nullptr;
+  int loc_iwb = INT_MIN;
+  bool loc_has = false;
+  // accumulators
+  z64 *chi_loc_d = nullptr, *chi_loc_m = nullptr, *sigma_nl = nullptr, *sigma_dmft = nullptr;
+  z64 *chi_qw_d = nullptr, *chi_qw_m = nullptr, *bub_nl = nullptr;
+  int out_cap = 0;
+  std::vector<void *> owned;
+};
+// batch work and constants shared by the directions (they run one after another)
+struct TanWork {
+  z64 *zero_nd4 = nullptr, *zero_N = nullptr, *zero_gam = nullptr, *opg_scr = nullptr, *bub_scr = nullptr;
+  std::vector<void *> owned, work;
+  int cap = 0;
+  z64 *chi0_all = nullptr, *chi0_tmp = nullptr, *chi0q_big = nullptr, *zero_chi0 = nullptr;
+  z64 *Xc = nullptr, *XS = nullptr, *XD = nullptr, *Rt = nullptr, *wk = nullptr, *gq = nullptr;
+  z64 *cA_d = nullptr, *cA_m = nullptr, *cB_d = nullptr, *cB_m = nullptr, *mA = nullptr, *mB = nullptr;
+  z64 *eta_d = nullptr, *eta_m = nullptr;
+  int *perm = nullptr;
+};
+static void tan_free(adga_handle *h);
 
 #define CK(call)                                                                  \
   do {                                                                            \
@@ -235,6 +268,7 @@ extern "C" int adga_destroy(adga_handle *h) {
   if (h->vq_d) cudaFree(h->vq_d);
   if (h->nfock_d) cudaFree(h->nfock_d);
   if (h->vq_extra) cudaFree(h->vq_extra);
+  tan_free(h);
   if (h->qidx_h) cudaFreeHost(h->qidx_h);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
@@ -264,6 +298,13 @@ extern "C" int adga_reset_outputs(adga_handle *h) {
   CK(cudaMemsetAsync(h->sigma_nl, 0, sizeof(z64) * c.nd2 * 2 * c.iwf * c.nkp_eom, st));
   CK(cudaMemsetAsync(h->sigma_dmft, 0, sizeof(z64) * c.nd2 * 2 * c.iwf, st));
   CK(cudaMemsetAsync(h->sigma_hf, 0, sizeof(z64) * c.nd2 * c.nkp_eom, st));
+  for (TanState *t : h->tan) {
+    if (!t) continue;
+    CK(cudaMemsetAsync(t->chi_loc_d, 0, sizeof(z64) * h->nd4 * h->nw, st));
+    CK(cudaMemsetAsync(t->chi_loc_m, 0, sizeof(z64) * h->nd4 * h->nw, st));
+    CK(cudaMemsetAsync(t->sigma_nl, 0, sizeof(z64) * c.nd2 * 2 * c.iwf * c.nkp_eom, st));
+    CK(cudaMemsetAsync(t->sigma_dmft, 0, sizeof(z64) * c.nd2 * 2 * c.iwf, st));
+  }
   CK(cudaStreamSynchronize(st));
   return 0;
 }
@@ -516,7 +557,7 @@ static int ensure_work(adga_handle *h, int prec, int want) {
   size_t per = bytes_per_point(h, prec, NB);
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
-  double frac = 0.6;
+  double frac = h->tan_on ? 0.3 : 0.6;   // tangent runs hold about as much again
   const char *e = getenv("ADGA_WORK_FRAC");
   if (e) frac = atof(e);
   size_t budget = (size_t)(fr * frac);
@@ -604,6 +645,270 @@ static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool ap
 
 // one batch of np consecutive q at omega = iwb: chi0 -> build -> LU/solve -> post -> EOM.
 // qidx_h[0..np) hold the 0-based q indices; outputs go to point slot `off`.
+// ---------------------------------------------------------------------------
+// Tangent (forward-mode) ladder: derivatives of the FP64 outputs along one
+// parameter direction, given the direction's dH(k), du, du~ and dchi_loc(omega)
+// (k_tangent.cu has the BSE algebra; every other stage reuses the forward
+// kernels with swapped pointers, since they are linear in each argument).
+// ---------------------------------------------------------------------------
+
+static bool tan_dir_ok(int d) { return d >= 0 && d < ADGA_MAX_TANGENTS; }
+
+// shared constants of the tangent passes
+static int tan_shared(adga_handle *h) {
+  if (h->tw) return 0;
+  const DevCtx &c = h->c;
+  TanWork *w = new TanWork();
+  h->tw = w;
+  const size_t N = c.N, nd2 = c.nd2;
+  auto &L = w->owned;
+  if (!(alloc_into(h, w->zero_nd4, nd2 * nd2, L) && alloc_into(h, w->zero_N, N, L) &&
+        alloc_into(h, w->zero_gam, nd2 * N, L) && alloc_into(h, w->opg_scr, nd2 * N, L) &&
+        alloc_into(h, w->bub_scr, nd2 * nd2, L)))
+    return fail(h, ADGA_ENOMEM, "tangent constants");
+  CK(cudaMemsetAsync(w->zero_nd4, 0, sizeof(z64) * nd2 * nd2, h->st));
+  CK(cudaMemsetAsync(w->zero_N, 0, sizeof(z64) * N, h->st));
+  CK(cudaMemsetAsync(w->zero_gam, 0, sizeof(z64) * nd2 * N, h->st));
+  return 0;
+}
+
+static int tan_state(adga_handle *h, int d) {
+  int r = tan_shared(h);
+  if (r) return r;
+  if (h->tan[d]) return 0;
+  const DevCtx &c = h->c;
+  TanState *t = new TanState();
+  h->tan[d] = t;
+  t->vd.assign(h->nw, nullptr);
+  t->vm.assign(h->nw, nullptr);
+  const size_t N = c.N, nd2 = c.nd2, nw = h->nw;
+  auto &L = t->owned;
+  bool ok = alloc_into(h, t->gdot, (size_t)c.nnu * c.nkp * nd2, L) && alloc_into(h, t->du, nd2 * nd2, L) &&
+            alloc_into(h, t->dut, nd2 * nd2, L) && alloc_into(h, t->Fd, N * N, L) &&
+            alloc_into(h, t->Fm, N * N, L) && alloc_into(h, t->gd, nd2 * N, L) && alloc_into(h, t->gm, nd2 * N, L) &&
+            alloc_into(h, t->chi_loc_d, nd2 * nd2 * nw, L) && alloc_into(h, t->chi_loc_m, nd2 * nd2 * nw, L) &&
+            alloc_into(h, t->sigma_nl, nd2 * 2 * c.iwf * (size_t)c.nkp_eom, L) &&
+            alloc_into(h, t->sigma_dmft, nd2 * 2 * c.iwf, L);
+  if (!ok) return fail(h, ADGA_ENOMEM, "tangent direction");
+  CK(cudaMemsetAsync(t->du, 0, sizeof(z64) * nd2 * nd2, h->st));
+  CK(cudaMemsetAsync(t->dut, 0, sizeof(z64) * nd2 * nd2, h->st));
+  CK(cudaMemsetAsync(t->chi_loc_d, 0, sizeof(z64) * nd2 * nd2 * nw, h->st));
+  CK(cudaMemsetAsync(t->chi_loc_m, 0, sizeof(z64) * nd2 * nd2 * nw, h->st));
+  CK(cudaMemsetAsync(t->sigma_nl, 0, sizeof(z64) * nd2 * 2 * c.iwf * c.nkp_eom, h->st));
+  CK(cudaMemsetAsync(t->sigma_dmft, 0, sizeof(z64) * nd2 * 2 * c.iwf, h->st));
+  return 0;
+}
+
+static void tan_free(adga_handle *h) {
+  for (TanState *&t : h->tan) {
+    if (!t) continue;
+    free_list(t->owned);
+    for (auto p : t->vd) if (p) cudaFree(p);
+    for (auto p : t->vm) if (p) cudaFree(p);
+    for (z64 *p : {t->chi_qw_d, t->chi_qw_m, t->bub_nl}) if (p) cudaFree(p);
+    delete t;
+    t = nullptr;
+  }
+  if (h->tw) {
+    free_list(h->tw->work);
+    free_list(h->tw->owned);
+    delete h->tw;
+    h->tw = nullptr;
+  }
+}
+
+extern "C" int adga_set_tangent(adga_handle *h, int dir, const adga_z *dhk, const adga_z *du,
+                                const adga_z *du_tilde) {
+  if (!h) return ADGA_EINVAL;
+  if (!tan_dir_ok(dir)) return fail(h, ADGA_EINVAL, "set_tangent: direction outside 0..ADGA_MAX_TANGENTS-1");
+  int r = tan_state(h, dir);
+  if (r) return r;
+  TanState *t = h->tan[dir];
+  const DevCtx &c = h->c;
+  const size_t nd4 = (size_t)c.nd2 * c.nd2;
+  if (du) CK(cudaMemcpyAsync(t->du, du, sizeof(z64) * nd4, cudaMemcpyHostToDevice, h->st));
+  else CK(cudaMemsetAsync(t->du, 0, sizeof(z64) * nd4, h->st));
+  if (du_tilde) CK(cudaMemcpyAsync(t->dut, du_tilde, sizeof(z64) * nd4, cudaMemcpyHostToDevice, h->st));
+  else CK(cudaMemsetAsync(t->dut, 0, sizeof(z64) * nd4, h->st));
+  t->has_dhk = dhk != nullptr;
+  if (dhk) {
+    z64 *dh = nullptr;
+    if (cudaMalloc(&dh, sizeof(z64) * c.nd2 * c.nkp) != cudaSuccess) return fail(h, ADGA_ENOMEM, "dhk");
+    cudaError_t e = cudaMemcpyAsync(dh, dhk, sizeof(z64) * c.nd2 * c.nkp, cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = launch_gtable_dot(c, dh, t->gdot, h->st);   // dG = G dH G
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    cudaFree(dh);
+    if (e != cudaSuccess) return fail(h, ADGA_ECUDA, "set_tangent: dG table");
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+extern "C" int adga_clear_tangents(adga_handle *h) {
+  if (!h) return ADGA_EINVAL;
+  cudaStreamSynchronize(h->st);
+  tan_free(h);
+  return 0;
+}
+
+extern "C" int adga_set_vertex_tangent(adga_handle *h, int dir, int iwb, const adga_z *dchi_d,
+                                       const adga_z *dchi_m) {
+  if (!h) return ADGA_EINVAL;
+  if (!tan_dir_ok(dir)) return fail(h, ADGA_EINVAL, "set_vertex_tangent: direction out of range");
+  if (iwb < -h->c.iwb || iwb > h->c.iwb) return fail(h, ADGA_EINVAL, "iwb out of range");
+  int r = tan_state(h, dir);
+  if (r) return r;
+  TanState *t = h->tan[dir];
+  const int w = iwb + h->c.iwb;
+  const size_t n = (size_t)h->c.N * h->c.N;
+  t->loc_iwb = INT_MIN;
+  if (!dchi_d || !dchi_m) {
+    if (t->vd[w]) { cudaFree(t->vd[w]); cudaFree(t->vm[w]); t->vd[w] = t->vm[w] = nullptr; }
+    return 0;
+  }
+  if (!t->vd[w] && (cudaMalloc(&t->vd[w], n * sizeof(z64)) != cudaSuccess ||
+                    cudaMalloc(&t->vm[w], n * sizeof(z64)) != cudaSuccess))
+    return fail(h, ADGA_ENOMEM, "vertex tangent");
+  CK(cudaMemcpyAsync(t->vd[w], dchi_d, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(t->vm[w], dchi_m, n * sizeof(z64), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+// dF~ and dgamma^w of direction d at omega = iwb (after ensure_local)
+static int tan_local(adga_handle *h, int d, int iwb) {
+  TanState *t = h->tan[d];
+  if (t->loc_iwb == iwb) return 0;
+  const int w = iwb + h->c.iwb;
+  t->loc_has = t->vd[w] != nullptr;
+  if (t->loc_has) {
+    // F~ = sym(chi_loc) chi0_loc^-1 - 1 is affine in chi_loc: dF~ = sym(dchi_loc) chi0_loc^-1
+    CK(launch_local_F(h->c, t->vd[w], h->c0inv, t->Fd, h->st, false));
+    CK(launch_local_F(h->c, t->vm[w], h->c0inv, t->Fm, h->st, false));
+    CK(launch_local_gamma(h->c, t->Fd, t->gd, h->tw->opg_scr, h->st));
+    CK(launch_local_gamma(h->c, t->Fm, t->gm, h->tw->opg_scr, h->st));
+  }
+  t->loc_iwb = iwb;
+  return 0;
+}
+
+static int tan_work(adga_handle *h) {
+  TanWork *t = h->tw;
+  if (t->cap >= h->cap) return 0;
+  free_list(t->work);
+  t->cap = 0;
+  const DevCtx &c = h->c;
+  const size_t cap = h->cap, N = c.N, R = c.R, nd2 = c.nd2, nd4 = (size_t)h->nd4;
+  const size_t per = R * N;
+  auto &W = t->work;
+  bool ok = alloc_into(h, t->chi0_all, cap * nd4 * h->nnu_all, W) &&
+            alloc_into(h, t->chi0_tmp, cap * nd4 * h->nnu_all, W) &&
+            alloc_into(h, t->zero_chi0, cap * nd4 * 2 * c.iwf, W) && alloc_into(h, t->Xc, 2 * cap * per, W) &&
+            alloc_into(h, t->XS, 2 * cap * per, W) && alloc_into(h, t->XD, 2 * cap * per, W) &&
+            alloc_into(h, t->Rt, 2 * cap * per, W) && alloc_into(h, t->wk, 2 * cap * ((R + 15) / 16) * 16 * N, W) &&
+            alloc_into(h, t->gq, cap * nd2 * N, W) && alloc_into(h, t->cA_d, cap * nd4, W) &&
+            alloc_into(h, t->cA_m, cap * nd4, W) && alloc_into(h, t->cB_d, cap * nd4, W) &&
+            alloc_into(h, t->cB_m, cap * nd4, W) && alloc_into(h, t->mA, cap * nd2 * c.iwf * nd2, W) &&
+            alloc_into(h, t->mB, cap * nd2 * c.iwf * nd2, W) && alloc_into(h, t->eta_d, cap * nd2 * N, W) &&
+            alloc_into(h, t->eta_m, cap * nd2 * N, W) && alloc_into(h, t->perm, 2 * cap * N, W);
+  if (ok && h->bigbox) ok = alloc_into(h, t->chi0q_big, cap * nd4 * 2 * c.iwf, W);
+  if (!ok) return fail(h, ADGA_ENOMEM, "tangent batch buffers");
+  CK(cudaMemsetAsync(t->zero_chi0, 0, sizeof(z64) * cap * nd4 * 2 * c.iwf, h->st));
+  t->cap = (int)cap;
+  return 0;
+}
+
+// the tangent of direction d for one FP64 batch, after its forward pass (T holds
+// the LU factors of the transposed BSE matrices, factorised with the left interchanges)
+static int tan_batch(adga_handle *h, int d, int iwb, int np, int off, z64 *T, LUBatch lb, const z64 *chi0q,
+                     bool do_chi, bool do_eom) {
+  TanState *t = h->tan[d];
+  DevCtx &c = h->c;
+  cudaStream_t st = h->st;
+  const size_t N = c.N, R = c.R, per = R * N, strideM = N * (N + R);
+  int r = tan_work(h);
+  if (r) return r;
+  TanWork *w = h->tw;
+  // dchi0^q = -(beta/nkp) sum_k [dG(k) G(k-q) + G(k) dG(k-q)]
+  const z64 *dchi0q = nullptr;
+  if (t->has_dhk) {
+    DevCtx cg = c;
+    cg.gtab = t->gdot;
+    CK(launch_chi0(cg, iwb, h->qidx_d, np, w->chi0_all, h->nnu_all, st, c.gtab));
+    CK(launch_chi0(c, iwb, h->qidx_d, np, w->chi0_tmp, h->nnu_all, st, t->gdot));
+    CK(launch_zadd((size_t)np * h->nd4 * h->nnu_all, w->chi0_tmp, w->chi0_all, st));
+    dchi0q = h->bigbox ? w->chi0q_big : w->chi0_all;
+    CK(launch_chi0_finish(c, w->chi0_all, h->nnu_all, np, w->zero_nd4, h->bigbox ? w->chi0q_big : nullptr,
+                          do_chi ? t->bub_nl + (size_t)off * h->nd4 : nullptr, st));
+  }
+  // X (compact) and the tangent right-hand sides dB + XS F~ + XD dF~
+  CK(cudaMemcpy2DAsync(w->Xc, per * sizeof(z64), T + N * N, strideM * sizeof(z64), per * sizeof(z64), 2 * np,
+                       cudaMemcpyDeviceToDevice, st));
+  CK(launch_xd(c, np, w->Xc, chi0q, h->c0inv, w->XD, true, st));
+  if (dchi0q) CK(launch_xd(c, np, w->Xc, dchi0q, h->c0inv, w->XS, false, st));
+  for (int ch = 0; ch < 2; ++ch)
+    CK(launch_tan_rhs(c, np, ch, dchi0q ? w->XS : nullptr, ch ? h->Frow_m : h->Frow_d,
+                      t->loc_has ? w->XD : nullptr, t->loc_has ? (ch ? t->Fm : t->Fd) : nullptr,
+                      t->loc_has ? (ch ? t->gm : t->gd) : nullptr, w->Rt, st));
+  // dX = r A^-1 with the forward LU factors: T dX^T = r^T (forward, then back substitution)
+  CK(lu_build_perm(lb, w->perm, st));
+  lb.perm = w->perm;
+  CK(lu_fwdsolve_ws<z64>(T, lb, w->Rt, per, (int)N, (int)R, w->wk, st));
+  CK(lu_backsolve<z64>(T, lb, w->Rt, per, (int)N, (int)R, st));
+  // dgamma^q_d
+  CK(launch_gamq_tan(c, np, chi0q, dchi0q, h->c0inv, h->Frow_d, t->loc_has ? t->Fd : nullptr, w->gq, st));
+  // chi sums and m_tot are bilinear: (a) with the tangents of X, gamma^w, gamma^q
+  // against chi0^q and u; (b) with X, gamma^w, gamma^q against dchi0^q and du
+  const z64 *gdw = t->loc_has ? t->gd : w->zero_gam, *gmw = t->loc_has ? t->gm : w->zero_gam;
+  CK(launch_post(c, np, w->Rt, 2 * per, per, (int)N, gdw, gmw, gdw, gmw, w->gq, chi0q, h->c0w, w->cA_d, w->cA_m,
+                 do_eom ? w->mA : nullptr, w->eta_d, w->eta_m, h->qidx_d, st));
+  DevCtx cu = c;
+  cu.u = t->du;
+  cu.ut = t->dut;
+  cu.vq = nullptr;
+  CK(launch_post(cu, np, w->Xc, 2 * per, per, (int)N, h->opg_d, h->opg_m, h->gam_d, h->gam_m, h->gq,
+                 dchi0q ? dchi0q : w->zero_chi0, w->zero_N, w->cB_d, w->cB_m, do_eom ? w->mB : nullptr, w->eta_d,
+                 w->eta_m, h->qidx_d, st));
+  if (do_chi) {
+    const size_t nc = (size_t)np * h->nd4;
+    CK(launch_zadd(nc, w->cB_d, w->cA_d, st));
+    CK(launch_zadd(nc, w->cB_m, w->cA_m, st));
+    CK(cudaMemcpyAsync(t->chi_qw_d + (size_t)off * h->nd4, w->cA_d, nc * sizeof(z64), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(t->chi_qw_m + (size_t)off * h->nd4, w->cA_m, nc * sizeof(z64), cudaMemcpyDeviceToDevice, st));
+  }
+  if (do_eom) {
+    // dSigma += dm_tot G(k-q) + m_tot dG(k-q)
+    CK(launch_zadd((size_t)np * c.nd2 * c.iwf * c.nd2, w->mB, w->mA, st));
+    CK(launch_eom_dynamic(c, iwb, h->qidx_d, np, w->mA, t->sigma_nl, st));
+    if (t->has_dhk) {
+      DevCtx cg = c;
+      cg.gtab = t->gdot;
+      CK(launch_eom_dynamic(cg, iwb, h->qidx_d, np, h->mtot, t->sigma_nl, st));
+    }
+  }
+  return 0;
+}
+
+// local tangents of direction d at omega = iwb where the block holds iq = 1
+static int tan_local_update(adga_handle *h, int d, int iwb, bool do_chi, bool do_eom) {
+  TanState *t = h->tan[d];
+  TanWork *w = h->tw;
+  DevCtx &c = h->c;
+  const int wi = iwb + c.iwb;
+  if (do_chi && t->loc_has)
+    CK(launch_chi_loc_update(c, t->gd, t->gm, h->c0w, w->zero_nd4, t->chi_loc_d + (size_t)wi * h->nd4,
+                             t->chi_loc_m + (size_t)wi * h->nd4, w->bub_scr, h->st));
+  if (do_eom) {
+    DevCtx cu = c;
+    cu.u = t->du;
+    cu.ut = t->dut;
+    if (iwb == 0) CK(launch_eom_static(cu, t->sigma_dmft, h->st));
+    CK(launch_eom_dmft(cu, iwb, h->gam_d, t->sigma_dmft, h->st));
+    if (t->loc_has) CK(launch_eom_dmft(c, iwb, t->gd, t->sigma_dmft, h->st));
+  }
+  return 0;
+}
+
 static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *status,
                      z64 *chi_qw_d, z64 *chi_qw_m, z64 *bub_nl, bool do_eom, bool do_chi) {
   DevCtx &c = h->c;
@@ -637,7 +942,8 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     CK(launch_bse_build<z64>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
                              strideM, h->gq, h->qidx_d, st));
     cudaEventRecord(ev[2], st);
-    CK(factor_batch<z64>(h, T, lb, false, false, &tt));
+    // tangents solve with L as well: keep the interchanges on the left columns
+    CK(factor_batch<z64>(h, T, lb, h->tan_on, false, &tt));
     CK(lu_backsolve<z64>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     X = T + N * N; sp = 2 * strideM; sc = strideM;
   } else {
@@ -706,6 +1012,12 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
                        sizeof(z64) * c.nd2 * c.iwf * c.nd2, st));
   cudaEventRecord(ev[4], st);
   if (do_eom) CK(launch_eom_dynamic(c, iwb, h->qidx_d, np, h->mtot, h->sigma_nl, st));
+  if (prec == ADGA_FP64 && h->tan_on)
+    for (int d = 0; d < ADGA_MAX_TANGENTS; ++d)
+      if (h->tan[d]) {
+        int rt = tan_batch(h, d, iwb, np, off, (z64 *)h->Tm, lb, chi0q, do_chi, do_eom);
+        if (rt) return rt;
+      }
   cudaEventRecord(ev[5], st);
   std::vector<int> info(2 * np);
   CK(cudaMemcpyAsync(info.data(), h->info, sizeof(int) * 2 * np, cudaMemcpyDeviceToHost, st));
@@ -796,7 +1108,11 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
     const int seg = std::min(npts - p, c.nqp - iq0);
     r = ensure_local(h, iwb);
     if (r) return r;
+    for (int d = 0; h->tan_on && d < ADGA_MAX_TANGENTS; ++d)
+      if (h->tan[d] && (r = tan_local(h, d, iwb))) return r;
     if (iq0 == 0) {
+      for (int d = 0; h->tan_on && d < ADGA_MAX_TANGENTS; ++d)
+        if (h->tan[d] && (r = tan_local_update(h, d, iwb, do_chi, do_eom))) return r;
       if (do_chi)
         CK(launch_chi_loc_update(c, h->gam_d, h->gam_m, h->c0w, h->bubtmp,
                                  h->ext_cld ? nullptr : h->chi_loc_d + (size_t)(iwb + c.iwb) * h->nd4,
@@ -828,6 +1144,67 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   h->stats.kernel_launches = g_adga_launches.load() - launches0;
   h->last_npts = npts;
   if (stats) *stats = h->stats;
+  return 0;
+}
+
+extern "C" int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, int *status,
+                                       adga_run_stats *stats) {
+  if (!h) return ADGA_EINVAL;
+  int ndir = 0;
+  for (TanState *t : h->tan) ndir += t != nullptr;
+  if (!ndir) return fail(h, ADGA_ESTATE, "ladder_run_tangent: no tangent direction set");
+  if (h->c.vq) return fail(h, ADGA_EINVAL, "ladder_run_tangent: V(q) tangents are not supported");
+  const DevCtx &c = h->c;
+  if (qwstart < 1 || qwstop > c.nqp * h->nw || qwstop < qwstart) return fail(h, ADGA_EINVAL, "qw range");
+  const int npts = qwstop - qwstart + 1;
+  for (TanState *t : h->tan) {
+    if (!t) continue;
+    if (t->out_cap < npts) {
+      for (z64 *p : {t->chi_qw_d, t->chi_qw_m, t->bub_nl}) if (p) cudaFree(p);
+      t->chi_qw_d = t->chi_qw_m = t->bub_nl = nullptr;
+      t->out_cap = 0;
+      if (cudaMalloc(&t->chi_qw_d, sizeof(z64) * npts * h->nd4) != cudaSuccess ||
+          cudaMalloc(&t->chi_qw_m, sizeof(z64) * npts * h->nd4) != cudaSuccess ||
+          cudaMalloc(&t->bub_nl, sizeof(z64) * npts * h->nd4) != cudaSuccess)
+        return fail(h, ADGA_ENOMEM, "tangent per-point outputs");
+      t->out_cap = npts;
+    }
+    CK(cudaMemsetAsync(t->chi_qw_d, 0, sizeof(z64) * npts * h->nd4, h->st));
+    CK(cudaMemsetAsync(t->chi_qw_m, 0, sizeof(z64) * npts * h->nd4, h->st));
+    CK(cudaMemsetAsync(t->bub_nl, 0, sizeof(z64) * npts * h->nd4, h->st));
+    t->loc_iwb = INT_MIN;
+  }
+  h->tan_on = true;
+  h->loc_iwb = INT_MIN;
+  int r = adga_ladder_run(h, qwstart, qwstop, ADGA_FP64, status, stats);
+  h->tan_on = false;
+  return r;
+}
+
+extern "C" int adga_get_tangent_outputs(adga_handle *h, int dir, const adga_outputs *o) {
+  if (!h || !o) return ADGA_EINVAL;
+  if (!tan_dir_ok(dir) || !h->tan[dir]) return fail(h, ADGA_ESTATE, "get_tangent_outputs: direction not set");
+  TanState *t = h->tan[dir];
+  const DevCtx &c = h->c;
+  cudaStream_t st = h->st;
+  CK(launch_mirror_sigma(c, t->sigma_nl, c.nkp_eom, st));
+  const size_t np = h->last_npts;
+#define TDN(dst, src, n) \
+  if (dst) CK(cudaMemcpyAsync(dst, src, sizeof(z64) * (n), cudaMemcpyDeviceToHost, st))
+  if (np && t->chi_qw_d) {
+    TDN(o->chi_qw_dens, t->chi_qw_d, np * h->nd4);
+    TDN(o->chi_qw_magn, t->chi_qw_m, np * h->nd4);
+    TDN(o->bubble_nl, t->bub_nl, np * h->nd4);
+  }
+  TDN(o->chi_loc_dens, t->chi_loc_d, (size_t)h->nd4 * h->nw);
+  TDN(o->chi_loc_magn, t->chi_loc_m, (size_t)h->nd4 * h->nw);
+  TDN(o->sigma_nl, t->sigma_nl, (size_t)c.nd2 * 2 * c.iwf * c.nkp_eom);
+  TDN(o->sigma_dmft, t->sigma_dmft, (size_t)c.nd2 * 2 * c.iwf);
+#undef TDN
+  CK(cudaStreamSynchronize(st));
+  // the local bubble and sigma_hf do not depend on the direction (G_loc, n fixed; no V(q))
+  if (o->bubble_loc) memset(o->bubble_loc, 0, sizeof(z64) * h->nd4 * h->nw);
+  if (o->sigma_hf) memset(o->sigma_hf, 0, sizeof(z64) * c.nd2 * c.nkp_eom);
   return 0;
 }
 

@@ -39,7 +39,8 @@ cudaError_t launch_kq_index(int nkpx, int nkpy, int nkpz, const int *k_sel, int 
 cudaError_t launch_local_diag(const DevCtx &c, int iwb, z64 *c0inv, z64 *c0w, z64 *bubloc_tmp,
                               cudaStream_t st);
 cudaError_t launch_local_F(const DevCtx &c, const z64 *chi_loc, const z64 *c0inv, z64 *Frow,
-                           cudaStream_t st);
+                           cudaStream_t st, bool minus_one = true);
+cudaError_t launch_gtable_dot(const DevCtx &c, const z64 *dhk, z64 *gdot, cudaStream_t st);
 cudaError_t launch_local_gamma(const DevCtx &c, const z64 *Frow, z64 *gam, z64 *opg, cudaStream_t st);
 cudaError_t launch_chi_loc_update(const DevCtx &c, const z64 *gam_d, const z64 *gam_m,
                                   const z64 *c0w, const z64 *bubloc_tmp, z64 *chi_loc_d,
@@ -76,9 +77,17 @@ cudaError_t launch_eom_static_vq(const DevCtx &c, const int *qidx, int npts, z64
 cudaError_t launch_vq_resid_extra(const DevCtx &c, int npts, const int *qidx, const z64 *X, const z64 *chi0q,
                                   const z64 *opg_d, z64 *extra, cudaStream_t st);
 
+// k_tangent.cu: forward-mode tangents of one batch (FP64 path)
+cudaError_t launch_tan_rhs(const DevCtx &c, int npts, int ch, const z64 *XS, const z64 *Frow, const z64 *XD,
+                           const z64 *Fdot, const z64 *dB, z64 *out, cudaStream_t st);
+cudaError_t launch_gamq_tan(const DevCtx &c, int npts, const z64 *chi0q, const z64 *dchi0q, const z64 *c0inv,
+                            const z64 *Frow_d, const z64 *Fdot_d, z64 *dgq, cudaStream_t st);
+cudaError_t launch_zadd(size_t n, const z64 *x, z64 *y, cudaStream_t st);
+
 // k_chi0.cu: chi0q[p] (nd2, nd2, nnu_out) for a batch of points at one omega
+// (the G(k-q, nu-omega) factor from g2tab when given: tangents)
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,
-                        int nnu_all, cudaStream_t st);
+                        int nnu_all, cudaStream_t st, const z64 *g2tab = nullptr);
 cudaError_t launch_chi0_finish(const DevCtx &c, const z64 *chi0_all, int nnu_all, int npts,
                                const z64 *bubloc_tmp, z64 *chi0q, z64 *bubble_nl, cudaStream_t st);
 
@@ -102,5 +111,7 @@ cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *
                             const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
                             const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, const z64 *extra_d,
                             cudaStream_t st);
+cudaError_t launch_xd(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q, const z64 *c0inv, z64 *XD,
+                      bool minus_one, cudaStream_t st);
 cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,
                           const int *active, cudaStream_t st);

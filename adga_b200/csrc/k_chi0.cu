@@ -14,7 +14,8 @@
 // staged beside it.  Each gathered G(k-q) value feeds nd2 complex FMAs.
 template <int ND, int QG>
 __global__ void __launch_bounds__(QG * ND * ND)
-k_chi0(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, z64 *__restrict__ out, int nnu_all) {
+k_chi0(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, z64 *__restrict__ out, int nnu_all,
+       const z64 *__restrict__ g2tab) {
   constexpr int ND2 = ND * ND, KC = 64, NTH = QG * ND2;
   __shared__ z64 g1s[KC][ND2];
   __shared__ int kqs[KC][QG];
@@ -24,7 +25,7 @@ k_chi0(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, z64 *__restric
   const bool act = p < npts;
   const int nu = c.iwstart + inu;
   const z64 *g1t = c.gtab + (size_t)(nu - c.nu_lo) * c.nkp * ND2;
-  const z64 *g2t = c.gtab + (size_t)(nu - iwb - c.nu_lo) * c.nkp * ND2;
+  const z64 *g2t = (g2tab ? g2tab : c.gtab) + (size_t)(nu - iwb - c.nu_lo) * c.nkp * ND2;
   z64 acc[ND2];
 #pragma unroll
   for (int a = 0; a < ND2; ++a) acc[a] = make_double2(0.0, 0.0);
@@ -59,11 +60,11 @@ k_chi0(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, z64 *__restric
 }
 
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,
-                        int nnu_all, cudaStream_t st) {
+                        int nnu_all, cudaStream_t st, const z64 *g2tab) {
   if (npts <= 0) return cudaSuccess;
 #define CHI0(NDD, QGG)                                                                      \
   k_chi0<NDD, QGG><<<dim3(nnu_all, cdiv_u(npts, QGG)), QGG * NDD * NDD, 0, st>>>(c, iwb, qidx, \
-                                                                                npts, chi0_all, nnu_all)
+                                                                                npts, chi0_all, nnu_all, g2tab)
   switch (c.nd) {
     case 1: CHI0(1, 128); break;
     case 2: CHI0(2, 32); break;

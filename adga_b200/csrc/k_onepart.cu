@@ -33,6 +33,35 @@ __global__ void k_gtable(DevCtx c, z64 *gtab) {
   for (int i = 0; i < nd * nd; ++i) o[i] = a[i];
 }
 
+// tangent of the G table for a direction dH(k): dG = G dH G (the self-energy,
+// mu and dc are held fixed)
+__global__ void k_gtable_dot(DevCtx c, const z64 *__restrict__ dhk, z64 *__restrict__ gdot) {
+  size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t total = (size_t)c.nkp * c.nnu;
+  if (idx >= total) return;
+  const int k = (int)(idx % c.nkp), nd = c.nd;
+  const z64 *g = c.gtab + idx * c.nd2, *dh = dhk + (size_t)k * c.nd2;
+  z64 t[MAXND * MAXND];
+  for (int i = 0; i < nd; ++i)
+    for (int j = 0; j < nd; ++j) {
+      z64 s = czero<z64>();
+      for (int m = 0; m < nd; ++m) cfma(s, g[i + m * nd], dh[m + j * nd]);
+      t[i + j * nd] = s;
+    }
+  for (int i = 0; i < nd; ++i)
+    for (int j = 0; j < nd; ++j) {
+      z64 s = czero<z64>();
+      for (int m = 0; m < nd; ++m) cfma(s, t[i + m * nd], g[m + j * nd]);
+      gdot[idx * c.nd2 + i + j * nd] = s;
+    }
+}
+
+cudaError_t launch_gtable_dot(const DevCtx &c, const z64 *dhk, z64 *gdot, cudaStream_t st) {
+  size_t total = (size_t)c.nkp * c.nnu;
+  k_gtable_dot<<<cdiv_u(total, 128), 128, 0, st>>>(c, dhk, gdot);
+  return ADGA_LAUNCH_CHECK();
+}
+
 cudaError_t launch_gtable(const DevCtx &c, z64 *gtab, cudaStream_t st) {
   size_t total = (size_t)c.nkp * c.nnu;
   k_gtable<<<cdiv_u(total, 128), 128, 0, st>>>(c, gtab);
@@ -110,7 +139,7 @@ cudaError_t launch_local_diag(const DevCtx &c, int iwb, z64 *c0inv, z64 *c0w, z6
 
 // F~ = sym(chi_loc) * diag(chi0_loc^-1) - 1 (src/main.F90:529-553), written
 // row-major: Frow[r*N + c] = F~(r, c).  chi_loc is column-major.
-__global__ void k_local_F(int N, const z64 *chi, const z64 *c0inv, z64 *Frow) {
+__global__ void k_local_F(int N, const z64 *chi, const z64 *c0inv, z64 *Frow, int minus_one) {
   __shared__ z64 A[32][33];   // A[cc][rr] = chi(r0+rr, c0+cc)
   __shared__ z64 B[32][33];   // B[rr][cc] = chi(c0+cc, r0+rr)
   int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
@@ -128,16 +157,16 @@ __global__ void k_local_F(int N, const z64 *chi, const z64 *c0inv, z64 *Frow) {
       z64 a = A[tx][k], b = B[k][tx];
       z64 s = (r == cc) ? a : make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
       z64 v = cmul(s, c0inv[cc]);
-      if (r == cc) v.x -= 1.0;
+      if (r == cc && minus_one) v.x -= 1.0;
       Frow[(size_t)r * N + cc] = v;
     }
   }
 }
 
 cudaError_t launch_local_F(const DevCtx &c, const z64 *chi_loc, const z64 *c0inv, z64 *Frow,
-                           cudaStream_t st) {
+                           cudaStream_t st, bool minus_one) {
   dim3 grid(cdiv_u(c.N, 32), cdiv_u(c.N, 32));
-  k_local_F<<<grid, dim3(32, 8), 0, st>>>(c.N, chi_loc, c0inv, Frow);
+  k_local_F<<<grid, dim3(32, 8), 0, st>>>(c.N, chi_loc, c0inv, Frow, minus_one ? 1 : 0);
   return ADGA_LAUNCH_CHECK();
 }
 

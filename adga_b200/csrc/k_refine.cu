@@ -28,7 +28,8 @@ __global__ void k_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat,
 }
 
 // XD(i1, i3 + nu*nd2) = sum_i2 X(i1, i2 + nu*nd2) sw_nu(i2, i3), row-major R x N
-__global__ void k_xd(DevCtx c, int npts, const z64 *X, const z64 *chi0q, const z64 *c0inv, z64 *XD) {
+__global__ void k_xd(DevCtx c, int npts, const z64 *X, const z64 *chi0q, const z64 *c0inv, z64 *XD,
+                     int minus_one) {
   const int nd2 = c.nd2, N = c.N;
   size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   size_t per = (size_t)nd2 * N;
@@ -43,7 +44,7 @@ __global__ void k_xd(DevCtx c, int npts, const z64 *X, const z64 *chi0q, const z
   z64 s = make_double2(0.0, 0.0);
   for (int i2 = 0; i2 < nd2; ++i2) {
     z64 sw = cmul(cq[i2], ci);
-    if (i2 == i3) sw.x -= 1.0;
+    if (i2 == i3 && minus_one) sw.x -= 1.0;
     cfma(s, x[i2], sw);
   }
   XD[m * per + e] = s;
@@ -154,10 +155,18 @@ cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *
                             const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, const z64 *extra_d,
                             cudaStream_t st) {
   size_t total = (size_t)c.nd2 * c.N * 2 * npts;
-  k_xd<<<cdiv_u(total, 256), 256, 0, st>>>(c, npts, X, chi0q, c0inv, XD);
+  k_xd<<<cdiv_u(total, 256), 256, 0, st>>>(c, npts, X, chi0q, c0inv, XD, 1);
   cudaError_t e = ADGA_LAUNCH_CHECK();
   if (e != cudaSuccess) return e;
   return launch_resid_z64(c, npts, XD, X, Frow_d, Frow_m, opg_d, opg_m, V, extra_d, st);
+}
+
+// XD = X blockdiag(chi0q chi0_loc^-1 - 1), or without the -1 (a tangent direction)
+cudaError_t launch_xd(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q, const z64 *c0inv, z64 *XD,
+                      bool minus_one, cudaStream_t st) {
+  size_t total = (size_t)c.nd2 * c.N * 2 * npts;
+  k_xd<<<cdiv_u(total, 256), 256, 0, st>>>(c, npts, X, chi0q, c0inv, XD, minus_one ? 1 : 0);
+  return ADGA_LAUNCH_CHECK();
 }
 
 cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,

@@ -230,6 +230,61 @@ class Ladder:
         self._check(self._lib.adga_get_outputs(self._h, C.byref(o)), "get_outputs")
         return out
 
+    # ---- derivatives (forward-mode tangents) ------------------------------
+    def set_tangent(self, dhk=None, du=None, du_tilde=None, direction=0):
+        """Input tangents of parameter direction `direction` (0..3): dH(k)
+        (ndim, ndim, nkp), du and du_tilde (ndim2, ndim2); None = zero."""
+        nd, nd2 = self.ndim, self.ndim2
+        a = None if dhk is None else _z(dhk, (nd, nd, self.nkp))
+        b = None if du is None else _z(du, (nd2, nd2))
+        c = None if du_tilde is None else _z(du_tilde, (nd2, nd2))
+        self._check(self._lib.adga_set_tangent(self._h, int(direction), ptr(a), ptr(b), ptr(c)), "set_tangent")
+
+    def set_vertex_tangent(self, iwb, dchi_loc_dens, dchi_loc_magn, direction=0):
+        """dchi_loc^{dens,magn}(omega = iwb) of a direction (None clears it)."""
+        if dchi_loc_dens is None:
+            self._check(self._lib.adga_set_vertex_tangent(self._h, int(direction), int(iwb), None, None),
+                        "set_vertex_tangent")
+            return
+        N = self.maxdim
+        d, m = _z(dchi_loc_dens, (N, N)), _z(dchi_loc_magn, (N, N))
+        self._check(self._lib.adga_set_vertex_tangent(self._h, int(direction), int(iwb), ptr(d), ptr(m)),
+                    "set_vertex_tangent")
+
+    def clear_tangents(self):
+        self._check(self._lib.adga_clear_tangents(self._h), "clear_tangents")
+
+    def ladder_run_tangent(self, qwstart=1, qwstop=None):
+        """FP64 ladder plus the tangents of every direction set before."""
+        if qwstop is None:
+            qwstop = self.nqp * (2 * self.iwb + 1)
+        n = qwstop - qwstart + 1
+        status = np.zeros(n, dtype=np.int32)
+        st = RunStats()
+        rc = self._lib.adga_ladder_run_tangent(self._h, int(qwstart), int(qwstop),
+                                               status.ctypes.data_as(C.POINTER(C.c_int)), C.byref(st))
+        self._check(rc, "ladder_run_tangent")
+        self.last_npts = n
+        self.last_range = (qwstart, qwstop)
+        return status, st.as_dict()
+
+    def get_tangent_outputs(self, direction=0) -> Dict[str, np.ndarray]:
+        """Tangents of the accumulators of one direction, shapes as get_outputs."""
+        nd, nd2, nw, n = self.ndim, self.ndim2, 2 * self.iwb + 1, self.last_npts
+        z = lambda *s: np.zeros(s, dtype=np.complex128, order="F")
+        out = dict(chi_qw_dens=z(nd2, nd2, n), chi_qw_magn=z(nd2, nd2, n), bubble_nl=z(nd2, nd2, n),
+                   bubble_loc=z(nd2, nd2, nw), chi_loc_dens=z(nd2, nd2, nw),
+                   chi_loc_magn=z(nd2, nd2, nw), sigma_nl=z(nd, nd, 2 * self.iwf, self.nkp_eom),
+                   sigma_dmft=z(nd, nd, 2 * self.iwf), sigma_hf=z(nd, nd, self.nkp_eom))
+        o = Outputs(*[out[k].ctypes.data for k, _ in Outputs._fields_])
+        self._check(self._lib.adga_get_tangent_outputs(self._h, int(direction), C.byref(o)), "get_tangent_outputs")
+        return out
+
+    def assemble_tangent(self, dout):
+        """Tangents of the assembled chi(q, w) and Sigma (siw is held fixed)."""
+        zero_siw = np.zeros((2 * self.iwmax, self.ndim), complex)
+        return self.assemble(dout, zero_siw)
+
     def assemble(self, out, siw):
         """chi(q,w) = chi_nl + bubble_nl + chi_loc(w) (with chi_loc += bubble_loc)
         and Sigma = Sigma_nl + siw (src/main.F90:935-936,1050-1063,1127-1140;

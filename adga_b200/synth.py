@@ -23,6 +23,7 @@ Everything is FP64 / complex128 and deterministic in the seed.
 """
 from __future__ import annotations
 
+import dataclasses
 import math
 from dataclasses import dataclass, field
 from functools import lru_cache
@@ -310,3 +311,67 @@ def _make_vertex(prob: Problem, iwb: int):
         M = np.diag(1.0 / c0) + Gam
         out.append(np.asfortranarray(np.linalg.inv(M)))
     return out[0], out[1]
+
+
+# ---------------------------------------------------------------------------
+# Parameter derivatives of the synthetic model (inputs of the tangent ladder)
+# ---------------------------------------------------------------------------
+PARAMS = ("U", "J", "t")
+
+
+def _vertex_parts(prob: Problem, iwb: int):
+    """(W_d, V_d), (W_m, V_m) of _make_vertex: Gamma_ch = kron(W_ch, V_ch) / beta^2."""
+    spec = prob.spec
+    n2 = 2 * spec.iwf
+    parts = []
+    for ch, V in enumerate((2 * prob.u - prob.u_tilde, -prob.u_tilde)):
+        rng = np.random.default_rng([spec.seed, iwb + 1000, ch])
+        R = rng.uniform(-1, 1, (n2, n2)) + 1j * rng.uniform(-1, 1, (n2, n2))
+        P = 0.5 * (R + R.conj().T)
+        parts.append((1.0 + spec.vertex_eps * P, V))
+    return parts
+
+
+def tangent_inputs(prob: Problem, param: str):
+    """Input tangents (dhk, du, du_tilde, dvertex(iwb)) of the ladder for one
+    model parameter at fixed DMFT one-particle inputs (siw, giw, mu, n_dmft):
+      U, J  Kanamori tensors with V = U - 2J (linear: du = u at unit couplings),
+            and the local vertex chi_loc = (chi0_loc^-1 + Gamma(u, u~))^-1:
+            dchi_loc = -chi_loc dGamma chi_loc;
+      t     the hopping scale: dH/dt (H is linear in t)."""
+    spec = prob.spec
+    nd = spec.ndim
+    if param == "t":
+        hop = dict(spec.hop)
+        hop["t"] = hop["t"] + 1.0
+        dhk = hamiltonian(dataclasses.replace(spec, hop=hop)) - hamiltonian(spec)
+        return np.asfortranarray(dhk), None, None, None
+    if param not in ("U", "J"):
+        raise ValueError(param)
+    cU, cV, cJ = (1.0, 1.0, 0.0) if param == "U" else (0.0, -2.0, 1.0)
+    du, dut = compound_u(kanamori_umat(nd, cU, cV, cJ))
+
+    def dvertex(iwb):
+        chis = prob.vertex(iwb)
+        out = []
+        for (W, _), chi, dV in zip(_vertex_parts(prob, iwb), chis, (2 * du - dut, -dut)):
+            dG = np.kron(W, dV) / prob.beta ** 2
+            out.append(np.asfortranarray(-chi @ dG @ chi))
+        return out[0], out[1]
+
+    return None, du, dut, dvertex
+
+
+def perturbed_problem(prob: Problem, dU=0.0, dJ=0.0, dt=0.0) -> Problem:
+    """The same problem with U, J (V = U - 2J) and the hopping scale t moved,
+    the DMFT one-particle inputs (siw, giw, mu, n_dmft) kept: finite-difference
+    checks of the tangent ladder."""
+    spec = prob.spec
+    hop = dict(spec.hop)
+    if dt:
+        hop["t"] = hop["t"] + dt
+    V = (spec.Vval + dU - 2 * dJ)
+    s2 = dataclasses.replace(spec, U=spec.U + dU, J=spec.J + dJ, V=V, hop=hop)
+    Um = kanamori_umat(s2.ndim, s2.U, s2.Vval, s2.J)
+    u, ut = compound_u(Um)
+    return dataclasses.replace(prob, spec=s2, hk=hamiltonian(s2), u=u, u_tilde=ut, Umat=Um, _vcache={})

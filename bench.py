@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 arm")
+    ap.add_argument("--no-grad", action="store_true",
+                    help="skip the gradient arm (FP64 ladder + tangents in U, J, t)")
     ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--points", type=int, default=0,
@@ -281,6 +283,31 @@ def main():
         ms64, st64, clk64 = timed("fp64")
         res["fp64"] = world * npts * args.steps / (ms64 * 1e-3)
 
+    # gradient arm: the FP64 ladder with the tangents of (U, J, t) in the same
+    # pass (everything the backward of adga_b200.grad needs), on the same steps
+    grad = None
+    if not args.no_grad:
+        for d, par in enumerate(synth.PARAMS):
+            dhk, du, dut, dvertex = synth.tangent_inputs(p, par)
+            lad.set_tangent(dhk, du, dut, direction=d)
+            if dvertex is not None:
+                for iwb in sorted(set(omegas)):
+                    lad.set_vertex_tangent(iwb, *dvertex(iwb), direction=d)
+        p.clear_vertex_cache()
+        for s in range(args.warmup):
+            lad.ladder_run_tangent(*slice_range(omegas[s]))
+        barrier()
+        ms_g = 0.0
+        for s in range(args.warmup, nsteps):
+            ms_g += lad.ladder_run_tangent(*slice_range(omegas[s]))[1]["ms_total"]
+        barrier()
+        ms_g = allmax(ms_g)
+        lad.clear_tangents()
+        grad = {"directions": list(synth.PARAMS), "value": world * npts * args.steps / (ms_g * 1e-3),
+                "unit": UNIT, "ms_per_step": ms_g / args.steps,
+                "over_fp64_forward": (ms_g / ms64) if not args.no_fp64 else None,
+                "over_mixed_forward": ms_g / ms_mixed}
+
     # accuracy: mixed vs FP64 on the same slice, and vs the oracle on sampled points
     iwb_chk = omegas[-1]
     acc = {}
@@ -368,6 +395,7 @@ def main():
             "accuracy": acc, "stage_ms_per_step": stage,
             "refine": {"max_iters": max(s["max_refine_iters"] for s in st_mixed),
                        "fallbacks": sum(s["mixed_fallbacks"] for s in st_mixed)},
+            "gradient": grad,
             "roofline": roof, "cpu_baseline": cpu_line, "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in st_mixed)),
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}

@@ -225,6 +225,34 @@ typedef struct adga_outputs {
 } adga_outputs;
 int adga_get_outputs(adga_handle *h, const adga_outputs *o);
 
+/*
+ * Derivatives of the FP64 ladder outputs along up to ADGA_MAX_TANGENTS
+ * parameter directions at once (forward-mode tangents; the gradient of any
+ * scalar of chi and Sigma follows by contraction).  Direction dir is given by
+ * its input tangents, each optional (NULL = zero): dH(k) (ndim, ndim, nkp), du
+ * and du_tilde (ndim2, ndim2), and per omega dchi_loc^{dens,magn}
+ * (maxdim x maxdim).  The DMFT one-particle inputs (siw, giw, mu, dc,
+ * n_dmft) are held fixed.  The tangent follows every stage of the loop:
+ * dG = G dH G in chi0 and the EOM, d(F~) = sym(dchi_loc) chi0_loc^-1,
+ * dX = (d(1+gamma^w) - X dA) A^-1 through the BSE (d(A^-1) = -A^-1 dA A^-1,
+ * with the LU factors of the forward solve), the chi sums and m_tot.
+ * adga_ladder_run_tangent runs the FP64 ladder over qwstart..qwstop once (its
+ * forward outputs accumulate as with adga_ladder_run) together with every
+ * direction set; adga_get_tangent_outputs returns direction dir in the layouts
+ * of adga_get_outputs (bubble_loc and sigma_hf: zero).  Not with V(q).
+ * adga_clear_tangents drops every direction.
+ */
+#define ADGA_MAX_TANGENTS 4
+int adga_set_tangent(adga_handle *h, int dir, const adga_z *dhk, const adga_z *du,
+                     const adga_z *du_tilde);
+int adga_set_vertex_tangent(adga_handle *h, int dir, int iwb, const adga_z *dchi_loc_dens,
+                            const adga_z *dchi_loc_magn);
+int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, int *status,
+                            adga_run_stats *stats);
+int adga_get_tangent_outputs(adga_handle *h, int dir, const adga_outputs *o);
+int adga_clear_tangents(adga_handle *h);
+
+
 /* ---- per-routine entry points (one (q, omega) point, host buffers) ---- */
 
 /* diag of chi0_loc / chi0_loc^-1 at (iwf, iwb) as ndim2 x ndim2 matrices;
