@@ -88,6 +88,7 @@ struct adga_handle {
 struct TanState {
   bool has_dhk = false;
   z64 *gdot = nullptr, *du = nullptr, *dut = nullptr;
+  z64 *ghat_dot = nullptr;                 // transform of gdot (transform path only)
   std::vector<z64 *> vd, vm;               // dchi_loc per omega (N x N), or null
   z64 *Fd = nullptr, *Fm = nullptr, *gd = nullptr, *gm = nullptr;
   int loc_iwb = INT_MIN;
@@ -149,6 +150,78 @@ extern "C" const char *adga_last_error(const adga_handle *h) {
 }
 
 // ---------------------------------------------------------------------------
+// Transform path (k_dft.cu): the fold mesh of the q points, their indices on it,
+// twiddles, G^ and scratch.  ADGA_DFT_MIN_POINTS sets the smallest batch that
+// uses it (default 4); ADGA_BUBBLE=direct keeps the direct kernels only.  If its
+// buffers cannot be allocated the direct kernels are used.
+static int gcd_int(int a, int b) {
+  while (b) { const int t = a % b; a = b; b = t; }
+  return a;
+}
+
+static int setup_dft(adga_handle *h, const int *q_data) {
+  DevCtx &c = h->c;
+  c.dft = DftView{};
+  const char *mode = getenv("ADGA_BUBBLE");
+  if (mode && !strcmp(mode, "direct")) return 0;
+  const char *mp = getenv("ADGA_DFT_MIN_POINTS");
+  c.dft.min_points = mp ? std::max(1, atoi(mp)) : 4;
+  const int nk[3] = {c.nkpx, c.nkpy, c.nkpz};
+  std::vector<int> qc(3 * (size_t)c.nqp);
+  int s[3] = {nk[0], nk[1], nk[2]};
+  for (int q = 0; q < c.nqp; ++q) {
+    const int k0 = q_data[q] - 1;
+    if (k0 < 0 || k0 >= c.nkp) return fail(h, ADGA_EINVAL, "q_data outside the k mesh");
+    qc[3 * q] = k0 / (nk[1] * nk[2]);
+    qc[3 * q + 1] = (k0 / nk[2]) % nk[1];
+    qc[3 * q + 2] = k0 % nk[2];
+    for (int ax = 0; ax < 3; ++ax) s[ax] = gcd_int(s[ax], qc[3 * q + ax]);
+  }
+  for (int ax = 0; ax < 3; ++ax) c.dft.m[ax] = nk[ax] / s[ax];
+  const int m3 = c.dft.m[0] * c.dft.m[1] * c.dft.m[2];
+  std::vector<int> ql(c.nqp);
+  for (int q = 0; q < c.nqp; ++q) {
+    const int ax = qc[3 * q] / s[0], ay = qc[3 * q + 1] / s[1], az = qc[3 * q + 2] / s[2];
+    ql[q] = az + c.dft.m[2] * (ay + c.dft.m[1] * ax);
+  }
+  std::vector<double2> tw;
+  int off[6];
+  const int lens[6] = {nk[0], nk[1], nk[2], c.dft.m[0], c.dft.m[1], c.dft.m[2]};
+  for (int i = 0; i < 6; ++i) {
+    off[i] = (int)tw.size();
+    for (int j = 0; j < lens[i]; ++j) {
+      const long double ang = 2.0L * 3.141592653589793238462643383279502884L * j / lens[i];
+      tw.push_back(make_double2((double)cosl(ang), (double)sinl(ang)));
+    }
+  }
+  const size_t nd4 = (size_t)c.nd2 * c.nd2;
+  const size_t scr = std::max({(size_t)h->nnu_all * m3 * nd4, (size_t)c.iwf * m3 * nd4,
+                               (size_t)c.iwf * c.nkp * c.nd2, (size_t)c.nnu * c.nkp * c.nd2});
+  auto &L = h->owned;
+  z64 *ghat, *a, *b;
+  int *qlin;
+  double2 *twd;
+  if (!alloc_into(h, ghat, (size_t)c.nnu * c.nkp * c.nd2, L) || !alloc_into(h, a, scr, L) ||
+      !alloc_into(h, b, scr, L) || !alloc_into(h, qlin, c.nqp, L) || !alloc_into(h, twd, tw.size(), L)) {
+    h->err.clear();
+    c.dft = DftView{};
+    return 0;
+  }
+  CK(cudaMemcpyAsync(qlin, ql.data(), sizeof(int) * c.nqp, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(twd, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice, h->st));
+  c.dft.qlin = qlin;
+  for (int i = 0; i < 3; ++i) {
+    c.dft.twk[i] = twd + off[i];
+    c.dft.twm[i] = twd + off[3 + i];
+  }
+  c.dft.a = a;
+  c.dft.b = b;
+  CK(launch_gtable_dft(c, c.gtab, ghat, a, h->st));
+  CK(cudaStreamSynchronize(h->st));   // the host vectors above go out of scope
+  c.dft.ghat = ghat;
+  return 0;
+}
+
 extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga_z *hk,
                            const adga_z *siw, const adga_z *giw, const adga_z *dc,
                            const adga_z *u, const adga_z *u_tilde, const adga_z *n_dmft,
@@ -229,6 +302,7 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   else
     CK(launch_kq_index(c.nkpx, c.nkpy, c.nkpz, kde, c.nkp_eom, qd, c.nqp, 0, kqe, st));
   CK(launch_gtable(c, gt, st));
+  if (int rd = setup_dft(h, q_data)) { adga_destroy(h); return rd; }
   // per-omega local buffers and accumulators
   const size_t N = c.N;
   ok = alloc_into(h, h->c0inv, N, L) && alloc_into(h, h->c0w, N, L) &&
@@ -689,6 +763,7 @@ static int tan_state(adga_handle *h, int d) {
             alloc_into(h, t->chi_loc_d, nd2 * nd2 * nw, L) && alloc_into(h, t->chi_loc_m, nd2 * nd2 * nw, L) &&
             alloc_into(h, t->sigma_nl, nd2 * 2 * c.iwf * (size_t)c.nkp_eom, L) &&
             alloc_into(h, t->sigma_dmft, nd2 * 2 * c.iwf, L);
+  if (ok && c.dft.ghat) ok = alloc_into(h, t->ghat_dot, (size_t)c.nnu * c.nkp * nd2, L);
   if (!ok) return fail(h, ADGA_ENOMEM, "tangent direction");
   CK(cudaMemsetAsync(t->du, 0, sizeof(z64) * nd2 * nd2, h->st));
   CK(cudaMemsetAsync(t->dut, 0, sizeof(z64) * nd2 * nd2, h->st));
@@ -736,6 +811,7 @@ extern "C" int adga_set_tangent(adga_handle *h, int dir, const adga_z *dhk, cons
     if (cudaMalloc(&dh, sizeof(z64) * c.nd2 * c.nkp) != cudaSuccess) return fail(h, ADGA_ENOMEM, "dhk");
     cudaError_t e = cudaMemcpyAsync(dh, dhk, sizeof(z64) * c.nd2 * c.nkp, cudaMemcpyHostToDevice, h->st);
     if (e == cudaSuccess) e = launch_gtable_dot(c, dh, t->gdot, h->st);   // dG = G dH G
+    if (e == cudaSuccess && t->ghat_dot) e = launch_gtable_dft(c, t->gdot, t->ghat_dot, c.dft.a, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     cudaFree(dh);
     if (e != cudaSuccess) return fail(h, ADGA_ECUDA, "set_tangent: dG table");
@@ -834,8 +910,9 @@ static int tan_batch(adga_handle *h, int d, int iwb, int np, int off, z64 *T, LU
   if (t->has_dhk) {
     DevCtx cg = c;
     cg.gtab = t->gdot;
-    CK(launch_chi0(cg, iwb, h->qidx_d, np, w->chi0_all, h->nnu_all, st, c.gtab));
-    CK(launch_chi0(c, iwb, h->qidx_d, np, w->chi0_tmp, h->nnu_all, st, t->gdot));
+    cg.dft.ghat = t->ghat_dot;
+    CK(launch_chi0(cg, iwb, h->qidx_d, np, w->chi0_all, h->nnu_all, st, c.gtab, c.dft.ghat));
+    CK(launch_chi0(c, iwb, h->qidx_d, np, w->chi0_tmp, h->nnu_all, st, t->gdot, t->ghat_dot));
     CK(launch_zadd((size_t)np * h->nd4 * h->nnu_all, w->chi0_tmp, w->chi0_all, st));
     dchi0q = h->bigbox ? w->chi0q_big : w->chi0_all;
     CK(launch_chi0_finish(c, w->chi0_all, h->nnu_all, np, w->zero_nd4, h->bigbox ? w->chi0q_big : nullptr,
@@ -883,6 +960,7 @@ static int tan_batch(adga_handle *h, int d, int iwb, int np, int off, z64 *T, LU
     if (t->has_dhk) {
       DevCtx cg = c;
       cg.gtab = t->gdot;
+      cg.dft.ghat = t->ghat_dot;
       CK(launch_eom_dynamic(cg, iwb, h->qidx_d, np, h->mtot, t->sigma_nl, st));
     }
   }

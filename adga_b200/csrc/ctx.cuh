@@ -4,6 +4,19 @@
 #include "common.cuh"
 #include "adga.h"
 
+// Transform path of the bubble and the EOM (k_dft.cu): G^ = DFT over k of the G
+// table, the fold mesh m of the q points (q = (n/m).a per axis) with each q's
+// linear index a on it, twiddle tables e^{2 pi i j/n} of the k and m axes, and
+// two scratch arrays of max(nnu_all m^3 nd2^2, iwf m^3 nd2^2, iwf nkp nd2) elements.
+struct DftView {
+  const z64 *ghat;               // null: the direct k-sum kernels only
+  int m[3];
+  int min_points;                // batches with fewer points use the direct kernels
+  const int *qlin;               // (nqp)
+  const double2 *twk[3], *twm[3];
+  z64 *a, *b;
+};
+
 struct DevCtx {
   int nd, nd2, nkp, nqp, nkp_eom;
   int nkpx, nkpy, nkpz;
@@ -24,6 +37,7 @@ struct DevCtx {
   const z64 *vq;                 // V(q) (nd2, nd2, nqp) in read_vq's layout, null without do_vq
   const z64 *nfock;              // n_fock(k, i, j) (nkp, nd, nd), with vq
   const z64 *gtab;               // G(k, nu): [(nu - nu_lo)*nkp + k][nd2], column-major nd x nd
+  DftView dft;
 };
 
 // correlated-subspace atom (1-based) of every band, 0 for uncorrelated bands
@@ -85,9 +99,19 @@ cudaError_t launch_gamq_tan(const DevCtx &c, int npts, const z64 *chi0q, const z
 cudaError_t launch_zadd(size_t n, const z64 *x, z64 *y, cudaStream_t st);
 
 // k_chi0.cu: chi0q[p] (nd2, nd2, nnu_out) for a batch of points at one omega
-// (the G(k-q, nu-omega) factor from g2tab when given: tangents)
+// (the G(k-q, nu-omega) factor from g2tab, with its transform g2hat, when given:
+// tangents); the transform path when c.dft.ghat is set and the batch is large enough
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,
-                        int nnu_all, cudaStream_t st, const z64 *g2tab = nullptr);
+                        int nnu_all, cudaStream_t st, const z64 *g2tab = nullptr, const z64 *g2hat = nullptr);
+
+// k_dft.cu: transforms (see DftView)
+z64 *dft3(const z64 *src, z64 *x, z64 *y, int batch, const int n[3], const double2 *const tw[3], int C,
+          double sign, cudaStream_t st, cudaError_t *err);
+cudaError_t launch_gtable_dft(const DevCtx &c, const z64 *gtab, z64 *ghat, z64 *scratch, cudaStream_t st);
+cudaError_t launch_chi0_dft(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all, int nnu_all,
+                            const z64 *ghat1, const z64 *ghat2, cudaStream_t st);
+cudaError_t launch_eom_dft(const DevCtx &c, int iwb, const int *qidx, int npts, const z64 *mtot, const z64 *ghat,
+                           z64 *sigma, cudaStream_t st);
 cudaError_t launch_chi0_finish(const DevCtx &c, const z64 *chi0_all, int nnu_all, int npts,
                                const z64 *bubloc_tmp, z64 *chi0q, z64 *bubble_nl, cudaStream_t st);
 

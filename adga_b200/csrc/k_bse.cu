@@ -253,6 +253,8 @@ k_eom_dyn(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, const z64 *
 cudaError_t launch_eom_dynamic(const DevCtx &c, int iwb, const int *qidx, int npts,
                                const z64 *mtot, z64 *sigma_nl, cudaStream_t st) {
   if (npts <= 0) return cudaSuccess;
+  if (c.dft.ghat && npts >= c.dft.min_points)
+    return launch_eom_dft(c, iwb, qidx, npts, mtot, c.dft.ghat, sigma_nl, st);
   dim3 grid(cdiv_u(c.nkp_eom, 128), c.iwf);
   switch (c.nd) {
     case 1: k_eom_dyn<1><<<grid, 128, 0, st>>>(c, iwb, qidx, npts, mtot, sigma_nl); break;

@@ -60,8 +60,10 @@ k_chi0(DevCtx c, int iwb, const int *__restrict__ qidx, int npts, z64 *__restric
 }
 
 cudaError_t launch_chi0(const DevCtx &c, int iwb, const int *qidx, int npts, z64 *chi0_all,
-                        int nnu_all, cudaStream_t st, const z64 *g2tab) {
+                        int nnu_all, cudaStream_t st, const z64 *g2tab, const z64 *g2hat) {
   if (npts <= 0) return cudaSuccess;
+  if (c.dft.ghat && npts >= c.dft.min_points && (!g2tab || g2hat))
+    return launch_chi0_dft(c, iwb, qidx, npts, chi0_all, nnu_all, c.dft.ghat, g2tab ? g2hat : c.dft.ghat, st);
 #define CHI0(NDD, QGG)                                                                      \
   k_chi0<NDD, QGG><<<dim3(nnu_all, cdiv_u(npts, QGG)), QGG * NDD * NDD, 0, st>>>(c, iwb, qidx, \
                                                                                 npts, chi0_all, nnu_all, g2tab)
