@@ -59,6 +59,8 @@ struct adga_handle {
   z64 *c0inv = nullptr, *c0w = nullptr, *bubtmp = nullptr;
   z64 *Frow_d = nullptr, *Frow_m = nullptr, *gam_d = nullptr, *gam_m = nullptr;
   z64 *opg_d = nullptr, *opg_m = nullptr;
+  z32 *Frow32_m = nullptr;       // FP32 copy of F~_m for the mixed build, valid for omega f32_iwb
+  int f32_iwb = INT_MIN;
   // accumulators
   z64 *bubble_loc = nullptr, *chi_loc_d = nullptr, *chi_loc_m = nullptr;
   z64 *sigma_nl = nullptr, *sigma_dmft = nullptr, *sigma_hf = nullptr;
@@ -309,7 +311,7 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
        alloc_into(h, h->bubtmp, nd2 * nd2, L) && alloc_into(h, h->Frow_d, N * N, L) &&
        alloc_into(h, h->Frow_m, N * N, L) && alloc_into(h, h->gam_d, nd2 * N, L) &&
        alloc_into(h, h->gam_m, nd2 * N, L) && alloc_into(h, h->opg_d, nd2 * N, L) &&
-       alloc_into(h, h->opg_m, nd2 * N, L) &&
+       alloc_into(h, h->opg_m, nd2 * N, L) && alloc_into(h, h->Frow32_m, N * N, L) &&
        alloc_into(h, h->bubble_loc, (size_t)h->nd4 * h->nw, L) &&
        alloc_into(h, h->chi_loc_d, (size_t)h->nd4 * h->nw, L) &&
        alloc_into(h, h->chi_loc_m, (size_t)h->nd4 * h->nw, L) &&
@@ -588,6 +590,7 @@ static int ensure_local(adga_handle *h, int iwb) {
   if (r) return r;
   CK(launch_local_F(h->c, h->vd[w], h->c0inv, h->Frow_d, h->st));
   CK(launch_local_F(h->c, h->vm[w], h->c0inv, h->Frow_m, h->st));
+  h->f32_iwb = INT_MIN;
   if (h->tl_d[w]) {
     // external three-leg vertex (src/main.F90:560-561), then 1 + gamma^w
     const size_t ng = (size_t)h->c.nd2 * h->c.N;
@@ -1026,8 +1029,12 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     X = T + N * N; sp = 2 * strideM; sc = strideM;
   } else {
     z32 *T = (z32 *)h->Tm;
+    if (h->f32_iwb != iwb) {
+      CK(launch_to32(N * N, h->Frow_m, h->Frow32_m, st));
+      h->f32_iwb = iwb;
+    }
     CK(launch_bse_build<z32>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
-                             strideM, h->gq, h->qidx_d, st));
+                             strideM, h->gq, h->qidx_d, st, h->Frow32_m));
     cudaEventRecord(ev[2], st);
     CK(factor_batch<z32>(h, T, lb, true, h->tc != nullptr, &tt));
     CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));

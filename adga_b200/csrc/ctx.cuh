@@ -120,7 +120,9 @@ template <typename T>
 cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const z64 *c0inv,
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, T *Tmat, size_t strideM, z64 *gammaqd,
-                             const int *qidx, cudaStream_t st);
+                             const int *qidx, cudaStream_t st, const z32 *F32_m = nullptr);
+// FP32 copy of an N x N FP64 matrix (the magnetic F~ of the mixed build)
+cudaError_t launch_to32(size_t n, const z64 *x, z32 *y, cudaStream_t st);
 // X of point p, channel ch at X + p*sp + ch*sc: N x R column-major (ld ldX)
 cudaError_t launch_post(const DevCtx &c, int npts, const z64 *X, size_t sp, size_t sc, int ldX,
                         const z64 *opg_d, const z64 *opg_m, const z64 *gam_d, const z64 *gam_m,

@@ -9,6 +9,8 @@
 //   * eom    -- Sigma(k, nu) += m_tot G(k-q, nu-w) over a batch of points
 //               (src/eom_module.f90:209-230), one owner thread per (k, nu).
 #include "ctx.cuh"
+#include <algorithm>
+#include <type_traits>
 
 // ---------------------------------------------------------------------------
 // build: one block per (column tile of A^T rows c, channel, point).
@@ -85,12 +87,179 @@ k_bse_build(DevCtx c, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0i
   }
 }
 
+// Fast build (no V(q) term): one block per (128-column tile, P points) of one
+// channel.  A thread owns one column c of T; the F~ rows of each nu block are
+// staged into shared memory one nu ahead by cp.async (each thread copies and
+// reads only its own column), and sw_nu of the block's points is formed in
+// shared memory one nu ahead from chi0^q / chi0_loc^-1 values prefetched into
+// registers; one barrier per nu.  F32 selects complex FP32 arithmetic from an
+// FP32 copy of F~ -- used for the magnetic channel of the mixed path, whose T
+// only feeds the FP32 LU (the FP64 residual of the refinement restores the
+// FP64 answer); GQ accumulates gamma^q_d (the density channel, always FP64).
+template <int ND2, bool GQ> struct BuildP { static constexpr int P = GQ ? 1 : 2; };
+
+__device__ __forceinline__ void cp_async_bytes(void *smem, const void *gmem, int pred16or8, int nbytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (pred16or8 == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(nbytes));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(nbytes));
+}
+
+template <typename TW, int ND2, bool F32, bool GQ>
+__global__ void __launch_bounds__(128)
+k_bse_build_fast(DevCtx c, int npts, int ch, const z64 *__restrict__ chi0q, const z64 *__restrict__ c0inv,
+                 const void *__restrict__ Fv, const z64 *__restrict__ opg, TW *Tm, size_t strideM, z64 *gammaqd) {
+  typedef typename std::conditional<F32, z32, z64>::type A;
+  constexpr int P = BuildP<ND2, GQ>::P, ND4 = ND2 * ND2, NE = P * ND4, EPT = (NE + 127) / 128;
+  __shared__ __align__(16) A fs[2][ND2][128];
+  __shared__ __align__(16) A sws[2][NE];
+  const A *F = (const A *)Fv;
+  const int N = c.N, nnu = 2 * c.iwf, t = threadIdx.x;
+  const int cc = blockIdx.x * 128 + t, p0 = blockIdx.y * P;
+  const bool act = cc < N;
+  z64 pc[EPT], pinv[EPT];
+  auto load_sw = [&](int dum) {
+#pragma unroll
+    for (int k = 0; k < EPT; ++k) {
+      const int e = t + 128 * k;
+      if (e < NE) {
+        const int pp = e / ND4, el = e % ND4, i3 = el / ND2;
+        const int p = p0 + pp;
+        pc[k] = p < npts ? chi0q[((size_t)p * nnu + dum) * ND4 + el] : make_double2(0.0, 0.0);
+        pinv[k] = c0inv[dum * ND2 + i3];
+      }
+    }
+  };
+  auto store_sw = [&](int buf) {
+#pragma unroll
+    for (int k = 0; k < EPT; ++k) {
+      const int e = t + 128 * k;
+      if (e < NE) {
+        const int el = e % ND4, i1 = el % ND2, i3 = el / ND2;
+        z64 v = cmul(pc[k], pinv[k]);
+        if (i1 == i3) v.x -= 1.0;
+        if constexpr (F32) sws[buf][e] = to32(v);
+        else sws[buf][e] = v;
+      }
+    }
+  };
+  auto stage_f = [&](int dum, int buf) {
+#pragma unroll
+    for (int i3 = 0; i3 < ND2; ++i3) {
+      const A *g = F + (size_t)(i3 + dum * ND2) * N + (act ? cc : 0);
+      cp_async_bytes(&fs[buf][i3][t], g, (int)sizeof(A), act ? (int)sizeof(A) : 0);
+    }
+    asm volatile("cp.async.commit_group;");
+  };
+  z64 gq[GQ ? P * ND2 : 1];
+  if constexpr (GQ) {
+#pragma unroll
+    for (int a = 0; a < P * ND2; ++a) gq[a] = make_double2(0.0, 0.0);
+  }
+  stage_f(0, 0);
+  load_sw(0);
+  store_sw(0);
+  __syncthreads();
+  for (int dum = 0; dum < nnu; ++dum) {
+    const bool more = dum + 1 < nnu;
+    if (more) {
+      stage_f(dum + 1, (dum + 1) & 1);
+      load_sw(dum + 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    const A *sw = sws[dum & 1];
+    A f[ND2];
+#pragma unroll
+    for (int i3 = 0; i3 < ND2; ++i3) f[i3] = fs[dum & 1][i3][t];
+#pragma unroll
+    for (int pp = 0; pp < P; ++pp) {
+      const int p = p0 + pp;
+      if (act && p < npts) {
+        TW *Tp = Tm + (size_t)(2 * p + ch) * strideM;
+#pragma unroll
+        for (int i1 = 0; i1 < ND2; ++i1) {
+          A w = cx<A>::make(0, 0);
+#pragma unroll
+          for (int i3 = 0; i3 < ND2; ++i3) cfma(w, sw[pp * ND4 + i1 + i3 * ND2], f[i3]);
+          const int r = i1 + dum * ND2;
+          A tv = cx<A>::make(-w.x, -w.y);
+          if (r == cc) tv.x += 1;
+          if constexpr (F32) Tp[cc + (size_t)r * N] = tv;
+          else Tp[cc + (size_t)r * N] = from64<TW>(tv);
+          if constexpr (GQ) gq[pp * ND2 + i1] = cadd(gq[pp * ND2 + i1], w);
+        }
+      }
+    }
+    if (more) store_sw((dum + 1) & 1);
+    __syncthreads();
+  }
+  if (!act) return;
+#pragma unroll
+  for (int pp = 0; pp < P; ++pp) {
+    const int p = p0 + pp;
+    if (p >= npts) continue;
+    TW *Tp = Tm + (size_t)(2 * p + ch) * strideM;
+#pragma unroll
+    for (int i1 = 0; i1 < ND2; ++i1) Tp[cc + (size_t)(N + i1) * N] = from64<TW>(opg[i1 + (size_t)cc * ND2]);
+    if constexpr (GQ) {
+      if (gammaqd) {
+        z64 *g = gammaqd + (size_t)p * ND2 * N;
+#pragma unroll
+        for (int i1 = 0; i1 < ND2; ++i1) g[i1 + (size_t)cc * ND2] = gq[pp * ND2 + i1];
+      }
+    }
+  }
+}
+
+__global__ void k_to32(size_t n, const z64 *__restrict__ x, z32 *__restrict__ y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = to32(x[i]);
+}
+
+cudaError_t launch_to32(size_t n, const z64 *x, z32 *y, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  k_to32<<<(unsigned)std::min<size_t>(cdiv_u(n, 256), 4096), 256, 0, st>>>(n, x, y);
+  return ADGA_LAUNCH_CHECK();
+}
+
 template <typename T>
 cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const z64 *c0inv,
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, T *Tmat, size_t strideM, z64 *gammaqd,
-                             const int *qidx, cudaStream_t st) {
+                             const int *qidx, cudaStream_t st, const z32 *F32_m) {
   if (npts <= 0) return cudaSuccess;
+  if (!c.vq && c.nd2 <= 9) {
+    cudaError_t e = cudaSuccess;
+#define FAST(NDD)                                                                                          \
+  {                                                                                                        \
+    dim3 g(cdiv_u(c.N, 128), cdiv_u(npts, BuildP<NDD, true>::P));                                         \
+    k_bse_build_fast<T, NDD, false, true><<<g, 128, 0, st>>>(c, npts, 0, chi0q, c0inv, Frow_d, opg_d,      \
+                                                             Tmat, strideM, gammaqd);                      \
+    if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;                                                \
+    g.y = cdiv_u(npts, BuildP<NDD, false>::P);                                                             \
+    bool done = false;                                                                                     \
+    if constexpr (std::is_same<T, z32>::value) {                                                           \
+      if (F32_m) {                                                                                         \
+        k_bse_build_fast<T, NDD, true, false><<<g, 128, 0, st>>>(c, npts, 1, chi0q, c0inv, F32_m, opg_m,   \
+                                                                 Tmat, strideM, nullptr);                  \
+        done = true;                                                                                       \
+      }                                                                                                    \
+    }                                                                                                      \
+    if (!done)                                                                                             \
+      k_bse_build_fast<T, NDD, false, false><<<g, 128, 0, st>>>(c, npts, 1, chi0q, c0inv, Frow_m, opg_m,   \
+                                                                Tmat, strideM, nullptr);                   \
+  }
+    switch (c.nd2) {      // nd <= 3; larger orbital counts take the general kernel below
+      case 1: FAST(1); break;
+      case 4: FAST(4); break;
+      case 9: FAST(9); break;
+    }
+#undef FAST
+    if (c.nd2 <= 9) return ADGA_LAUNCH_CHECK();
+  }
   dim3 grid(cdiv_u(c.N, 128), 2, npts);
 #define BUILD(NDD)                                                                            \
   k_bse_build<T, NDD><<<grid, 128, 0, st>>>(c, chi0q, c0inv, Frow_d, Frow_m, opg_d, opg_m,     \
@@ -108,10 +277,10 @@ cudaError_t launch_bse_build(const DevCtx &c, int npts, const z64 *chi0q, const 
 }
 template cudaError_t launch_bse_build<z64>(const DevCtx &, int, const z64 *, const z64 *,
                                            const z64 *, const z64 *, const z64 *, const z64 *,
-                                           z64 *, size_t, z64 *, const int *, cudaStream_t);
+                                           z64 *, size_t, z64 *, const int *, cudaStream_t, const z32 *);
 template cudaError_t launch_bse_build<z32>(const DevCtx &, int, const z64 *, const z64 *,
                                            const z64 *, const z64 *, const z64 *, const z64 *,
-                                           z32 *, size_t, z64 *, const int *, cudaStream_t);
+                                           z32 *, size_t, z64 *, const int *, cudaStream_t, const z32 *);
 
 // ---------------------------------------------------------------------------
 // post: one block per point.
