@@ -81,6 +81,7 @@ struct adga_handle {
   void *tc = nullptr;
   // refinement settings
   int max_iter = 8;
+  bool mixed_nopiv = true;   // FP32 factorisation without row interchanges (ADGA_MIXED_PIVOT=1: with)
   double tol = 1e-10;   // stop when max|dX| <= tol * max|X| (the error is then far below)
   // last-run statistics
   adga_run_stats stats{};
@@ -258,6 +259,8 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   h->nnu_all = d->iwstop - d->iwstart + 1;
   h->bigbox = h->nnu_all != 2 * c.iwf;
   h->nd4 = c.nd2 * c.nd2;
+  if (const char *mpv = getenv("ADGA_MIXED_PIVOT")) h->mixed_nopiv = atoi(mpv) == 0;
+  if (const char *mr = getenv("ADGA_MAX_REFINE")) h->max_iter = std::max(1, atoi(mr));
   const char *ev = getenv("ADGA_NB");
   if (ev) h->NB = std::max(16, std::min(64, atoi(ev) / 8 * 8));   // the LU kernels assume NB <= 64
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -694,14 +697,14 @@ static void stage_ms(adga_handle *h, double *acc, cudaEvent_t a, cudaEvent_t b) 
 // (first half's) trailing updates.
 template <typename T>
 static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool apply_left, bool tc,
-                                TrailTiming *tt) {
+                                TrailTiming *tt, bool nopiv = false) {
   cudaStream_t st = h->st;
   // measured: the trailing-update grids fill every SM, so the split gives no
   // overlap on the t2g workload; kept as an option (ADGA_TWO_STREAMS=1)
   const bool split = h->st2 && lb.batch >= 8 && getenv("ADGA_TWO_STREAMS");
   if (!split) {
     TcRange r{h->tc, 0, lb.batch};
-    return lu_factor<T>(M, lb, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &r : nullptr, st, tt);
+    return lu_factor<T>(M, lb, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &r : nullptr, st, tt, nopiv);
   }
   const int na = lb.batch / 2, nb = lb.batch - na;
   LUBatch la = lu_sub<T>(lb, 0, na), lbb = lu_sub<T>(lb, na, nb);
@@ -710,10 +713,10 @@ static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool ap
   cudaError_t e = cudaEventRecord(h->fork, st);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(h->st2, h->fork, 0);
   for (int s = 0; e == cudaSuccess && s < lb.nsteps(); ++s) {
-    e = lu_step<T>(M, la, s, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &ra : nullptr, st, tt);
+    e = lu_step<T>(M, la, s, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &ra : nullptr, st, tt, nopiv);
     if (e == cudaSuccess)
       e = lu_step<T>(Mb, lbb, s, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &rb : nullptr, h->st2,
-                     nullptr);
+                     nullptr, nopiv);
   }
   if (e == cudaSuccess) e = cudaEventRecord(h->join, h->st2);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->join, 0);
@@ -1036,7 +1039,7 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     CK(launch_bse_build<z32>(c, np, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, T,
                              strideM, h->gq, h->qidx_d, st, h->Frow32_m));
     cudaEventRecord(ev[2], st);
-    CK(factor_batch<z32>(h, T, lb, true, h->tc != nullptr, &tt));
+    CK(factor_batch<z32>(h, T, lb, true, h->tc != nullptr, &tt, h->mixed_nopiv));
     CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     CK(launch_init_x(T, strideM, (int)N, (int)R, 2 * np, h->X64, st));
     CK(lu_build_perm(lb, h->perm, st));

@@ -43,13 +43,15 @@ struct TrailTiming {
   double gflop = 0.0;          // algorithmic flops of the recorded updates
   double gbytes = 0.0;         // algorithmic HBM bytes: C read+write, L21 and U12 read once
 };
+// nopiv: no row interchanges (identity ipiv, empty maps); the mixed path's
+// FP32 factorisation, whose refinement falls back to the pivoted FP64 path
 template <typename T>
 cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, void *trail_ctx,
-                      cudaStream_t st, TrailTiming *tt = nullptr);
+                      cudaStream_t st, TrailTiming *tt = nullptr, bool nopiv = false);
 // one step s (panel, block inverses, interchanges + U12, trailing update)
 template <typename T>
 cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
-                    cudaStream_t st, TrailTiming *tt = nullptr);
+                    cudaStream_t st, TrailTiming *tt = nullptr, bool nopiv = false);
 // the matrices [first, first + count) of a batch as a batch of their own
 template <typename T>
 inline LUBatch lu_sub(const LUBatch &lb, int first, int count) {

@@ -1,4 +1,6 @@
 """Shared helpers of the test-suite: problem cache, oracle adapters, errors."""
+import contextlib
+import os
 from functools import lru_cache
 
 import numpy as np
@@ -42,3 +44,24 @@ def rel_err(a, b):
     if den == 0:
         return float(np.max(np.abs(a)))
     return float(np.max(np.abs(a - b)) / den)
+
+
+LIBRARY_ENV = ("ADGA_DFT_MIN_POINTS", "ADGA_BUBBLE", "ADGA_MIXED_PIVOT", "ADGA_MAX_REFINE")
+
+
+@contextlib.contextmanager
+def library_env(settings):
+    """The library's ADGA_* switches (read when a handle is created) set to
+    `settings` and every other one unset, restored afterwards."""
+    old = {k: os.environ.get(k) for k in LIBRARY_ENV}
+    for k in old:
+        os.environ.pop(k, None)
+    os.environ.update(settings)
+    try:
+        yield
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v

@@ -5,36 +5,17 @@ k - q kernels and the oracle.
 ADGA_DFT_MIN_POINTS=1 forces the transform for every batch, ADGA_BUBBLE=direct
 keeps the direct kernels; both are read when a handle is created.
 """
-import contextlib
-import os
-
 import numpy as np
 import pytest
 
 from adga_b200 import Ladder, synth
 from adga_b200.ladder import generate_q_vol
-from tests.helpers import oracle_run, problem, rel_err
+from tests.helpers import library_env as env, oracle_run, problem, rel_err
 
 pytestmark = pytest.mark.gpu
 TRANSFORM = {"ADGA_DFT_MIN_POINTS": "1"}
 DIRECT = {"ADGA_BUBBLE": "direct"}
 OUT_KEYS = ("chi_qw_dens", "chi_qw_magn", "bubble_nl", "sigma_nl", "chi_loc_dens", "chi_loc_magn", "sigma_dmft")
-
-
-@contextlib.contextmanager
-def env(settings):
-    old = {k: os.environ.get(k) for k in ("ADGA_DFT_MIN_POINTS", "ADGA_BUBBLE")}
-    for k in old:
-        os.environ.pop(k, None)
-    os.environ.update(settings)
-    try:
-        yield
-    finally:
-        for k, v in old.items():
-            if v is None:
-                os.environ.pop(k, None)
-            else:
-                os.environ[k] = v
 
 
 def make_ladder(p, settings, q_data=None, k_data_eom=None, bubble_big_box=False):

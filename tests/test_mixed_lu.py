@@ -1,0 +1,47 @@
+"""The FP32 factorisation of the mixed path: without row interchanges (the
+default; the BSE matrices have growth factor ~1), with them
+(ADGA_MIXED_PIVOT=1), and the FP64 re-solve of points whose refinement does
+not converge (ADGA_MAX_REFINE=1 leaves every point unconverged)."""
+import pytest
+
+from adga_b200 import Ladder
+from tests.helpers import library_env, oracle_run, problem, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def run_mixed(p, settings):
+    s = p.spec
+    with library_env(settings):
+        lad = Ladder.from_problem(p)
+    try:
+        for iwb in range(-s.iwb, s.iwb + 1):
+            lad.set_vertex(iwb, *p.vertex(iwb))
+        status, stats = lad.ladder_run(1, None, "mixed")
+        out = lad.get_outputs()
+        out.update(lad.assemble(out, p.siw))
+        return status, stats, out
+    finally:
+        lad.close()
+
+
+@pytest.mark.parametrize("name", ["t3b", "t3m", "t2"])
+@pytest.mark.parametrize("pivot", ["0", "1"])
+def test_mixed_factorisation_matches_oracle(name, pivot):
+    p = problem(name)
+    status, stats, got = run_mixed(p, {"ADGA_MIXED_PIVOT": pivot})
+    want = oracle_run(p)
+    assert stats["mixed_fallbacks"] == 0 and not status.any()
+    for k in ("chi_dens", "chi_magn", "sigma"):
+        assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
+
+
+def test_unconverged_points_are_resolved_in_fp64():
+    p = problem("t3m")
+    status, stats, got = run_mixed(p, {"ADGA_MAX_REFINE": "1"})
+    npts = p.spec.nqp * (2 * p.spec.iwb + 1)
+    assert stats["mixed_fallbacks"] == npts
+    assert (status == -1).all()
+    want = oracle_run(p)
+    for k in ("chi_dens", "chi_magn", "sigma"):
+        assert rel_err(got[k], want[k]) < 1e-10, (k, rel_err(got[k], want[k]))
