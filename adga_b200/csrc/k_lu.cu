@@ -583,6 +583,207 @@ k_l21(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, const T *U
   }
 }
 
+// Diagonal block of an unpivoted step with its inverses, one CTA per matrix
+// (FP32): the jb x jb block is padded with the identity to 64 x 64 and
+// factored right-looking with one barrier per column (the column scaling by
+// 1/u_kk is deferred to the end, so no thread writes what another reads);
+// L11^-1 and U11^-1 then follow in 16 x 16 blocks: eight warps invert the
+// diagonal blocks of both triangles (lane = column, no barriers), and three
+// block rows of L^-1 (downwards) and U^-1 (upwards) are filled in pairs of
+// small block products, two barriers each.
+constexpr int DI_SCR = 6 * 256;
+
+__device__ __forceinline__ void cfma2(z32 &acc, z32 a, z32 u) {
+  acc = __ffma2_rn(make_float2(a.x, a.x), u, acc);
+  acc = __ffma2_rn(make_float2(-a.y, a.y), make_float2(u.y, u.x), acc);
+}
+__device__ __forceinline__ void cfma2(z64 &acc, z64 a, z64 u) { cfma(acc, a, u); }
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Linv, T *Uinv, int *ipiv_all,
+           int *rmap_all) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *D = reinterpret_cast<T *>(smraw);          // [64][DN_LD] factored block
+  T *XL = D + 64 * DN_LD;                       // L11^-1
+  T *XU = XL + 64 * DN_LD;                      // U11^-1
+  T *S = XU + 64 * DN_LD;                       // block-product scratch: L blocks 0..2, U blocks 3..5
+  __shared__ T rcps[64];
+  const int b = blockIdx.x, t = threadIdx.x;
+  T *A = M + (size_t)b * strideM;
+  const T one = cx<T>::make(1, 0), zero = czero<T>();
+  for (int e = t; e < 64 * 64; e += 256) {
+    const int i = e & 63, j = e >> 6;
+    D[i + j * DN_LD] = (i < jb && j < jb) ? A[(size_t)(J + i) + (size_t)(J + j) * N] : (i == j ? one : zero);
+  }
+  __syncthreads();
+  {
+    const int i = t & 63, part = t >> 6;
+    for (int k = 0; k < 64; ++k) {
+      const T rcp = crcp(D[k + k * DN_LD]);
+      if (t == 0) rcps[k] = rcp;
+      if (i > k) {
+        const T l = cmul(D[i + k * DN_LD], rcp);
+        for (int j = k + 1 + part; j < 64; j += 4) D[i + j * DN_LD] = csub(D[i + j * DN_LD], cmul(l, D[k + j * DN_LD]));
+      }
+      __syncthreads();
+    }
+  }
+  for (int e = t; e < 64 * 64; e += 256) {
+    const int i = e & 63, k = e >> 6;
+    if (i > k) D[i + k * DN_LD] = cmul(D[i + k * DN_LD], rcps[k]);
+  }
+  __syncthreads();
+  {
+    const int w = t >> 5, lane = t & 31;
+    if (lane < 16) {
+      const int o = 16 * (w & 3), l = lane;
+      T x[16];
+      const T xd = w < 4 ? one : rcps[o + l];    // diagonal entry of the inverse's column l
+#pragma unroll
+      for (int r = 0; r < 16; ++r) x[r] = r == l ? xd : zero;
+      if (w < 4) {                                // unit lower: column l of the block inverse
+#pragma unroll
+        for (int r = 1; r < 16; ++r) {
+          if (r > l) {
+            T s = zero;
+#pragma unroll
+            for (int kk = 0; kk < r; ++kk)
+              if (kk >= l) cfma(s, D[(o + r) + (o + kk) * DN_LD], x[kk]);
+            x[r] = cneg(s);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r) XL[(o + r) + (o + l) * DN_LD] = x[r];
+      } else {                                    // upper
+#pragma unroll
+        for (int r = 14; r >= 0; --r) {
+          if (r < l) {
+            T s = zero;
+#pragma unroll
+            for (int kk = r + 1; kk < 16; ++kk)
+              if (kk <= l) cfma(s, D[(o + r) + (o + kk) * DN_LD], x[kk]);
+            x[r] = cneg(cmul(rcps[o + r], s));
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r) XU[(o + r) + (o + l) * DN_LD] = x[r];
+      }
+    }
+  }
+  __syncthreads();
+  for (int st = 1; st < 4; ++st) {
+    const int bl = st, bu = 3 - st;               // block row of L^-1 / U^-1 filled in this round
+    for (int e = t; e < 512 * st; e += 256) {     // S = sum of block products
+      const int blk = e >> 8, r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      if (blk < st) {                             // L: S_bj = sum_{bk=bj}^{bl-1} L(bl,bk) XL(bk,bj), bj = blk
+        const int bj = blk;
+        for (int m = 16 * bj; m < 16 * bl; ++m)
+          cfma(s, D[(16 * bl + r) + m * DN_LD], XL[m + (16 * bj + c) * DN_LD]);
+        S[blk * 256 + r + 16 * c] = s;
+      } else {                                    // U: S_bj = sum_{bk=bu+1}^{bj} U(bu,bk) XU(bk,bj)
+        const int bj = bu + 1 + (blk - st);
+        for (int m = 16 * (bu + 1); m < 16 * (bj + 1); ++m)
+          cfma(s, D[(16 * bu + r) + m * DN_LD], XU[m + (16 * bj + c) * DN_LD]);
+        S[(3 + blk - st) * 256 + r + 16 * c] = s;
+      }
+    }
+    __syncthreads();
+    for (int e = t; e < 512 * st; e += 256) {     // X(bi,bj) = -X(bi,bi) S_bj
+      const int blk = e >> 8, r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      if (blk < st) {
+        const int bj = blk;
+        for (int m = 0; m < 16; ++m) cfma(s, XL[(16 * bl + r) + (16 * bl + m) * DN_LD], S[blk * 256 + m + 16 * c]);
+        XL[(16 * bl + r) + (16 * bj + c) * DN_LD] = cneg(s);
+      } else {
+        const int bj = bu + 1 + (blk - st);
+        for (int m = 0; m < 16; ++m)
+          cfma(s, XU[(16 * bu + r) + (16 * bu + m) * DN_LD], S[(3 + blk - st) * 256 + m + 16 * c]);
+        XU[(16 * bu + r) + (16 * bj + c) * DN_LD] = cneg(s);
+      }
+    }
+    __syncthreads();
+  }
+  const size_t off = ((size_t)b * nsteps + J / NB) * NB * NB;
+  for (int e = t; e < NB * NB; e += 256) {
+    const int i = e % NB, k = e / NB;
+    T lv = zero, uv = zero;
+    if (i < jb && k < jb) {
+      if (i > k) lv = XL[i + k * DN_LD];
+      else if (i == k) lv = one;
+      if (i <= k) uv = XU[i + k * DN_LD];
+    }
+    Linv[off + e] = lv;
+    Uinv[off + e] = uv;
+  }
+  for (int e = t; e < jb * jb; e += 256) {
+    const int i = e % jb, j = e / jb;
+    A[(size_t)(J + i) + (size_t)(J + j) * N] = D[i + j * DN_LD];
+  }
+  int *ip = ipiv_all + (size_t)b * N + J;
+  for (int i = t; i < jb; i += 256) ip[i] = J + i;
+  if (t == 0) rmap_all[(size_t)b * RMAP_STRIDE] = 0;
+}
+
+// Off-diagonal tiles of an unpivoted step, 64 x 64 per CTA:
+//   LEFT  U12 = L11^-1 A12  (rows J.., columns J+jb+64 x)
+//   !LEFT L21 = A21 U11^-1  (rows J+jb+64 x.., columns J..)
+// The tile and the triangle are staged in shared memory (column stride 65,
+// conflict-free); thread (t % 16, t / 16) owns rows rq + 16 i and columns
+// cq + 16 j, and stops at the triangle's last nonzero for its rows/columns.
+template <typename T, bool LEFT>
+__global__ void __launch_bounds__(256)
+k_tri_tile(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const T *Tri) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *Ts = reinterpret_cast<T *>(smraw);        // triangle, [k or row][DN_LD]
+  T *Xs = Ts + 64 * DN_LD;                      // tile
+  const int b = blockIdx.y, t = threadIdx.x;
+  T *A = M + (size_t)b * strideM;
+  const T *Q = Tri + ((size_t)b * nsteps + J / NB) * NB * NB;
+  const int r0 = LEFT ? J : J + jb + blockIdx.x * 64;
+  const int c0 = LEFT ? J + jb + blockIdx.x * 64 : J;
+  const int nr = LEFT ? jb : min(64, N - r0);
+  const int nc = LEFT ? min(64, ncols - c0) : jb;
+  for (int e = t; e < 64 * 64; e += 256) {
+    const int i = e & 63, j = e >> 6;           // i fastest: coalesced loads, conflict-free stores
+    Ts[i + j * DN_LD] = (i < jb && j < jb) ? Q[i + j * NB] : czero<T>();
+    Xs[i + j * DN_LD] = (i < nr && j < nc) ? A[(size_t)(r0 + i) + (size_t)(c0 + j) * N] : czero<T>();
+  }
+  __syncthreads();
+  const int rq = t & 15, cq = t >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = czero<T>();
+  // LEFT: out(r, c) = sum_{k <= r} L^-1(r, k) X(k, c); !LEFT: out(r, c) = sum_{k <= c} X(r, k) U^-1(k, c)
+  const int kend = min(jb, (LEFT ? rq : cq) + 49);
+#pragma unroll 2
+  for (int k = 0; k < kend; ++k) {
+    T a[4], u[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = LEFT ? Ts[(rq + 16 * i) + k * DN_LD] : Xs[(rq + 16 * i) + k * DN_LD];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) u[j] = LEFT ? Xs[k + (cq + 16 * j) * DN_LD] : Ts[k + (cq + 16 * j) * DN_LD];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) cfma2(acc[i][j], a[i], u[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = cq + 16 * j;
+    if (c >= nc) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = rq + 16 * i;
+      if (r < nr) A[(size_t)(r0 + r) + (size_t)(c0 + c) * N] = acc[i][j];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Trailing update on CUDA cores: C[J+jb.., J+jb..] -= A[J+jb.., J:J+jb] * A[J:J+jb, J+jb..]
 // 64 x 64 tiles, BK = 16, 256 threads with 4 x 4 complex outputs each.
@@ -872,6 +1073,32 @@ cudaError_t lu_trail_cuda(T *M, const LUBatch &lb, int J, int jb, cudaStream_t s
   return ADGA_LAUNCH_CHECK();
 }
 
+// trailing update of step (J, jb) through `trail` (or the CUDA-core GEMM), timed into tt
+template <typename T>
+static cudaError_t lu_trail_step(T *M, const LUBatch &lb, int J, int jb, trail_fn trail, void *trail_ctx,
+                                 cudaStream_t st, TrailTiming *tt) {
+  cudaError_t e;
+  if (J + jb < lb.N) {
+    cudaEvent_t ev0 = (tt && tt->ev) ? tt->ev[2 * tt->n] : nullptr;
+    cudaEvent_t ev1 = (tt && tt->ev) ? tt->ev[2 * tt->n + 1] : nullptr;
+    if (trail) {
+      e = trail(trail_ctx, J, jb, st, ev0, ev1);
+    } else {
+      if (ev0) cudaEventRecord(ev0, st);
+      e = lu_trail_cuda<T>(M, lb, J, jb, st);
+      if (ev1) cudaEventRecord(ev1, st);
+    }
+    if (e != cudaSuccess) return e;
+    if (tt && tt->ev) {
+      const double m = lb.N - J - jb, n = lb.ncols - J - jb;
+      tt->gflop += 8.0 * m * n * jb * lb.batch * 1e-9;
+      tt->gbytes += (2.0 * sizeof(T) * m * n + sizeof(T) * (double)jb * (m + n)) * lb.batch * 1e-9;
+      tt->n++;
+    }
+  }
+  return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
                     cudaStream_t st, TrailTiming *tt, bool nopiv) {
@@ -891,6 +1118,33 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
     attr_done[ti] = true;
   }
   const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
+  if constexpr (sizeof(T) == sizeof(z32)) {
+    if (nopiv) {
+      // FP32 unpivoted step: block LU + inverses, L21, U12 (k_diag_inv, k_tri_tile)
+      const size_t sm_di = sizeof(T) * (3 * 64 * DN_LD + DI_SCR), sm_tt = sizeof(T) * 2 * 64 * DN_LD;
+      static bool attr_np = false;
+      if (!attr_np) {
+        cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_di);
+        cudaFuncSetAttribute(k_tri_tile<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
+        cudaFuncSetAttribute(k_tri_tile<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
+        attr_np = true;
+      }
+      k_diag_inv<T><<<lb.batch, 256, sm_di, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps, (T *)lb.Linv,
+                                                  (T *)lb.Uinv, lb.ipiv, lb.rmap);
+      if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+      if (J + jb < lb.N) {
+        k_tri_tile<T, false><<<dim3(cdiv_u(lb.N - J - jb, 64), lb.batch), 256, sm_tt, st>>>(
+            M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps, (const T *)lb.Uinv);
+        if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+      }
+      if (lb.ncols > J + jb) {
+        k_tri_tile<T, true><<<dim3(cdiv_u(lb.ncols - J - jb, 64), lb.batch), 256, sm_tt, st>>>(
+            M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps, (const T *)lb.Linv);
+        if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+      }
+      return lu_trail_step<T>(M, lb, J, jb, trail, trail_ctx, st, tt);
+    }
+  }
   if (nopiv) {
     k_diag_nopiv<T><<<lb.batch, 256, sm_diag, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.rmap);
     if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
@@ -916,25 +1170,7 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
                                                                  nsteps, lb.rmap, (const T *)lb.Linv);
     if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
   }
-  if (J + jb < lb.N) {
-    cudaEvent_t ev0 = (tt && tt->ev) ? tt->ev[2 * tt->n] : nullptr;
-    cudaEvent_t ev1 = (tt && tt->ev) ? tt->ev[2 * tt->n + 1] : nullptr;
-    if (trail) {
-      e = trail(trail_ctx, J, jb, st, ev0, ev1);
-    } else {
-      if (ev0) cudaEventRecord(ev0, st);
-      e = lu_trail_cuda<T>(M, lb, J, jb, st);
-      if (ev1) cudaEventRecord(ev1, st);
-    }
-    if (e != cudaSuccess) return e;
-    if (tt && tt->ev) {
-      const double m = lb.N - J - jb, n = lb.ncols - J - jb;
-      tt->gflop += 8.0 * m * n * jb * lb.batch * 1e-9;
-      tt->gbytes += (2.0 * sizeof(T) * m * n + sizeof(T) * (double)jb * (m + n)) * lb.batch * 1e-9;
-      tt->n++;
-    }
-  }
-  return cudaSuccess;
+  return lu_trail_step<T>(M, lb, J, jb, trail, trail_ctx, st, tt);
 }
 
 template <typename T>
