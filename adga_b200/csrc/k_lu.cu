@@ -617,14 +617,17 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
     D[i + j * DN_LD] = (i < jb && j < jb) ? A[(size_t)(J + i) + (size_t)(J + j) * N] : (i == j ? one : zero);
   }
   __syncthreads();
+  if (t == 0) rcps[0] = crcp(D[0]);
+  __syncthreads();
   {
+    // the thread that finishes pivot k+1 (row k+1, part 0: its first column) forms 1/u for the next column
     const int i = t & 63, part = t >> 6;
     for (int k = 0; k < 64; ++k) {
-      const T rcp = crcp(D[k + k * DN_LD]);
-      if (t == 0) rcps[k] = rcp;
+      const T rcp = rcps[k];
       if (i > k) {
         const T l = cmul(D[i + k * DN_LD], rcp);
         for (int j = k + 1 + part; j < 64; j += 4) D[i + j * DN_LD] = csub(D[i + j * DN_LD], cmul(l, D[k + j * DN_LD]));
+        if (i == k + 1 && part == 0) rcps[k + 1] = crcp(D[i + i * DN_LD]);
       }
       __syncthreads();
     }
@@ -731,8 +734,11 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
 //   LEFT  U12 = L11^-1 A12  (rows J.., columns J+jb+64 x)
 //   !LEFT L21 = A21 U11^-1  (rows J+jb+64 x.., columns J..)
 // The tile and the triangle are staged in shared memory (column stride 65,
-// conflict-free); thread (t % 16, t / 16) owns rows rq + 16 i and columns
-// cq + 16 j, and stops at the triangle's last nonzero for its rows/columns.
+// conflict-free).  Along the triangle's free index (rows of U12, columns of
+// L21) a thread owns 4 consecutive entries and the other index strides by
+// 16; that index's owner, (t / 16), is nearly warp-uniform, so each warp
+// stops at its own edge of the triangle and the product does the triangular
+// half of the work.  U12 is written back through shared memory (coalesced).
 template <typename T, bool LEFT>
 __global__ void __launch_bounds__(256)
 k_tri_tile(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const T *Tri) {
@@ -752,34 +758,48 @@ k_tri_tile(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
     Xs[i + j * DN_LD] = (i < nr && j < nc) ? A[(size_t)(r0 + i) + (size_t)(c0 + j) * N] : czero<T>();
   }
   __syncthreads();
-  const int rq = t & 15, cq = t >> 4;
+  const int w4 = 4 * (t >> 4), s16 = t & 15;    // 4 consecutive triangle-side entries, the rest by 16
   T acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = czero<T>();
-  // LEFT: out(r, c) = sum_{k <= r} L^-1(r, k) X(k, c); !LEFT: out(r, c) = sum_{k <= c} X(r, k) U^-1(k, c)
-  const int kend = min(jb, (LEFT ? rq : cq) + 49);
+  // LEFT: out(w4 + i, s16 + 16 j) = sum_{k <= row} L^-1(row, k) X(k, col)
+  // !LEFT: out(s16 + 16 i, w4 + j) = sum_{k <= col} X(row, k) U^-1(k, col)
+  const int kend = min(jb, w4 + 4);
 #pragma unroll 2
   for (int k = 0; k < kend; ++k) {
     T a[4], u[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = LEFT ? Ts[(rq + 16 * i) + k * DN_LD] : Xs[(rq + 16 * i) + k * DN_LD];
+    for (int i = 0; i < 4; ++i) a[i] = LEFT ? Ts[(w4 + i) + k * DN_LD] : Xs[(s16 + 16 * i) + k * DN_LD];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) u[j] = LEFT ? Xs[k + (cq + 16 * j) * DN_LD] : Ts[k + (cq + 16 * j) * DN_LD];
+    for (int j = 0; j < 4; ++j) u[j] = LEFT ? Xs[k + (s16 + 16 * j) * DN_LD] : Ts[k + (w4 + j) * DN_LD];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) cfma2(acc[i][j], a[i], u[j]);
   }
+  if (LEFT) {
+    __syncthreads();                            // every Xs read is done
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int c = cq + 16 * j;
-    if (c >= nc) continue;
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = rq + 16 * i;
-      if (r < nr) A[(size_t)(r0 + r) + (size_t)(c0 + c) * N] = acc[i][j];
+      for (int j = 0; j < 4; ++j) Xs[(w4 + i) + (s16 + 16 * j) * DN_LD] = acc[i][j];
+    __syncthreads();
+    for (int e = t; e < 64 * 64; e += 256) {
+      const int i = e & 63, j = e >> 6;
+      if (i < nr && j < nc) A[(size_t)(r0 + i) + (size_t)(c0 + j) * N] = Xs[i + j * DN_LD];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = w4 + j;
+      if (c >= nc) continue;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = s16 + 16 * i;
+        if (r < nr) A[(size_t)(r0 + r) + (size_t)(c0 + c) * N] = acc[i][j];
+      }
     }
   }
 }
