@@ -30,6 +30,10 @@ void tc_trail_free(void *ctx);
 int tc_available();
 int tc_trail_error(void *ctx);
 
+// Refinement stop on an estimate: the next correction d = r A^-1 is taken as at
+// most kEstSafety * rho * max|r| (rho from the first sweep)
+constexpr double kEstSafety = 10.0;
+
 struct TanState;
 struct TanWork;
 
@@ -81,6 +85,7 @@ struct adga_handle {
   void *tc = nullptr;
   // refinement settings
   int max_iter = 8;
+  bool refine_estimate = true;   // stop on the bounded next correction (ADGA_REFINE_EXACT=1: on a solved one)
   bool mixed_nopiv = true;   // FP32 factorisation without row interchanges (ADGA_MIXED_PIVOT=1: with)
   double tol = 1e-10;   // stop when max|dX| <= tol * max|X| (the error is then far below)
   // last-run statistics
@@ -261,6 +266,7 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   h->nd4 = c.nd2 * c.nd2;
   if (const char *mpv = getenv("ADGA_MIXED_PIVOT")) h->mixed_nopiv = atoi(mpv) == 0;
   if (const char *mr = getenv("ADGA_MAX_REFINE")) h->max_iter = std::max(1, atoi(mr));
+  if (const char *re = getenv("ADGA_REFINE_EXACT")) h->refine_estimate = atoi(re) == 0;
   const char *ev = getenv("ADGA_NB");
   if (ev) h->NB = std::max(16, std::min(64, atoi(ev) / 8 * 8));   // the LU kernels assume NB <= 64
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -668,7 +674,7 @@ static int ensure_work(adga_handle *h, int prec, int want) {
          alloc_into(h, h->V32, (size_t)2 * cap * R * N, W) &&
          alloc_into(h, h->work32, (size_t)2 * cap * ((R + 15) / 16) * 16 * N, W) &&
          alloc_into(h, h->perm, (size_t)2 * cap * N, W) &&
-         alloc_into(h, h->norms, (size_t)4 * cap, W);
+         alloc_into(h, h->norms, (size_t)6 * cap, W);   // [max|d|, max|X|] per matrix, then max|r|
   }
   if (!ok) {
     free_list(h->work);
@@ -1046,10 +1052,14 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     lb.perm = h->perm;
     const int nmat = 2 * np;
     const size_t per = N * R;
-    std::vector<unsigned long long> nh(2 * nmat);
+    std::vector<unsigned long long> nh(3 * nmat);
     std::vector<char> conv(nmat, 0);
+    std::vector<double> rho(nmat, 1.0), xmax(nmat, 0.0);
+    unsigned long long *rnorm = h->norms + 4 * (size_t)h->cap;
+    auto bits = [](unsigned long long u) { double d; memcpy(&d, &u, 8); return d; };
     for (int it = 0; it < h->max_iter; ++it) {
       CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
+      CK(cudaMemsetAsync(rnorm, 0, sizeof(unsigned long long) * nmat, st));
       z64 *extra = nullptr;
       if (c.vq) {     // density-channel V(q) term of the residual
         const size_t ne = (size_t)np * c.nd2 * c.N;
@@ -1065,24 +1075,52 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
         CK(launch_vq_resid_extra(c, np, h->qidx_d, h->X64, chi0q, h->opg_d, extra, st));
       }
       CK(launch_residual(c, np, h->X64, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m,
-                         h->XD, h->V32, extra, st));
+                         h->XD, h->V32, extra, rnorm, st));
+      if (it > 0 && h->refine_estimate) {
+        // after a correction: its successor d = r A^-1 is bounded by kEstSafety * rho * max|r|,
+        // rho = max|d_1| / max|r_1| of the first sweep (the solve's amplification, at least 1);
+        // when that bound is within tol for every matrix the last solve is skipped
+        CK(cudaMemcpyAsync(nh.data() + 2 * nmat, rnorm, sizeof(unsigned long long) * nmat,
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        bool all = true;
+        double west = 0.0;
+        for (int m = 0; m < nmat && all; ++m) {
+          const double est = kEstSafety * std::max(rho[m], 1.0) * bits(nh[2 * nmat + m]);
+          const double rel = xmax[m] > 0 ? est / xmax[m] : est;
+          if (!(rel <= h->tol)) all = false;
+          if (!(rel <= west)) west = rel;
+        }
+        if (all) {
+          iters = it + 1;
+          worst = west;
+          std::fill(conv.begin(), conv.end(), 1);
+          break;
+        }
+      }
       CK(lu_fwdsolve_ws<z32>(T, lb, h->V32, per, (int)N, (int)R, h->work32, st));
       CK(lu_backsolve<z32>(T, lb, h->V32, per, (int)N, (int)R, st));
       CK(launch_update((int)per, nmat, h->V32, h->X64, h->norms, nullptr, st));
       CK(cudaMemcpyAsync(nh.data(), h->norms, sizeof(unsigned long long) * 2 * nmat,
                          cudaMemcpyDeviceToHost, st));
+      if (it == 0)
+        CK(cudaMemcpyAsync(nh.data() + 2 * nmat, rnorm, sizeof(unsigned long long) * nmat,
+                           cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       iters = it + 1;
       bool all = true;
       worst = 0.0;
       for (int m = 0; m < nmat; ++m) {
-        double md, mx;
-        memcpy(&md, &nh[2 * m], 8);
-        memcpy(&mx, &nh[2 * m + 1], 8);
+        const double md = bits(nh[2 * m]), mx = bits(nh[2 * m + 1]);
         double rel = mx > 0 ? md / mx : md;
         if (!(rel <= h->tol)) all = false;
         conv[m] = rel <= h->tol;
         if (!(rel <= worst)) worst = rel;
+        xmax[m] = mx;
+        if (it == 0) {
+          const double r1 = bits(nh[2 * nmat + m]);
+          rho[m] = r1 > 0 ? md / r1 : 1.0;
+        }
       }
       if (all) break;
     }

@@ -185,8 +185,9 @@ typedef struct adga_run_stats {
   int points;                  /* (q, omega) points processed                  */
   int lu_info_nonzero;         /* points whose LU hit an exactly-zero pivot    */
   int mixed_fallbacks;         /* mixed points re-solved in FP64               */
-  int max_refine_iters;        /* largest refinement count of a mixed point    */
-  double max_refine_resid;     /* largest final relative correction            */
+  int max_refine_iters;        /* largest count of FP64 residuals of a batch   */
+  double max_refine_resid;     /* largest final relative correction, or its
+                                  bound when the last solve was skipped        */
   double ms_total;             /* device time of the run (CUDA events)         */
   double ms_chi0, ms_bse, ms_lu, ms_post, ms_eom;   /* per-stage device time   */
   long long kernel_launches;   /* kernels this run launched                      */

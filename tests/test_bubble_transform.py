@@ -54,10 +54,13 @@ def test_transform_matches_oracle(name):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_transform_matches_direct(prec):
+    """The mixed path agrees with itself to its refinement tolerance (its last
+    correction, bounded by 1e-10 max|X|, may be left unapplied)."""
     p = problem("t3b")
     a, b = run(p, TRANSFORM, prec), run(p, DIRECT, prec)
+    tol = 1e-12 if prec == "fp64" else 1e-9
     for k in OUT_KEYS:
-        assert rel_err(a[k], b[k]) < 1e-12, (k, rel_err(a[k], b[k]))
+        assert rel_err(a[k], b[k]) < tol, (k, rel_err(a[k], b[k]))
 
 
 def test_transform_on_an_irregular_q_list():

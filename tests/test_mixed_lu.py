@@ -1,7 +1,9 @@
 """The FP32 factorisation of the mixed path: without row interchanges (the
 default; the BSE matrices have growth factor ~1), with them
 (ADGA_MIXED_PIVOT=1), and the FP64 re-solve of points whose refinement does
-not converge (ADGA_MAX_REFINE=1 leaves every point unconverged)."""
+not converge (ADGA_MAX_REFINE=1 leaves every point unconverged); the
+refinement's two stopping rules: the bounded next correction (default) and a
+solved one (ADGA_REFINE_EXACT=1)."""
 import pytest
 
 from adga_b200 import Ladder
@@ -45,3 +47,14 @@ def test_unconverged_points_are_resolved_in_fp64():
     want = oracle_run(p)
     for k in ("chi_dens", "chi_magn", "sigma"):
         assert rel_err(got[k], want[k]) < 1e-10, (k, rel_err(got[k], want[k]))
+
+
+@pytest.mark.parametrize("exact", ["0", "1"])
+def test_refinement_stopping_rules(exact):
+    p = problem("t3m")
+    status, stats, got = run_mixed(p, {"ADGA_REFINE_EXACT": exact})
+    want = oracle_run(p)
+    assert stats["mixed_fallbacks"] == 0 and not status.any()
+    assert stats["max_refine_resid"] <= 1e-10
+    for k in ("chi_dens", "chi_magn", "sigma"):
+        assert rel_err(got[k], want[k]) < (1e-12 if exact == "1" else 1e-9), (k, rel_err(got[k], want[k]))
