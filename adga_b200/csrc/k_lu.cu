@@ -739,6 +739,16 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
 // 16; that index's owner, (t / 16), is nearly warp-uniform, so each warp
 // stops at its own edge of the triangle and the product does the triangular
 // half of the work.  U12 is written back through shared memory (coalesced).
+// one element global -> shared by cp.async (8 or 16 bytes); zeros when !valid
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0));
+}
+
 template <typename T, bool LEFT>
 __global__ void __launch_bounds__(256)
 k_tri_tile(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const T *Tri) {
@@ -752,11 +762,15 @@ k_tri_tile(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   const int c0 = LEFT ? J + jb + blockIdx.x * 64 : J;
   const int nr = LEFT ? jb : min(64, N - r0);
   const int nc = LEFT ? min(64, ncols - c0) : jb;
+  // asynchronous staging (zero-filled outside the triangle / tile): every load in flight at once
   for (int e = t; e < 64 * 64; e += 256) {
     const int i = e & 63, j = e >> 6;           // i fastest: coalesced loads, conflict-free stores
-    Ts[i + j * DN_LD] = (i < jb && j < jb) ? Q[i + j * NB] : czero<T>();
-    Xs[i + j * DN_LD] = (i < nr && j < nc) ? A[(size_t)(r0 + i) + (size_t)(c0 + j) * N] : czero<T>();
+    const bool inq = i < jb && j < jb, inx = i < nr && j < nc;
+    cp_async_elem<T>(Ts + i + j * DN_LD, inq ? Q + i + (size_t)j * NB : Q, inq);
+    cp_async_elem<T>(Xs + i + j * DN_LD, inx ? A + (size_t)(r0 + i) + (size_t)(c0 + j) * N : A, inx);
   }
+  asm volatile("cp.async.commit_group;");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
   const int w4 = 4 * (t >> 4), s16 = t & 15;    // 4 consecutive triangle-side entries, the rest by 16
   T acc[4][4];
