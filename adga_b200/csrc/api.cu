@@ -29,6 +29,21 @@ static cudaError_t tc_trail_range_fn(void *r, int J, int jb, cudaStream_t st, cu
 void tc_trail_free(void *ctx);
 int tc_available();
 int tc_trail_error(void *ctx);
+int tc_pair_supported(void *ctx);
+cudaError_t tc_pair_narrow(void *ctx, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
+                           cudaEvent_t ev0, cudaEvent_t ev1);
+cudaError_t tc_pair_wide(void *ctx, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
+                         cudaEvent_t ev0, cudaEvent_t ev1);
+static cudaError_t tc_pair_narrow_fn(void *r, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0,
+                                     cudaEvent_t ev1) {
+  TcRange *x = (TcRange *)r;
+  return tc_pair_narrow(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1);
+}
+static cudaError_t tc_pair_wide_fn(void *r, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0,
+                                   cudaEvent_t ev1) {
+  TcRange *x = (TcRange *)r;
+  return tc_pair_wide(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1);
+}
 
 // Refinement stop on an estimate: the next correction d = r A^-1 is taken as at
 // most kEstSafety * rho * max|r| (rho from the first sweep)
@@ -708,6 +723,14 @@ static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool ap
   // measured: the trailing-update grids fill every SM, so the split gives no
   // overlap on the t2g workload; kept as an option (ADGA_TWO_STREAMS=1)
   const bool split = h->st2 && lb.batch >= 8 && getenv("ADGA_TWO_STREAMS");
+  if constexpr (sizeof(T) == sizeof(z32)) {
+    // unpivoted FP32 with the tensor cores: delayed two-step updates (ADGA_NO_PAIRS=1: step by step)
+    if (!split && nopiv && tc && tc_pair_supported(h->tc) && !getenv("ADGA_NO_PAIRS")) {
+      TcRange r{h->tc, 0, lb.batch};
+      PairOps ops{tc_pair_narrow_fn, tc_pair_wide_fn, &r};
+      return lu_factor_pairs(M, lb, ops, st, tt);
+    }
+  }
   if (!split) {
     TcRange r{h->tc, 0, lb.batch};
     return lu_factor<T>(M, lb, apply_left, tc ? tc_trail_range_fn : nullptr, tc ? &r : nullptr, st, tt, nopiv);

@@ -1133,6 +1133,69 @@ static cudaError_t lu_trail_step(T *M, const LUBatch &lb, int J, int jb, trail_f
   return cudaSuccess;
 }
 
+// kernels of one unpivoted FP32 step: block LU + inverses, L21, U12 (k_diag_inv, k_tri_tile)
+static cudaError_t nopiv_step_kernels(z32 *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
+  typedef z32 T;
+  const int nsteps = lb.nsteps();
+  cudaError_t e;
+  const size_t sm_di = sizeof(T) * (3 * 64 * DN_LD + DI_SCR), sm_tt = sizeof(T) * 2 * 64 * DN_LD;
+  static bool attr_np = false;
+  if (!attr_np) {
+    cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_di);
+    cudaFuncSetAttribute(k_tri_tile<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
+    cudaFuncSetAttribute(k_tri_tile<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
+    attr_np = true;
+  }
+  k_diag_inv<T><<<lb.batch, 256, sm_di, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps, (T *)lb.Linv,
+                                              (T *)lb.Uinv, lb.ipiv, lb.rmap);
+  if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  if (J + jb < lb.N) {
+    k_tri_tile<T, false><<<dim3(cdiv_u(lb.N - J - jb, 64), lb.batch), 256, sm_tt, st>>>(
+        M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps, (const T *)lb.Uinv);
+    if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  }
+  if (lb.ncols > J + jb) {
+    k_tri_tile<T, true><<<dim3(cdiv_u(lb.ncols - J - jb, 64), lb.batch), 256, sm_tt, st>>>(
+        M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps, (const T *)lb.Linv);
+    if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static void trail_account(TrailTiming *tt, double m, double n, double k, int batch) {
+  if (!tt || !tt->ev || m <= 0 || n <= 0) return;
+  tt->gflop += 8.0 * m * n * k * batch * 1e-9;
+  tt->gbytes += (2.0 * sizeof(z32) * m * n + sizeof(z32) * k * (m + n)) * batch * 1e-9;
+}
+
+// Unpivoted FP32 factorisation with delayed updates: steps in pairs (J0, J1 = J0 + NB);
+// after J0 only the parts of its update that step J1 reads (ops.narrow), after J1
+// both steps' updates of the rest at once (ops.wide)
+cudaError_t lu_factor_pairs(z32 *M, const LUBatch &lb, const PairOps &ops, cudaStream_t st, TrailTiming *tt) {
+  const int nsteps = lb.nsteps();
+  for (int s = 0; s < nsteps; ++s) {
+    const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
+    cudaError_t e = nopiv_step_kernels(M, lb, J, jb, st);
+    if (e != cudaSuccess) return e;
+    if (J + jb >= lb.N) break;
+    cudaEvent_t ev0 = (tt && tt->ev) ? tt->ev[2 * tt->n] : nullptr;
+    cudaEvent_t ev1 = (tt && tt->ev) ? tt->ev[2 * tt->n + 1] : nullptr;
+    if (s % 2 == 0) {
+      const int J1 = J + jb, jb2 = min(lb.NB, lb.N - J1);
+      e = ops.narrow(ops.ctx, J, jb, jb2, st, ev0, ev1);
+      trail_account(tt, lb.N - J1, jb2, jb, lb.batch);
+      trail_account(tt, jb2, lb.ncols - J1 - jb2, jb, lb.batch);
+    } else {
+      const int J0 = J - lb.NB, R0 = J + jb;
+      e = ops.wide(ops.ctx, J0, lb.NB, jb, st, ev0, ev1);
+      trail_account(tt, lb.N - R0, lb.ncols - R0, lb.NB + jb, lb.batch);
+    }
+    if (e != cudaSuccess) return e;
+    if (tt && tt->ev) tt->n++;
+  }
+  return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
                     cudaStream_t st, TrailTiming *tt, bool nopiv) {
@@ -1154,28 +1217,7 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
   const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
   if constexpr (sizeof(T) == sizeof(z32)) {
     if (nopiv) {
-      // FP32 unpivoted step: block LU + inverses, L21, U12 (k_diag_inv, k_tri_tile)
-      const size_t sm_di = sizeof(T) * (3 * 64 * DN_LD + DI_SCR), sm_tt = sizeof(T) * 2 * 64 * DN_LD;
-      static bool attr_np = false;
-      if (!attr_np) {
-        cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_di);
-        cudaFuncSetAttribute(k_tri_tile<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
-        cudaFuncSetAttribute(k_tri_tile<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
-        attr_np = true;
-      }
-      k_diag_inv<T><<<lb.batch, 256, sm_di, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps, (T *)lb.Linv,
-                                                  (T *)lb.Uinv, lb.ipiv, lb.rmap);
-      if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-      if (J + jb < lb.N) {
-        k_tri_tile<T, false><<<dim3(cdiv_u(lb.N - J - jb, 64), lb.batch), 256, sm_tt, st>>>(
-            M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps, (const T *)lb.Uinv);
-        if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-      }
-      if (lb.ncols > J + jb) {
-        k_tri_tile<T, true><<<dim3(cdiv_u(lb.ncols - J - jb, 64), lb.batch), 256, sm_tt, st>>>(
-            M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps, (const T *)lb.Linv);
-        if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-      }
+      if ((e = nopiv_step_kernels(M, lb, J, jb, st)) != cudaSuccess) return e;
       return lu_trail_step<T>(M, lb, J, jb, trail, trail_ctx, st, tt);
     }
   }

@@ -268,8 +268,10 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 
 __global__ void __launch_bounds__(P_THREADS, 1)
 k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-             const __grid_constant__ CUtensorMap mapC, z32 *M, size_t strideM, int N, int J, int jb,
-             int Mrows, int Ncols, int Ncap, int nkb, int b0, int count, int *err) {
+             const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB2,
+             const __grid_constant__ CUtensorMap mapC, z32 *M, size_t strideM, int N, int crow0, int ccol0,
+             int arow0, int bcol0, int arow2, int bcol2, int nkb1, int Mrows, int Ncols, int Ncap, int nkb, int b0,
+             int count, int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
@@ -321,9 +323,13 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
             break;
           const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
           mbar_expect_tx(bar_full + 8 * s, STAGE_BYTES);
-          tma_load_3d(sa, &mapA, bar_full + 8 * s, kb * BK, tm * BM, b);
-          tma_load_3d(sb, &mapB, bar_full + 8 * s, kb * BK, tn * BN, b);
-          tma_load_3d(sb + B_BYTES / 2, &mapB, bar_full + 8 * s, kb * BK, Ncap + tn * BN, b);
+          // k-blocks [0, nkb1) from the first staging, the rest from the second
+          const bool second = kb >= nkb1;
+          const CUtensorMap *ma = second ? &mapA2 : &mapA, *mb = second ? &mapB2 : &mapB;
+          const int kx = (second ? kb - nkb1 : kb) * BK, ar = second ? arow2 : arow0, bc = second ? bcol2 : bcol0;
+          tma_load_3d(sa, ma, bar_full + 8 * s, kx, ar + tm * BM, b);
+          tma_load_3d(sb, mb, bar_full + 8 * s, kx, bc + tn * BN, b);
+          tma_load_3d(sb + B_BYTES / 2, mb, bar_full + 8 * s, kx, Ncap + bc + tn * BN, b);
         }
         if (!ok) break;
       }
@@ -362,9 +368,9 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           if (it > 0) ok = mbar_wait(bar_cempty + 8 * h, (it - 1) & 1, err, 14);
           if (!ok) break;
           mbar_expect_tx(bar_cfull + 8 * h, P_CH_BYTES);
-          // x counts floats: rows J+jb+m0.. as (re, im) pairs
-          tma_load_3d(scbase + h * P_CH_BYTES, &mapC, bar_cfull + 8 * h, 2 * (J + jb + tm * BM),
-                      J + jb + tn * BN + h * P_CH_COLS, b);
+          // x counts floats: rows crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
+          tma_load_3d(scbase + h * P_CH_BYTES, &mapC, bar_cfull + 8 * h, 2 * (crow0 + tm * BM),
+                      ccol0 + tn * BN + h * P_CH_COLS, b);
         }
         if (!ok) break;
       }
@@ -385,7 +391,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int m = tm * BM + row;
       const bool rowok = m < Mrows;
-      z32 *Cb = M + (size_t)b * strideM + (size_t)(J + jb + m);
+      z32 *Cb = M + (size_t)b * strideM + (size_t)(crow0 + m);
       const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * TMEM_COLS + h * P_CH_COLS);
       const int nbase = tn * BN + h * P_CH_COLS;
 #pragma unroll 1
@@ -404,7 +410,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
             z32 v = cv[j];
             v.x -= re[j];
             v.y -= im[j];
-            Cb[(size_t)(J + jb + n) * N] = v;
+            Cb[(size_t)(ccol0 + n) * N] = v;
           }
         }
       }
@@ -497,6 +503,8 @@ struct TcCtx {
   int nsm = 0;
   bool persist = false;        // C tiles by TMA: needs 16-byte column and matrix strides
   CUtensorMap mapA, mapB, mapC;
+  __nv_bfloat16 *A2 = nullptr, *B2 = nullptr;   // second staging (the later step of a delayed pair)
+  CUtensorMap mapA2, mapB2;
 };
 
 typedef CUresult (*encode_fn_t)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -563,10 +571,15 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   const size_t K6 = 6 * (size_t)lb.NB;
   cudaError_t e = cudaMalloc(&c->A, sizeof(__nv_bfloat16) * K6 * lb.N * lb.batch);
   if (e == cudaSuccess) e = cudaMalloc(&c->B, sizeof(__nv_bfloat16) * K6 * 2 * c->Ncap * lb.batch);
+  // second staging for the unpivoted path's delayed two-step updates
+  if (e == cudaSuccess) e = cudaMalloc(&c->A2, sizeof(__nv_bfloat16) * K6 * lb.N * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->B2, sizeof(__nv_bfloat16) * K6 * 2 * c->Ncap * lb.batch);
   if (e == cudaSuccess) e = cudaMalloc(&c->err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemsetAsync(c->err, 0, sizeof(int), st);
   if (e == cudaSuccess && (!make_map(&c->mapA, c->A, K6, lb.N, lb.batch) ||
-                           !make_map(&c->mapB, c->B, K6, 2 * (uint64_t)c->Ncap, lb.batch)))
+                           !make_map(&c->mapB, c->B, K6, 2 * (uint64_t)c->Ncap, lb.batch) ||
+                           !make_map(&c->mapA2, c->A2, K6, lb.N, lb.batch) ||
+                           !make_map(&c->mapB2, c->B2, K6, 2 * (uint64_t)c->Ncap, lb.batch)))
     e = cudaErrorInvalidValue;
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
@@ -581,7 +594,7 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
     c->persist = c->nsm > 0;
   }
   if (e != cudaSuccess) {
-    cudaFree(c->A); cudaFree(c->B); cudaFree(c->err);
+    cudaFree(c->A); cudaFree(c->B); cudaFree(c->A2); cudaFree(c->B2); cudaFree(c->err);
     delete c;
     return e;
   }
@@ -608,15 +621,96 @@ cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, 
   if (c->persist) {
     const long long ntiles = (long long)cdiv_u(Ncols, BN) * cdiv_u(Mrows, BM) * count;
     const int grid = (int)std::min<long long>(ntiles, c->nsm);
-    k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapC, c->M, lb.strideM, lb.N, J,
-                                                         jb, Mrows, Ncols, c->Ncap, 6 * NB / BK, first, count,
-                                                         c->err);
+    const int nkb = 6 * NB / BK;
+    k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapA, c->mapB, c->mapC, c->M,
+                                                         lb.strideM, lb.N, J + jb, J + jb, 0, 0, 0, 0, nkb, Mrows,
+                                                         Ncols, c->Ncap, nkb, first, count, c->err);
   } else {
     dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), count);
     k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA, c->mapB, c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
                                                c->Ncap, 6 * NB / BK, first, c->err);
   }
   e = ADGA_LAUNCH_CHECK();
+  if (ev1) cudaEventRecord(ev1, st);
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// Delayed updates of the unpivoted path, two steps J0 (width jb) and J1 = J0 + jb
+// (width jb2) at a time:
+//   tc_pair_narrow  after step J0: its update restricted to the columns of step
+//                   J1 (all rows below J0 + jb) and to the rows of step J1
+//                   (columns right of J1 + jb2) -- what step J1's factorisation reads;
+//   tc_pair_wide    after step J1: the rest, rows and columns from J1 + jb2, with
+//                   both steps' L21 / U12 as one K = 12 NB product.
+// The C read-modify-write of the largest region happens once per two steps.
+// ---------------------------------------------------------------------------
+namespace {
+// C[crow0 + m, ccol0 + n] -= A.B over rows m < Mrows, columns n < Ncols, from the first
+// staging at (arow0, bcol0) and, when two, the second at (arow2, bcol2)
+cudaError_t persist_region(TcCtx *c, bool two, int first, int count, int crow0, int ccol0, int arow0, int bcol0,
+                           int arow2, int bcol2, int Mrows, int Ncols, cudaStream_t st) {
+  if (Mrows <= 0 || Ncols <= 0 || count <= 0) return cudaSuccess;
+  const LUBatch &lb = c->lb;
+  const long long ntiles = (long long)cdiv_u(Ncols, BN) * cdiv_u(Mrows, BM) * count;
+  const int grid = (int)std::min<long long>(ntiles, c->nsm);
+  const int nkb1 = 6 * lb.NB / BK;
+  k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapA2, c->mapB2, c->mapC, c->M,
+                                                       lb.strideM, lb.N, crow0, ccol0, arow0, bcol0, arow2, bcol2,
+                                                       nkb1, Mrows, Ncols, c->Ncap, two ? 2 * nkb1 : nkb1, first,
+                                                       count, c->err);
+  return ADGA_LAUNCH_CHECK();
+}
+
+// staging of one step: L rows J + jb.., columns J..J + jb; U rows J..J + jb, columns J + jb..
+cudaError_t stage_step(TcCtx *c, __nv_bfloat16 *A, __nv_bfloat16 *B, int first, int count, int J, int jb,
+                       cudaStream_t st) {
+  const LUBatch &lb = c->lb;
+  const int Mrows = lb.N - J - jb, Ncols = lb.ncols - J - jb, NB = lb.NB;
+  if (Mrows > 0) {
+    k_split_a<<<dim3(cdiv_u(Mrows, 64), count), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Mrows, NB, A, first);
+    cudaError_t e = ADGA_LAUNCH_CHECK();
+    if (e != cudaSuccess) return e;
+  }
+  if (Ncols > 0) {
+    k_split_b<<<dim3(cdiv_u(Ncols, 256 / NB), count), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Ncols, c->Ncap,
+                                                                     NB, B, first);
+    return ADGA_LAUNCH_CHECK();
+  }
+  return cudaSuccess;
+}
+}  // namespace
+
+int tc_pair_supported(void *ctxp) { return ctxp && ((TcCtx *)ctxp)->persist && ((TcCtx *)ctxp)->lb.NB == 64; }
+
+cudaError_t tc_pair_narrow(void *ctxp, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
+                           cudaEvent_t ev0, cudaEvent_t ev1) {
+  TcCtx *c = (TcCtx *)ctxp;
+  const LUBatch &lb = c->lb;
+  cudaError_t e = stage_step(c, c->A, c->B, first, count, J0, jb, st);
+  if (e != cudaSuccess) return e;
+  const int J1 = J0 + jb;
+  if (ev0) cudaEventRecord(ev0, st);
+  // columns of step J1, every row below J1
+  e = persist_region(c, false, first, count, J1, J1, 0, 0, 0, 0, lb.N - J1, jb2, st);
+  // rows of step J1, the columns right of it
+  if (e == cudaSuccess)
+    e = persist_region(c, false, first, count, J1, J1 + jb2, 0, jb2, 0, 0, jb2, lb.ncols - J1 - jb2, st);
+  if (ev1) cudaEventRecord(ev1, st);
+  return e;
+}
+
+cudaError_t tc_pair_wide(void *ctxp, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
+                         cudaEvent_t ev0, cudaEvent_t ev1) {
+  TcCtx *c = (TcCtx *)ctxp;
+  const LUBatch &lb = c->lb;
+  const int J1 = J0 + jb, R0 = J1 + jb2;
+  if (lb.N - R0 <= 0) return cudaSuccess;
+  // step J0's staging (from tc_pair_narrow, rows / columns from J1) is still valid
+  cudaError_t e = stage_step(c, c->A2, c->B2, first, count, J1, jb2, st);
+  if (e != cudaSuccess) return e;
+  if (ev0) cudaEventRecord(ev0, st);
+  e = persist_region(c, true, first, count, R0, R0, jb2, jb2, 0, 0, lb.N - R0, lb.ncols - R0, st);
   if (ev1) cudaEventRecord(ev1, st);
   return e;
 }
@@ -633,6 +727,8 @@ void tc_trail_free(void *ctxp) {
   if (!c) return;
   cudaFree(c->A);
   cudaFree(c->B);
+  cudaFree(c->A2);
+  cudaFree(c->B2);
   cudaFree(c->err);
   delete c;
 }

@@ -52,6 +52,16 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
 template <typename T>
 cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
                     cudaStream_t st, TrailTiming *tt = nullptr, bool nopiv = false);
+// Delayed updates of the unpivoted FP32 factorisation (tensor cores): after step
+// J0 (width jb) `narrow` applies its update to what step J1 = J0 + jb (width jb2)
+// reads; after step J1 `wide` applies both steps' updates to the rest.
+struct PairOps {
+  cudaError_t (*narrow)(void *ctx, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
+  cudaError_t (*wide)(void *ctx, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
+  void *ctx;
+};
+cudaError_t lu_factor_pairs(z32 *M, const LUBatch &lb, const PairOps &ops, cudaStream_t st,
+                            TrailTiming *tt = nullptr);
 // the matrices [first, first + count) of a batch as a batch of their own
 template <typename T>
 inline LUBatch lu_sub(const LUBatch &lb, int first, int count) {
