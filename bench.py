@@ -30,9 +30,10 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "BSE q·ω pts/s at 1e-8 rel err vs FP64 oracle: mixed-prec vs plain FP64 on B200"
-# DRAM bytes / algorithmic bytes of one k_tc_persist launch measured with ncu
-# (64-point t2g case, LU step 3, 128 matrices); profiles/k_tc_persist_t2g.md
-TRAFFIC_OVER_ALG = 1.08
+# DRAM bytes / algorithmic bytes of the k_tc_persist launches of one step pair
+# (two narrow K = 64 regions and one wide K = 128 region) measured with ncu on the
+# 160-point t2g case, 320 matrices; profiles/k_tc_persist_t2g.md
+TRAFFIC_OVER_ALG = 1.27
 UNIT = "qw_points/s"
 WORKLOAD = "c1"
 
@@ -364,9 +365,9 @@ def main():
     # roofline of the dominant kernel: the LU trailing update (tensor cores).
     # Its C read-modify-write makes it HBM-bound, so it is reported against
     # the measured copy bandwidth with algorithmic bytes (C read + write, L21
-    # and U12 read once); `traffic` scales the DRAM bytes ncu measured on one
-    # launch of the same kernel (64-point case, per matrix) to the average
-    # launch here: TRAFFIC_OVER_ALG (see profiles/).
+    # and U12 read once per launch region); `traffic` scales them by the DRAM /
+    # algorithmic ratio ncu measured on the launches of one step pair:
+    # TRAFFIC_OVER_ALG (see profiles/).
     pk, pk_kind = peaks()
     gflop = sum(s["trail_gflop"] for s in st_mixed)
     gbytes = sum(s["trail_gbytes"] for s in st_mixed)
@@ -374,7 +375,8 @@ def main():
     nlaunch = max(sum(s["trail_launches"] for s in st_mixed), 1)
     achieved = gbytes / mst * 1e3 if mst else 0.0          # GB/s
     peak = pk.get("hbm_gbs")
-    roof = {"kernel": "k_tc_persist: tensor-core LU trailing update of the mixed path (GEMM launch only)",
+    roof = {"kernel": "k_tc_persist: tensor-core LU trailing updates of the mixed path (narrow K=64 and "
+                      "wide K=128 regions of each step pair; GEMM launches only)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if peak else None,
             "traffic": TRAFFIC_OVER_ALG * gbytes * 1e9 / nlaunch,
