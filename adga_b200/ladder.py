@@ -214,18 +214,31 @@ class Ladder:
         self.last_range = (qwstart, qwstop)
         return status, st.as_dict()
 
-    def get_outputs(self) -> Dict[str, np.ndarray]:
+    def output_shapes(self, npts=None) -> Dict[str, tuple]:
+        """Shapes of the accumulators get_outputs returns (npts: points of the run)."""
+        nd, nd2, nw = self.ndim, self.ndim2, 2 * self.iwb + 1
+        n = self.last_npts if npts is None else npts
+        return dict(chi_qw_dens=(nd2, nd2, n), chi_qw_magn=(nd2, nd2, n), bubble_nl=(nd2, nd2, n),
+                    bubble_loc=(nd2, nd2, nw), chi_loc_dens=(nd2, nd2, nw), chi_loc_magn=(nd2, nd2, nw),
+                    sigma_nl=(nd, nd, 2 * self.iwf, self.nkp_eom), sigma_dmft=(nd, nd, 2 * self.iwf),
+                    sigma_hf=(nd, nd, self.nkp_eom))
+
+    def get_outputs(self, out: Dict[str, np.ndarray] = None) -> Dict[str, np.ndarray]:
         """Accumulators with the reference's shapes (Fortran order):
         chi_qw_dens/magn, bubble_nl (ndim2, ndim2, npts); bubble_loc,
         chi_loc_dens/magn (ndim2, ndim2, 2*iwb+1); sigma_nl
         (ndim, ndim, 2*iwf, nkp_eom); sigma_dmft (ndim, ndim, 2*iwf);
-        sigma_hf (ndim, ndim, nkp_eom)."""
-        nd, nd2, nw, n = self.ndim, self.ndim2, 2 * self.iwb + 1, self.last_npts
-        z = lambda *s: np.zeros(s, dtype=np.complex128, order="F")
-        out = dict(chi_qw_dens=z(nd2, nd2, n), chi_qw_magn=z(nd2, nd2, n), bubble_nl=z(nd2, nd2, n),
-                   bubble_loc=z(nd2, nd2, nw), chi_loc_dens=z(nd2, nd2, nw),
-                   chi_loc_magn=z(nd2, nd2, nw), sigma_nl=z(nd, nd, 2 * self.iwf, self.nkp_eom),
-                   sigma_dmft=z(nd, nd, 2 * self.iwf), sigma_hf=z(nd, nd, self.nkp_eom))
+        sigma_hf (ndim, ndim, nkp_eom).  `out`: caller-owned arrays of these
+        shapes (complex128, Fortran order; pinned host memory makes the copies
+        fastest) to fill instead of new ones."""
+        shapes = self.output_shapes()
+        if out is None:
+            out = {k: np.zeros(sh, dtype=np.complex128, order="F") for k, sh in shapes.items()}
+        else:
+            for k, sh in shapes.items():
+                a = out[k]
+                if a.shape != sh or a.dtype != np.complex128 or not a.flags.f_contiguous:
+                    raise ValueError(f"out[{k!r}]: expected complex128 {sh} in Fortran order")
         o = Outputs(*[out[k].ctypes.data for k, _ in Outputs._fields_])
         self._check(self._lib.adga_get_outputs(self._h, C.byref(o)), "get_outputs")
         return out
