@@ -99,7 +99,7 @@ def load():
         "adga_set_vq": [vp, vp],
         "adga_set_tangent": [vp, i, vp, vp, vp],
         "adga_set_vertex_tangent": [vp, i, i, vp, vp],
-        "adga_ladder_run_tangent": [vp, i, i, ip, C.POINTER(RunStats)],
+        "adga_ladder_run_tangent": [vp, i, i, i, ip, C.POINTER(RunStats)],
         "adga_get_tangent_outputs": [vp, i, C.POINTER(Outputs)],
         "adga_clear_tangents": [vp],
     }

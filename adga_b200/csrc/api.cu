@@ -929,10 +929,74 @@ static int tan_work(adga_handle *h) {
   return 0;
 }
 
-// the tangent of direction d for one FP64 batch, after its forward pass (T holds
-// the LU factors of the transposed BSE matrices, factorised with the left interchanges)
-static int tan_batch(adga_handle *h, int d, int iwb, int np, int off, z64 *T, LUBatch lb, const z64 *chi0q,
-                     bool do_chi, bool do_eom) {
+// dX = r A^-1 for the tangents of a mixed batch: the forward pass's FP32
+// factors and FP64 refinement against 1 - D F~ with r in place of (1+gamma^w)
+// (the residual r - dX + (dX D) F~), the same stopping rules as the forward
+// refinement.  Matrices flagged in skip (points the forward re-solves in FP64)
+// are left out of the convergence test.
+static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 *chi0q, int np, const z64 *r,
+                           z64 *dX, const std::vector<char> &skip) {
+  DevCtx &c = h->c;
+  cudaStream_t st = h->st;
+  const size_t N = c.N, R = c.R, per = N * R;
+  const int nmat = 2 * np;
+  unsigned long long *rnorm = h->norms + 4 * (size_t)h->cap;
+  std::vector<unsigned long long> nh(3 * nmat);
+  std::vector<double> rho(nmat, 1.0), xmax(nmat, 0.0);
+  auto bits = [](unsigned long long u) { double x; memcpy(&x, &u, 8); return x; };
+  CK(cudaMemsetAsync(dX, 0, sizeof(z64) * nmat * per, st));
+  CK(launch_to32((size_t)nmat * per, r, h->V32, st));
+  CK(lu_fwdsolve_ws<z32>(T, lb, h->V32, per, (int)N, (int)R, h->work32, st));
+  CK(lu_backsolve<z32>(T, lb, h->V32, per, (int)N, (int)R, st));
+  CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
+  CK(launch_update((int)per, nmat, h->V32, dX, h->norms, nullptr, st));
+  for (int it = 0; it < h->max_iter; ++it) {
+    CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
+    CK(cudaMemsetAsync(rnorm, 0, sizeof(unsigned long long) * nmat, st));
+    CK(launch_residual(c, np, dX, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, h->XD, h->V32,
+                       nullptr, rnorm, st, r));
+    if (it > 0 && h->refine_estimate) {
+      CK(cudaMemcpyAsync(nh.data() + 2 * nmat, rnorm, sizeof(unsigned long long) * nmat, cudaMemcpyDeviceToHost,
+                         st));
+      CK(cudaStreamSynchronize(st));
+      bool all = true;
+      for (int m = 0; m < nmat && all; ++m) {
+        if (skip[m]) continue;
+        const double est = kEstSafety * std::max(rho[m], 1.0) * bits(nh[2 * nmat + m]);
+        if (!((xmax[m] > 0 ? est / xmax[m] : est) <= h->tol)) all = false;
+      }
+      if (all) return 0;
+    }
+    CK(lu_fwdsolve_ws<z32>(T, lb, h->V32, per, (int)N, (int)R, h->work32, st));
+    CK(lu_backsolve<z32>(T, lb, h->V32, per, (int)N, (int)R, st));
+    CK(launch_update((int)per, nmat, h->V32, dX, h->norms, nullptr, st));
+    CK(cudaMemcpyAsync(nh.data(), h->norms, sizeof(unsigned long long) * 2 * nmat, cudaMemcpyDeviceToHost, st));
+    if (it == 0)
+      CK(cudaMemcpyAsync(nh.data() + 2 * nmat, rnorm, sizeof(unsigned long long) * nmat, cudaMemcpyDeviceToHost,
+                         st));
+    CK(cudaStreamSynchronize(st));
+    bool all = true;
+    for (int m = 0; m < nmat; ++m) {
+      const double md = bits(nh[2 * m]), mx = bits(nh[2 * m + 1]);
+      xmax[m] = mx;
+      if (it == 0) {
+        const double r1 = bits(nh[2 * nmat + m]);
+        rho[m] = r1 > 0 ? md / r1 : 1.0;
+      }
+      if (!skip[m] && !((mx > 0 ? md / mx : md) <= h->tol)) all = false;
+    }
+    if (all) return 0;
+  }
+  return fail(h, ADGA_ENOCONV, "tangent refinement did not converge");
+}
+
+// the tangent of direction d for one batch, after its forward pass.  FP64: T holds
+// the LU factors of the transposed BSE matrices (factorised with the left
+// interchanges) and X sits beside them; mixed: T holds the FP32 factors, X is
+// the refined X64, and the points in skip are re-solved in FP64 (with their
+// tangents) after this batch, so their tangent EOM terms are left out here.
+static int tan_batch(adga_handle *h, int d, int iwb, int np, int off, void *Tv, LUBatch lb, const z64 *chi0q,
+                     bool do_chi, bool do_eom, bool mixed, const std::vector<int> &skip) {
   TanState *t = h->tan[d];
   DevCtx &c = h->c;
   cudaStream_t st = h->st;
@@ -954,31 +1018,43 @@ static int tan_batch(adga_handle *h, int d, int iwb, int np, int off, z64 *T, LU
                           do_chi ? t->bub_nl + (size_t)off * h->nd4 : nullptr, st));
   }
   // X (compact) and the tangent right-hand sides dB + XS F~ + XD dF~
-  CK(cudaMemcpy2DAsync(w->Xc, per * sizeof(z64), T + N * N, strideM * sizeof(z64), per * sizeof(z64), 2 * np,
-                       cudaMemcpyDeviceToDevice, st));
-  CK(launch_xd(c, np, w->Xc, chi0q, h->c0inv, w->XD, true, st));
-  if (dchi0q) CK(launch_xd(c, np, w->Xc, dchi0q, h->c0inv, w->XS, false, st));
+  z64 *T = (z64 *)Tv;
+  const z64 *Xp = mixed ? h->X64 : w->Xc;
+  if (!mixed)
+    CK(cudaMemcpy2DAsync(w->Xc, per * sizeof(z64), T + N * N, strideM * sizeof(z64), per * sizeof(z64), 2 * np,
+                         cudaMemcpyDeviceToDevice, st));
+  CK(launch_xd(c, np, Xp, chi0q, h->c0inv, w->XD, true, st));
+  if (dchi0q) CK(launch_xd(c, np, Xp, dchi0q, h->c0inv, w->XS, false, st));
   for (int ch = 0; ch < 2; ++ch)
     CK(launch_tan_rhs(c, np, ch, dchi0q ? w->XS : nullptr, ch ? h->Frow_m : h->Frow_d,
                       t->loc_has ? w->XD : nullptr, t->loc_has ? (ch ? t->Fm : t->Fd) : nullptr,
                       t->loc_has ? (ch ? t->gm : t->gd) : nullptr, w->Rt, st));
   // dX = r A^-1 with the forward LU factors: T dX^T = r^T (forward, then back substitution)
-  CK(lu_build_perm(lb, w->perm, st));
-  lb.perm = w->perm;
-  CK(lu_fwdsolve_ws<z64>(T, lb, w->Rt, per, (int)N, (int)R, w->wk, st));
-  CK(lu_backsolve<z64>(T, lb, w->Rt, per, (int)N, (int)R, st));
+  const z64 *dX = w->Rt;
+  if (!mixed) {
+    CK(lu_build_perm(lb, w->perm, st));
+    lb.perm = w->perm;
+    CK(lu_fwdsolve_ws<z64>(T, lb, w->Rt, per, (int)N, (int)R, w->wk, st));
+    CK(lu_backsolve<z64>(T, lb, w->Rt, per, (int)N, (int)R, st));
+  } else {
+    std::vector<char> skipm(2 * np, 0);
+    for (int p : skip) skipm[2 * p] = skipm[2 * p + 1] = 1;
+    int rs = tan_solve_mixed(h, (z32 *)Tv, lb, chi0q, np, w->Rt, w->Xc, skipm);
+    if (rs) return rs;
+    dX = w->Xc;
+  }
   // dgamma^q_d
   CK(launch_gamq_tan(c, np, chi0q, dchi0q, h->c0inv, h->Frow_d, t->loc_has ? t->Fd : nullptr, w->gq, st));
   // chi sums and m_tot are bilinear: (a) with the tangents of X, gamma^w, gamma^q
   // against chi0^q and u; (b) with X, gamma^w, gamma^q against dchi0^q and du
   const z64 *gdw = t->loc_has ? t->gd : w->zero_gam, *gmw = t->loc_has ? t->gm : w->zero_gam;
-  CK(launch_post(c, np, w->Rt, 2 * per, per, (int)N, gdw, gmw, gdw, gmw, w->gq, chi0q, h->c0w, w->cA_d, w->cA_m,
+  CK(launch_post(c, np, dX, 2 * per, per, (int)N, gdw, gmw, gdw, gmw, w->gq, chi0q, h->c0w, w->cA_d, w->cA_m,
                  do_eom ? w->mA : nullptr, w->eta_d, w->eta_m, h->qidx_d, st));
   DevCtx cu = c;
   cu.u = t->du;
   cu.ut = t->dut;
   cu.vq = nullptr;
-  CK(launch_post(cu, np, w->Xc, 2 * per, per, (int)N, h->opg_d, h->opg_m, h->gam_d, h->gam_m, h->gq,
+  CK(launch_post(cu, np, Xp, 2 * per, per, (int)N, h->opg_d, h->opg_m, h->gam_d, h->gam_m, h->gq,
                  dchi0q ? dchi0q : w->zero_chi0, w->zero_N, w->cB_d, w->cB_m, do_eom ? w->mB : nullptr, w->eta_d,
                  w->eta_m, h->qidx_d, st));
   if (do_chi) {
@@ -991,6 +1067,8 @@ static int tan_batch(adga_handle *h, int d, int iwb, int np, int off, z64 *T, LU
   if (do_eom) {
     // dSigma += dm_tot G(k-q) + m_tot dG(k-q)
     CK(launch_zadd((size_t)np * c.nd2 * c.iwf * c.nd2, w->mB, w->mA, st));
+    for (int p : skip)     // re-solved in FP64 with their tangents (m_tot of these points is zero already)
+      CK(cudaMemsetAsync(w->mA + (size_t)p * c.nd2 * c.iwf * c.nd2, 0, sizeof(z64) * c.nd2 * c.iwf * c.nd2, st));
     CK(launch_eom_dynamic(c, iwb, h->qidx_d, np, w->mA, t->sigma_nl, st));
     if (t->has_dhk) {
       DevCtx cg = c;
@@ -1161,10 +1239,10 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
                        sizeof(z64) * c.nd2 * c.iwf * c.nd2, st));
   cudaEventRecord(ev[4], st);
   if (do_eom) CK(launch_eom_dynamic(c, iwb, h->qidx_d, np, h->mtot, h->sigma_nl, st));
-  if (prec == ADGA_FP64 && h->tan_on)
+  if (h->tan_on)
     for (int d = 0; d < ADGA_MAX_TANGENTS; ++d)
       if (h->tan[d]) {
-        int rt = tan_batch(h, d, iwb, np, off, (z64 *)h->Tm, lb, chi0q, do_chi, do_eom);
+        int rt = tan_batch(h, d, iwb, np, off, h->Tm, lb, chi0q, do_chi, do_eom, prec == ADGA_MIXED, fallback);
         if (rt) return rt;
       }
   cudaEventRecord(ev[5], st);
@@ -1296,7 +1374,7 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   return 0;
 }
 
-extern "C" int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, int *status,
+extern "C" int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, int precision, int *status,
                                        adga_run_stats *stats) {
   if (!h) return ADGA_EINVAL;
   int ndir = 0;
@@ -1325,7 +1403,8 @@ extern "C" int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, 
   }
   h->tan_on = true;
   h->loc_iwb = INT_MIN;
-  int r = adga_ladder_run(h, qwstart, qwstop, ADGA_FP64, status, stats);
+  if (precision != ADGA_FP64 && precision != ADGA_MIXED) return fail(h, ADGA_EINVAL, "precision");
+  int r = adga_ladder_run(h, qwstart, qwstop, precision, status, stats);
   h->tan_on = false;
   return r;
 }

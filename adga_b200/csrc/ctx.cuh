@@ -133,11 +133,12 @@ cudaError_t launch_eom_dynamic(const DevCtx &c, int iwb, const int *qidx, int np
 
 // k_refine.cu
 cudaError_t launch_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X, cudaStream_t st);
-// rnorm (nullable): per-matrix max |re| + |im| of the FP64 residual, atomicMax on the bit patterns
+// rnorm (nullable): per-matrix max |re| + |im| of the FP64 residual, atomicMax on the bit patterns;
+// Bpt (nullable): per-point right-hand sides in X's layout instead of (1+gamma^w) (tangent solves)
 cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q,
                             const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
                             const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, const z64 *extra_d,
-                            unsigned long long *rnorm, cudaStream_t st);
+                            unsigned long long *rnorm, cudaStream_t st, const z64 *Bpt = nullptr);
 cudaError_t launch_xd(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q, const z64 *c0inv, z64 *XD,
                       bool minus_one, cudaStream_t st);
 cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,

@@ -17,7 +17,7 @@
 cudaError_t launch_resid_z64(const DevCtx &c, int npts, const z64 *XD, const z64 *X,
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, z32 *V, const z64 *extra_d, unsigned long long *rnorm,
-                             cudaStream_t st);
+                             const z64 *Bpt, cudaStream_t st);
 
 // X64 = up(Y32) from the RHS columns of the FP32 factorised matrices
 __global__ void k_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X) {
@@ -154,12 +154,12 @@ cudaError_t launch_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat
 cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q,
                             const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
                             const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, const z64 *extra_d,
-                            unsigned long long *rnorm, cudaStream_t st) {
+                            unsigned long long *rnorm, cudaStream_t st, const z64 *Bpt) {
   size_t total = (size_t)c.nd2 * c.N * 2 * npts;
   k_xd<<<cdiv_u(total, 256), 256, 0, st>>>(c, npts, X, chi0q, c0inv, XD, 1);
   cudaError_t e = ADGA_LAUNCH_CHECK();
   if (e != cudaSuccess) return e;
-  return launch_resid_z64(c, npts, XD, X, Frow_d, Frow_m, opg_d, opg_m, V, extra_d, rnorm, st);
+  return launch_resid_z64(c, npts, XD, X, Frow_d, Frow_m, opg_d, opg_m, V, extra_d, rnorm, Bpt, st);
 }
 
 // XD = X blockdiag(chi0q chi0_loc^-1 - 1), or without the -1 (a tangent direction)

@@ -60,7 +60,7 @@ cudaError_t lu_trail_z64(z64 *M, const LUBatch &lb, int J, int jb, cudaStream_t 
 __global__ void __launch_bounds__(NT)
 k_resid_z64(int N, int R, int npts, int ch, const z64 *__restrict__ XD, const z64 *__restrict__ X,
             const z64 *__restrict__ Frow, const z64 *__restrict__ opg, z32 *V, const z64 *__restrict__ extra,
-            unsigned long long *rnorm) {
+            unsigned long long *rnorm, const z64 *__restrict__ Bpt) {
   extern __shared__ __align__(16) z64 zg_smem[];
   z64 *As = zg_smem, *Bs = zg_smem + STAGES * BK * BM;
   const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
@@ -89,7 +89,8 @@ k_resid_z64(int N, int R, int npts, int ch, const z64 *__restrict__ XD, const z6
     for (int j = 0; j < TN; ++j) {
       const int cl = c0 + ty + 16 * j;
       if (row >= rows || cl >= N) continue;
-      const z64 b = opg[i1 + (size_t)cl * R];
+      // right-hand side: (1+gamma^w) shared by the slice, or per point (tangent solves)
+      const z64 b = Bpt ? Bpt[m * per + (size_t)i1 * N + cl] : opg[i1 + (size_t)cl * R];
       const z64 x = X[m * per + (size_t)i1 * N + cl];
       z64 r = make_double2(b.x - x.x + acc[i][j].x, b.y - x.y + acc[i][j].y);
       if (extra) r = cadd(r, extra[(size_t)p * per + (size_t)i1 * N + cl]);   // V(q) term (density)
@@ -106,16 +107,16 @@ k_resid_z64(int N, int R, int npts, int ch, const z64 *__restrict__ XD, const z6
 cudaError_t launch_resid_z64(const DevCtx &c, int npts, const z64 *XD, const z64 *X,
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, z32 *V, const z64 *extra_d, unsigned long long *rnorm,
-                             cudaStream_t st) {
+                             const z64 *Bpt, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_resid_z64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     attr = true;
   }
   dim3 g(cdiv_u(c.N, BN), cdiv_u((size_t)npts * c.R, BM));
-  k_resid_z64<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, 0, XD, X, Frow_d, opg_d, V, extra_d, rnorm);
+  k_resid_z64<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, 0, XD, X, Frow_d, opg_d, V, extra_d, rnorm, Bpt);
   cudaError_t e = ADGA_LAUNCH_CHECK();
   if (e != cudaSuccess) return e;
-  k_resid_z64<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, 1, XD, X, Frow_m, opg_m, V, nullptr, rnorm);
+  k_resid_z64<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, 1, XD, X, Frow_m, opg_m, V, nullptr, rnorm, Bpt);
   return ADGA_LAUNCH_CHECK();
 }

@@ -6,7 +6,7 @@ is differentiable in ``params = (U, J, t)``: the Kanamori couplings (V = U - 2J)
 and the hopping scale t of the synthetic model, at the DMFT one-particle
 inputs of ``base`` (siw, giw, mu held fixed).
 
-The forward pass runs the ladder once with the three tangent directions of
+The forward pass runs the ladder (FP64 or mixed precision) once with the three tangent directions of
 (U, J, t) (``adga_ladder_run_tangent``: the hand-written forward-mode
 derivative of every stage, d(A^-1) = -A^-1 dA A^-1 through the BSE with the
 forward LU factors, and the tangent chi0 and EOM contractions); the backward
@@ -28,7 +28,7 @@ from . import synth
 from .ladder import Ladder
 
 
-def _run(prob, tangents: bool):
+def _run(prob, tangents: bool, precision: str):
     s = prob.spec
     with Ladder.from_problem(prob) as lad:
         for iwb in range(-s.iwb, s.iwb + 1):
@@ -40,9 +40,9 @@ def _run(prob, tangents: bool):
                 if dvertex is not None:
                     for iwb in range(-s.iwb, s.iwb + 1):
                         lad.set_vertex_tangent(iwb, *dvertex(iwb), direction=d)
-            lad.ladder_run_tangent()
+            lad.ladder_run_tangent(precision=precision)
         else:
-            lad.ladder_run(1, None, "fp64")
+            lad.ladder_run(1, None, precision)
         fwd = lad.assemble(lad.get_outputs(), prob.siw)
         tans = [lad.assemble_tangent(lad.get_tangent_outputs(d)) for d in range(len(synth.PARAMS))] \
             if tangents else []
@@ -53,11 +53,11 @@ def _run(prob, tangents: bool):
 
 class _LadderFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, params, base, tangents):
+    def forward(ctx, params, base, tangents, precision):
         U, J, t = (float(x) for x in params.detach().cpu().numpy())
         s = base.spec
         prob = synth.perturbed_problem(base, dU=U - s.U, dJ=J - s.J, dt=t - s.hop["t"])
-        (chi_m, sig), tans = _run(prob, tangents)
+        (chi_m, sig), tans = _run(prob, tangents, precision)
         ctx.tans = tans
         return torch.from_numpy(chi_m), torch.from_numpy(sig)
 
@@ -71,12 +71,16 @@ class _LadderFn(torch.autograd.Function):
             if g_sig is not None:
                 v = v + (torch.conj(g_sig) * torch.from_numpy(dsig)).real.sum()
             out.append(v)
-        return torch.stack(out), None, None
+        return torch.stack(out), None, None, None
 
 
-def ladder_chi_sigma(params: torch.Tensor, base):
+def ladder_chi_sigma(params: torch.Tensor, base, precision: str = "fp64"):
     """(chi_m(q, omega=0) (ndim2, ndim2, nqp), Sigma (ndim, ndim, 2 iwf, nkp)), complex128,
-    differentiable in params = tensor([U, J, t], dtype=float64)."""
+    differentiable in params = tensor([U, J, t], dtype=float64).  precision "fp64"
+    (FP64 LU) or "mixed" (FP32 LU with FP64 refinement of the outputs and of
+    their tangents, agreeing with FP64 to ~1e-12)."""
     if params.shape != (3,) or params.dtype != torch.float64:
         raise ValueError("params must be a float64 tensor [U, J, t]")
-    return _LadderFn.apply(params, base, torch.is_grad_enabled() and params.requires_grad)
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("precision must be 'fp64' or 'mixed'")
+    return _LadderFn.apply(params, base, torch.is_grad_enabled() and params.requires_grad, precision)

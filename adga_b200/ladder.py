@@ -267,14 +267,14 @@ class Ladder:
     def clear_tangents(self):
         self._check(self._lib.adga_clear_tangents(self._h), "clear_tangents")
 
-    def ladder_run_tangent(self, qwstart=1, qwstop=None):
-        """FP64 ladder plus the tangents of every direction set before."""
+    def ladder_run_tangent(self, qwstart=1, qwstop=None, precision="fp64"):
+        """The ladder (FP64 or mixed) plus the tangents of every direction set before."""
         if qwstop is None:
             qwstop = self.nqp * (2 * self.iwb + 1)
         n = qwstop - qwstart + 1
         status = np.zeros(n, dtype=np.int32)
         st = RunStats()
-        rc = self._lib.adga_ladder_run_tangent(self._h, int(qwstart), int(qwstop),
+        rc = self._lib.adga_ladder_run_tangent(self._h, int(qwstart), int(qwstop), PRECISION[precision],
                                                status.ctypes.data_as(C.POINTER(C.c_int)), C.byref(st))
         self._check(rc, "ladder_run_tangent")
         self.last_npts = n

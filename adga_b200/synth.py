@@ -96,6 +96,8 @@ SPECS: Dict[str, Spec] = {
                hop=dict(t=0.2, t2=0.12), filling=0.3, seed=15, offdiag=0.03),
 }
 SPECS["c2"] = Spec(**{**SPECS["c1"].__dict__, "name": "c2"})
+# the differentiation model on a 4^3 k / 2^3 q sub-grid (dense-Jacobian checks): BSE 320 x 320
+SPECS["c3s"] = Spec(**{**SPECS["c3"].__dict__, "name": "c3s", "nk": (4, 4, 4), "nq": (2, 2, 2)})
 
 
 def sweep_specs(n=64, seed=4321):

@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 arm")
     ap.add_argument("--no-grad", action="store_true",
-                    help="skip the gradient arm (FP64 ladder + tangents in U, J, t)")
+                    help="skip the gradient arm (ladder + tangents in U, J, t, mixed and FP64)")
     ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--points", type=int, default=0,
@@ -284,8 +284,8 @@ def main():
         ms64, st64, clk64 = timed("fp64")
         res["fp64"] = world * npts * args.steps / (ms64 * 1e-3)
 
-    # gradient arm: the FP64 ladder with the tangents of (U, J, t) in the same
-    # pass (everything the backward of adga_b200.grad needs), on the same steps
+    # gradient arm: the ladder with the tangents of (U, J, t) in the same pass
+    # (everything the backward of adga_b200.grad needs), mixed and FP64, on the same steps
     grad = None
     if not args.no_grad:
         for d, par in enumerate(synth.PARAMS):
@@ -295,19 +295,26 @@ def main():
                 for iwb in sorted(set(omegas)):
                     lad.set_vertex_tangent(iwb, *dvertex(iwb), direction=d)
         p.clear_vertex_cache()
-        for s in range(args.warmup):
-            lad.ladder_run_tangent(*slice_range(omegas[s]))
-        barrier()
-        ms_g = 0.0
-        for s in range(args.warmup, nsteps):
-            ms_g += lad.ladder_run_tangent(*slice_range(omegas[s]))[1]["ms_total"]
-        barrier()
-        ms_g = allmax(ms_g)
+
+        def timed_grad(prec):
+            for s in range(args.warmup):
+                lad.ladder_run_tangent(*slice_range(omegas[s]), prec)
+            barrier()
+            ms = 0.0
+            for s in range(args.warmup, nsteps):
+                ms += lad.ladder_run_tangent(*slice_range(omegas[s]), prec)[1]["ms_total"]
+            barrier()
+            return allmax(ms)
+
+        ms_gm = timed_grad("mixed")
+        ms_g64 = timed_grad("fp64")
         lad.clear_tangents()
-        grad = {"directions": list(synth.PARAMS), "value": world * npts * args.steps / (ms_g * 1e-3),
-                "unit": UNIT, "ms_per_step": ms_g / args.steps,
-                "over_fp64_forward": (ms_g / ms64) if not args.no_fp64 else None,
-                "over_mixed_forward": ms_g / ms_mixed}
+        # the mixed-precision gradient against the mixed forward, the FP64 one against FP64
+        grad = {"directions": list(synth.PARAMS), "precision": "mixed",
+                "value": world * npts * args.steps / (ms_gm * 1e-3), "unit": UNIT,
+                "ms_per_step": ms_gm / args.steps, "over_mixed_forward": ms_gm / ms_mixed,
+                "fp64": {"value": world * npts * args.steps / (ms_g64 * 1e-3), "ms_per_step": ms_g64 / args.steps,
+                         "over_fp64_forward": (ms_g64 / ms64) if not args.no_fp64 else None}}
 
     # accuracy: mixed vs FP64 on the same slice, and vs the oracle on sampled points
     iwb_chk = omegas[-1]

@@ -237,10 +237,13 @@ int adga_get_outputs(adga_handle *h, const adga_outputs *o);
  * dG = G dH G in chi0 and the EOM, d(F~) = sym(dchi_loc) chi0_loc^-1,
  * dX = (d(1+gamma^w) - X dA) A^-1 through the BSE (d(A^-1) = -A^-1 dA A^-1,
  * with the LU factors of the forward solve), the chi sums and m_tot.
- * adga_ladder_run_tangent runs the FP64 ladder over qwstart..qwstop once (its
- * forward outputs accumulate as with adga_ladder_run) together with every
- * direction set; adga_get_tangent_outputs returns direction dir in the layouts
- * of adga_get_outputs (bubble_loc and sigma_hf: zero).  Not with V(q).
+ * adga_ladder_run_tangent runs the ladder over qwstart..qwstop once in the
+ * given precision (its forward outputs accumulate as with adga_ladder_run)
+ * together with every direction set: ADGA_FP64 solves the tangents with the
+ * FP64 LU factors, ADGA_MIXED with the FP32 factors and FP64 refinement
+ * (ADGA_ENOCONV if a tangent's refinement does not converge);
+ * adga_get_tangent_outputs returns direction dir in the layouts of
+ * adga_get_outputs (bubble_loc and sigma_hf: zero).  Not with V(q).
  * adga_clear_tangents drops every direction.
  */
 #define ADGA_MAX_TANGENTS 4
@@ -248,7 +251,7 @@ int adga_set_tangent(adga_handle *h, int dir, const adga_z *dhk, const adga_z *d
                      const adga_z *du_tilde);
 int adga_set_vertex_tangent(adga_handle *h, int dir, int iwb, const adga_z *dchi_loc_dens,
                             const adga_z *dchi_loc_magn);
-int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, int *status,
+int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, int precision, int *status,
                             adga_run_stats *stats);
 int adga_get_tangent_outputs(adga_handle *h, int dir, const adga_outputs *o);
 int adga_clear_tangents(adga_handle *h);

@@ -30,12 +30,14 @@ def test_gradcheck_chi_m_and_sigma():
     assert torch.autograd.gradcheck(lambda y: ladder_chi_sigma(y, p), (x,), eps=H, atol=1e-7, rtol=1e-5)
 
 
-@pytest.mark.parametrize("name", ["t2", "t3"])
-def test_loss_gradient_matches_finite_differences(name):
+@pytest.mark.parametrize("name,precision", [("t2", "fp64"), ("t3", "fp64"), ("t2", "mixed"), ("t3", "mixed")])
+def test_loss_gradient_matches_finite_differences(name, precision):
+    """The mixed forward leaves a ~1e-12 relative refinement remainder, so its
+    difference quotients carry ~1e-7 relative noise: 1e-5 for mixed."""
     p = problem(name)
     rng = np.random.default_rng(7)
     x = params_of(p)
-    chi, sig = ladder_chi_sigma(x, p)
+    chi, sig = ladder_chi_sigma(x, p, precision)
     wc = torch.from_numpy(rng.standard_normal(chi.shape) + 1j * rng.standard_normal(chi.shape))
     ws = torch.from_numpy(rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape))
 
@@ -48,11 +50,12 @@ def test_loss_gradient_matches_finite_differences(name):
         for i in range(3):
             e = torch.zeros(3, dtype=torch.float64)
             e[i] = H
-            lp = loss(*ladder_chi_sigma(x.detach() + e, p))
-            lm = loss(*ladder_chi_sigma(x.detach() - e, p))
+            lp = loss(*ladder_chi_sigma(x.detach() + e, p, precision))
+            lm = loss(*ladder_chi_sigma(x.detach() - e, p, precision))
             want.append(float((lp - lm) / (2 * H)))
     got = x.grad.numpy()
-    assert np.max(np.abs(got - want)) < 1e-6 * max(1.0, np.max(np.abs(want))), (got, want)
+    tol = 1e-6 if precision == "fp64" else 1e-5
+    assert np.max(np.abs(got - want)) < tol * max(1.0, np.max(np.abs(want))), (got, want)
 
 
 def oracle_chi_sigma(p):

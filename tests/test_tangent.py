@@ -1,5 +1,5 @@
 """Derivatives of the ladder outputs (forward-mode tangents through the BSE,
-the chi0 and EOM contractions; adga_ladder_run_tangent).
+the chi0 and EOM contractions; adga_ladder_run_tangent), FP64 and mixed.
 
 For each model parameter U, J (Kanamori, V = U - 2J) and the hopping scale t,
 at fixed DMFT one-particle inputs:
@@ -10,6 +10,7 @@ at fixed DMFT one-particle inputs:
 both to 1e-6 relative (finite-difference truncation ~h^2, rounding ~1e-11).
 """
 import dataclasses
+from functools import lru_cache
 
 import numpy as np
 import pytest
@@ -40,7 +41,7 @@ def oracle_forward(p):
     return out
 
 
-def gpu_tangent(p, par):
+def gpu_tangent(p, par, precision="fp64"):
     s = p.spec
     dhk, du, dut, dvertex = synth.tangent_inputs(p, par)
     with Ladder.from_problem(p) as lad:
@@ -49,7 +50,7 @@ def gpu_tangent(p, par):
             if dvertex is not None:
                 lad.set_vertex_tangent(iwb, *dvertex(iwb))
         lad.set_tangent(dhk, du, dut)
-        lad.ladder_run_tangent()
+        lad.ladder_run_tangent(precision=precision)
         fwd = lad.assemble(lad.get_outputs(), p.siw)
         tan = lad.assemble_tangent(lad.get_tangent_outputs())
     return fwd, tan
@@ -82,3 +83,52 @@ def test_tangent_matches_oracle_finite_differences(par):
     want = fd(oracle_forward, p, par)
     for k in KEYS:
         assert rel_err(tan[k], want[k]) < 1e-6, (par, k, rel_err(tan[k], want[k]))
+
+
+@pytest.mark.parametrize("name", ["t2", "t3m"])
+@pytest.mark.parametrize("par", synth.PARAMS)
+def test_mixed_tangent_matches_fp64(name, par):
+    """FP32 factors with FP64 refinement of the tangent solves: the tangents (and
+    the forward outputs of the same run) agree with the FP64 path to the
+    refinement's tolerance."""
+    p = problem(name)
+    f64, t64 = gpu_tangent(p, par, "fp64")
+    fmx, tmx = gpu_tangent(p, par, "mixed")
+    for k in KEYS:
+        assert rel_err(fmx[k], f64[k]) < 1e-9, (k, rel_err(fmx[k], f64[k]))
+        assert rel_err(tmx[k], t64[k]) < 1e-9, (par, k, rel_err(tmx[k], t64[k]))
+
+
+def c3s_pick(out, s):
+    w0 = s.iwb * s.nqp + np.arange(s.nqp)
+    return out["chi_magn"][:, :, w0], out["sigma"]
+
+
+@lru_cache(maxsize=None)
+def c3s_oracle_jacobian():
+    """Central differences (h = 1e-5, the 4-point stencil
+    (-f(2h) + 8 f(h) - 8 f(-h) + f(-2h)) / 12h) of the oracle's chi_m(q, omega=0)
+    and Sigma on the differentiation model's 4^3 sub-grid, one column per
+    parameter.  chi_m is large and steep in U at beta = 20, where the 2-point
+    quotient's h^2 truncation alone reaches 1e-5 relative."""
+    p = problem("c3s")
+    cols = {}
+    for par, kw in zip(synth.PARAMS, ("dU", "dJ", "dt")):
+        f = {m: c3s_pick(oracle_forward(synth.perturbed_problem(p, **{kw: m * H})), p.spec) for m in (-2, -1, 1, 2)}
+        cols[par] = tuple((-f[2][i] + 8 * f[1][i] - 8 * f[-1][i] + f[-2][i]) / (12 * H) for i in range(2))
+    return cols
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_c3_subgrid_tangents_match_oracle_dense_jacobian(precision):
+    """dchi_m(q, omega=0)/dU, /dJ and dSigma/dU, /dt (every parameter, both outputs) on
+    the differentiation model (2 e_g orbitals, beta = 20, 2 x 40 fermionic and 11
+    bosonic frequencies, BSE 320 x 320) restricted to a 4^3 k / 2^3 q grid."""
+    p = problem("c3s")
+    jac = c3s_oracle_jacobian()
+    for par in synth.PARAMS:
+        _, tan = gpu_tangent(p, par, precision)
+        dchi, dsig = c3s_pick(tan, p.spec)
+        wchi, wsig = jac[par]
+        assert rel_err(dchi, wchi) < 1e-6, (par, "chi_m", rel_err(dchi, wchi))
+        assert rel_err(dsig, wsig) < 1e-6, (par, "sigma", rel_err(dsig, wsig))
