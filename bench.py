@@ -50,6 +50,9 @@ def parse():
                     help="skip the gradient arm (ladder + tangents in U, J, t, mixed and FP64)")
     ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--compare-library-lu", action="store_true",
+                    help="also time the library batched LU (torch.linalg.lu_factor) on matrices of the "
+                         "workload's size, FP64 and FP32, for comparison with this library's LU")
     ap.add_argument("--points", type=int, default=0,
                     help="q points per step (0 = the whole slice); smaller cases are for profiling")
     return ap.parse_args()
@@ -316,6 +319,25 @@ def main():
                 "fp64": {"value": world * npts * args.steps / (ms_g64 * 1e-3), "ms_per_step": ms_g64 / args.steps,
                          "over_fp64_forward": (ms_g64 / ms64) if not args.no_fp64 else None}}
 
+    # comparison only: a library batched LU on matrices of the same size (not this library's path)
+    library_lu = None
+    if args.compare_library_lu:
+        library_lu = {}
+        gen = torch.Generator(device="cuda").manual_seed(0)
+        nbse = spec.ndim ** 2 * 2 * spec.iwf
+        for name, dt in (("complex128", torch.complex128), ("complex64", torch.complex64)):
+            nb = 128
+            A = torch.eye(nbse, dtype=dt, device="cuda").expand(nb, nbse, nbse).clone()
+            A += 0.02 * torch.randn(nb, nbse, nbse, dtype=dt, device="cuda", generator=gen)
+            torch.linalg.lu_factor(A.clone())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            X = A.clone()
+            torch.cuda.synchronize()
+            e0.record(); torch.linalg.lu_factor(X); e1.record(); torch.cuda.synchronize()
+            library_lu[name] = {"ms_per_matrix": e0.elapsed_time(e1) / nb, "batch": nb}
+            del A, X
+        torch.cuda.empty_cache()
+
     # accuracy: mixed vs FP64 on the same slice, and vs the oracle on sampled points
     iwb_chk = omegas[-1]
     acc = {}
@@ -396,8 +418,9 @@ def main():
             "alg_bytes_per_launch": gbytes * 1e9 / nlaunch, "avg_launch_ms": mst / nlaunch,
             "complex_tflops": gflop / mst if mst else 0.0,
             "bf16_tensor_tflops": 3 * gflop / mst if mst else 0.0}
-    stage = {k: sum(s[k] for s in st_mixed) / args.steps for k in
-             ("ms_chi0", "ms_bse", "ms_lu", "ms_trail", "ms_post", "ms_eom", "ms_total")}
+    stage_keys = ("ms_chi0", "ms_bse", "ms_lu", "ms_trail", "ms_post", "ms_eom", "ms_total")
+    stage = {k: sum(s[k] for s in st_mixed) / args.steps for k in stage_keys}
+    stage64 = {k: sum(s[k] for s in st64) / args.steps for k in stage_keys} if not args.no_fp64 else None
     line = {"metric": METRIC, "value": v_mixed, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
@@ -406,10 +429,10 @@ def main():
             "data": "synthetic (seeded SrVO3-like t2g model, chi_loc = (chi0_loc^-1 + Gamma)^-1)",
             "config": config(args, spec, npts), "fp64_value": res.get("fp64"),
             "mixed_over_fp64": (v_mixed / res["fp64"]) if res.get("fp64") else None,
-            "accuracy": acc, "stage_ms_per_step": stage,
+            "accuracy": acc, "stage_ms_per_step": stage, "fp64_stage_ms_per_step": stage64,
             "refine": {"max_iters": max(s["max_refine_iters"] for s in st_mixed),
                        "fallbacks": sum(s["mixed_fallbacks"] for s in st_mixed)},
-            "gradient": grad,
+            "gradient": grad, "library_lu": library_lu,
             "roofline": roof, "cpu_baseline": cpu_line, "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in st_mixed)),
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
