@@ -485,103 +485,15 @@ k_swap_trsm(T *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int n
 // of the FP64 refinement): the BSE matrices are close to the identity (growth
 // factor 1.00 and condition numbers of 1..40 on the t2g workload), so the
 // factorisation needs no row interchanges.  Per step:
-//   k_diag_nopiv  LU of the jb x jb diagonal block in shared memory (one CTA
-//                 per matrix); identity pivots and an empty interchange map;
-//   k_triinv      its inverted L11 / U11 blocks, as in the pivoted step;
-//   k_l21         L21 = A21 U11^-1, a 64-row x jb tile per CTA, every row
-//                 independent (no pivot search over the column);
-//   k_swap_trsm   U12 = L11^-1 A12 with the empty map.
+//   k_diag_inv    LU of the jb x jb diagonal block in shared memory with its
+//                 inverted L11 / U11 blocks (one CTA per matrix); identity
+//                 pivots and an empty interchange map;
+//   k_tri_tile    L21 = A21 U11^-1 and U12 = L11^-1 A12, every row / column
+//                 independent (no pivot search over the column).
 // A zero pivot gives non-finite factors; the refinement then fails to
 // converge and the point is re-solved in FP64 with partial pivoting.
 // ---------------------------------------------------------------------------
 constexpr int DN_LD = 65;
-
-template <typename T>
-__global__ void __launch_bounds__(256)
-k_diag_nopiv(T *M, size_t strideM, int N, int J, int jb, int *ipiv_all, int *rmap_all) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T *D = reinterpret_cast<T *>(smraw);          // [jb rows][DN_LD], column-major
-  __shared__ T s_rcp;
-  const int b = blockIdx.x, t = threadIdx.x;
-  T *A = M + (size_t)b * strideM;
-  for (int e = t; e < jb * jb; e += 256) {
-    const int i = e % jb, j = e / jb;
-    D[i + j * DN_LD] = A[(size_t)(J + i) + (size_t)(J + j) * N];
-  }
-  __syncthreads();
-  for (int k = 0; k < jb; ++k) {
-    if (t == 0) s_rcp = crcp(D[k + k * DN_LD]);
-    __syncthreads();
-    const T rcp = s_rcp;
-    for (int i = k + 1 + t; i < jb; i += 256) D[i + k * DN_LD] = cmul(D[i + k * DN_LD], rcp);
-    __syncthreads();
-    const int m = jb - k - 1;
-    for (int e = t; e < m * m; e += 256) {
-      const int i = k + 1 + e % m, j = k + 1 + e / m;
-      D[i + j * DN_LD] = csub(D[i + j * DN_LD], cmul(D[i + k * DN_LD], D[k + j * DN_LD]));
-    }
-    __syncthreads();
-  }
-  for (int e = t; e < jb * jb; e += 256) {
-    const int i = e % jb, j = e / jb;
-    A[(size_t)(J + i) + (size_t)(J + j) * N] = D[i + j * DN_LD];
-  }
-  int *ip = ipiv_all + (size_t)b * N + J;
-  for (int i = t; i < jb; i += 256) ip[i] = J + i;
-  if (t == 0) rmap_all[(size_t)b * RMAP_STRIDE] = 0;
-}
-
-// L21 = A21 U11^-1 in place for rows J+jb+r0 .. +64 of one matrix; thread
-// (t % 16, t / 16) owns rows rq + 16 i and columns cq + 16 j (i, j < 4), so
-// that every thread's columns reach about the same depth of the triangle.
-template <typename T>
-__global__ void __launch_bounds__(256)
-k_l21(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, const T *Uinv) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T *As = reinterpret_cast<T *>(smraw);        // [64 k][DN_LD rows]
-  T *Us = As + 64 * DN_LD;                      // [64 k][64 c] (row k of U11^-1)
-  const int b = blockIdx.y, t = threadIdx.x;
-  T *A = M + (size_t)b * strideM;
-  const int r0 = J + jb + blockIdx.x * 64;
-  const int nr = min(64, N - r0);
-  const T *U = Uinv + ((size_t)b * nsteps + J / NB) * NB * NB;
-  for (int e = t; e < 64 * 64; e += 256) {
-    const int r = e & 63, k = e >> 6;
-    As[r + k * DN_LD] = (r < nr && k < jb) ? A[(size_t)(r0 + r) + (size_t)(J + k) * N] : czero<T>();
-    const int kk = e & 63, c = e >> 6;       // U11^-1 (kk, c): zero below the diagonal
-    Us[c + kk * 64] = (kk < jb && c < jb) ? U[kk + c * NB] : czero<T>();
-  }
-  __syncthreads();
-  const int rq = t & 15, cq = t >> 4;
-  T acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = czero<T>();
-  const int kend = min(jb, cq + 49);           // U11^-1 (k, c) = 0 for k > c
-#pragma unroll 4
-  for (int k = 0; k < kend; ++k) {
-    T a[4], u[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = As[rq + 16 * i + k * DN_LD];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) u[j] = Us[cq + 16 * j + k * 64];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], u[j]);
-  }
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int c = cq + 16 * j;
-    if (c >= jb) continue;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = rq + 16 * i;
-      if (r < nr) A[(size_t)(r0 + r) + (size_t)(J + c) * N] = acc[i][j];
-    }
-  }
-}
 
 // Diagonal block of an unpivoted step with its inverses, one CTA per matrix
 // (FP32): the jb x jb block is padded with the identity to 64 x 64 and
@@ -1206,12 +1118,9 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
   const size_t sm_trsm = sizeof(typename TrsmOp<T>::L) * 64 * 64 + sizeof(typename TrsmOp<T>::X) * TW * TS_LD;
   static bool attr_done[2] = {false, false};
   const int ti = sizeof(T) == sizeof(z64) ? 0 : 1;
-  const size_t sm_diag = sizeof(T) * 64 * DN_LD, sm_l21 = sizeof(T) * (64 * DN_LD + 64 * 64);
   if (!attr_done[ti]) {
     cudaFuncSetAttribute(k_triinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_swap_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_diag_nopiv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_l21<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_done[ti] = true;
   }
   const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
@@ -1221,21 +1130,12 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
       return lu_trail_step<T>(M, lb, J, jb, trail, trail_ctx, st, tt);
     }
   }
-  if (nopiv) {
-    k_diag_nopiv<T><<<lb.batch, 256, sm_diag, st>>>(M, lb.strideM, lb.N, J, jb, lb.ipiv, lb.rmap);
-    if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-  } else if ((e = launch_panel<T>(M, lb, J, jb, st)) != cudaSuccess) {
-    return e;
-  }
+  if (nopiv) return cudaErrorInvalidValue;     // the unpivoted step is the FP32 factorisation only
+  if ((e = launch_panel<T>(M, lb, J, jb, st)) != cudaSuccess) return e;
   k_triinv<T><<<lb.batch, 256, sm_tri, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps,
                                              (T *)lb.Linv, (T *)lb.Uinv, lb.ipiv, lb.rmap);
   if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-  if (nopiv && J + jb < lb.N) {
-    k_l21<T><<<dim3(cdiv_u(lb.N - J - jb, 64), lb.batch), 256, sm_l21, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB,
-                                                                            nsteps, (const T *)lb.Uinv);
-    if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-  }
-  const int nleft = (apply_left && !nopiv) ? (J + TW - 1) / TW : 0;
+  const int nleft = apply_left ? (J + TW - 1) / TW : 0;
   const int nright = (lb.ncols - J - jb + TW - 1) / TW;
   if (nleft > 0) {
     k_swap_left<T><<<dim3(nleft, lb.batch), 256, 0, st>>>(M, lb.strideM, lb.N, J, lb.rmap);

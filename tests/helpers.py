@@ -46,7 +46,8 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b)) / den)
 
 
-LIBRARY_ENV = ("ADGA_DFT_MIN_POINTS", "ADGA_BUBBLE", "ADGA_MIXED_PIVOT", "ADGA_MAX_REFINE")
+LIBRARY_ENV = ("ADGA_DFT_MIN_POINTS", "ADGA_BUBBLE", "ADGA_MIXED_PIVOT", "ADGA_MAX_REFINE",
+               "ADGA_REFINE_EXACT", "ADGA_NO_PAIRS")
 
 
 @contextlib.contextmanager

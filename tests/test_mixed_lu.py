@@ -38,6 +38,18 @@ def test_mixed_factorisation_matches_oracle(name, pivot):
         assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
 
 
+@pytest.mark.parametrize("name", ["t3b", "t3m"])
+def test_step_by_step_updates_match_oracle(name):
+    """ADGA_NO_PAIRS=1: the unpivoted FP32 factorisation with one tensor-core
+    update per step instead of the delayed pair updates."""
+    p = problem(name)
+    status, stats, got = run_mixed(p, {"ADGA_NO_PAIRS": "1"})
+    want = oracle_run(p)
+    assert stats["mixed_fallbacks"] == 0 and not status.any()
+    for k in ("chi_dens", "chi_magn", "sigma"):
+        assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
+
+
 def test_unconverged_points_are_resolved_in_fp64():
     p = problem("t3m")
     status, stats, got = run_mixed(p, {"ADGA_MAX_REFINE": "1"})
