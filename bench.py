@@ -50,6 +50,9 @@ def parse():
                     help="skip the gradient arm (ladder + tangents in U, J, t, mixed and FP64)")
     ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--full-grid", action="store_true",
+                    help="also run every omega slice (the whole q x omega grid) in both precisions and "
+                         "report the errors of chi_d/m(q, omega) and of the accumulated Sigma(k, nu)")
     ap.add_argument("--compare-library-lu", action="store_true",
                     help="also time the library batched LU (torch.linalg.lu_factor) on matrices of the "
                          "workload's size, FP64 and FP32, for comparison with this library's LU")
@@ -319,6 +322,27 @@ def main():
                 "fp64": {"value": world * npts * args.steps / (ms_g64 * 1e-3), "ms_per_step": ms_g64 / args.steps,
                          "over_fp64_forward": (ms_g64 / ms64) if not args.no_fp64 else None}}
 
+    # whole grid: every omega slice in both precisions, Sigma accumulated over all of them
+    full_grid = None
+    if args.full_grid:
+        for iwb in range(-spec.iwb, spec.iwb + 1):
+            if iwb not in pinned:
+                lad.set_vertex(iwb, *p.vertex(iwb))
+        p.clear_vertex_cache()
+        nqw = spec.nqp * nw
+        grid_out, grid_ms = {}, {}
+        for prec in ("fp64", "mixed"):
+            lad.reset_outputs()
+            _, stg = lad.ladder_run(1, nqw, prec)
+            grid_ms[prec] = stg["ms_total"]
+            grid_out[prec] = lad.assemble(lad.get_outputs(), p.siw)
+        full_grid = {"qw_points": nqw, "ms_fp64": grid_ms["fp64"], "ms_mixed": grid_ms["mixed"],
+                     "mixed_over_fp64": grid_ms["fp64"] / grid_ms["mixed"],
+                     "mixed_vs_fp64": {k: float(np.max(np.abs(grid_out["mixed"][k] - grid_out["fp64"][k]))
+                                               / np.max(np.abs(grid_out["fp64"][k])))
+                                       for k in ("chi_dens", "chi_magn", "sigma")}}
+        del grid_out
+
     # comparison only: a library batched LU on matrices of the same size (not this library's path)
     library_lu = None
     if args.compare_library_lu:
@@ -432,7 +456,7 @@ def main():
             "accuracy": acc, "stage_ms_per_step": stage, "fp64_stage_ms_per_step": stage64,
             "refine": {"max_iters": max(s["max_refine_iters"] for s in st_mixed),
                        "fallbacks": sum(s["mixed_fallbacks"] for s in st_mixed)},
-            "gradient": grad, "library_lu": library_lu,
+            "gradient": grad, "library_lu": library_lu, "full_grid": full_grid,
             "roofline": roof, "cpu_baseline": cpu_line, "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in st_mixed)),
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
