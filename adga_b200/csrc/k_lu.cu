@@ -499,11 +499,12 @@ constexpr int DN_LD = 65;
 // (FP32): the jb x jb block is padded with the identity to 64 x 64 and
 // factored right-looking with one barrier per column (the column scaling by
 // 1/u_kk is deferred to the end, so no thread writes what another reads);
-// L11^-1 and U11^-1 then follow in 16 x 16 blocks: eight warps invert the
-// diagonal blocks of both triangles (lane = column, no barriers), and three
-// block rows of L^-1 (downwards) and U^-1 (upwards) are filled in pairs of
-// small block products, two barriers each.
-constexpr int DI_SCR = 6 * 256;
+// L11^-1 (strictly lower; unit diagonal implied) and U11^-1 (upper with the
+// diagonal) then share one array and follow in 16 x 16 blocks: eight warps
+// invert the diagonal blocks of both triangles (lane = column, no barriers),
+// and three block rounds fill L^-1 downwards and U^-1 upwards, each a pair of
+// small block products per triangle.  73 KB of shared memory: three CTAs per SM.
+constexpr int DI_SCR = 3 * 256;
 
 __device__ __forceinline__ void cfma2(z32 &acc, z32 a, z32 u) {
   acc = __ffma2_rn(make_float2(a.x, a.x), u, acc);
@@ -517,13 +518,15 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
            int *rmap_all) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T *D = reinterpret_cast<T *>(smraw);          // [64][DN_LD] factored block
-  T *XL = D + 64 * DN_LD;                       // L11^-1
-  T *XU = XL + 64 * DN_LD;                      // U11^-1
-  T *S = XU + 64 * DN_LD;                       // block-product scratch: L blocks 0..2, U blocks 3..5
+  T *X = D + 64 * DN_LD;                        // L11^-1 below the diagonal, U11^-1 on and above it
+  T *S = X + 64 * DN_LD;                        // block-product scratch (3 blocks)
   __shared__ T rcps[64];
   const int b = blockIdx.x, t = threadIdx.x;
   T *A = M + (size_t)b * strideM;
   const T one = cx<T>::make(1, 0), zero = czero<T>();
+  // entries of the two inverses: L^-1 with its unit diagonal and zeros above, U^-1 with zeros below
+  auto lval = [&](int r, int c) { return r > c ? X[r + c * DN_LD] : (r == c ? one : zero); };
+  auto uval = [&](int r, int c) { return r <= c ? X[r + c * DN_LD] : zero; };
   for (int e = t; e < 64 * 64; e += 256) {
     const int i = e & 63, j = e >> 6;
     D[i + j * DN_LD] = (i < jb && j < jb) ? A[(size_t)(J + i) + (size_t)(J + j) * N] : (i == j ? one : zero);
@@ -557,7 +560,7 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
       const T xd = w < 4 ? one : rcps[o + l];    // diagonal entry of the inverse's column l
 #pragma unroll
       for (int r = 0; r < 16; ++r) x[r] = r == l ? xd : zero;
-      if (w < 4) {                                // unit lower: column l of the block inverse
+      if (w < 4) {                                // unit lower: column l of the block inverse, below l
 #pragma unroll
         for (int r = 1; r < 16; ++r) {
           if (r > l) {
@@ -569,8 +572,9 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
           }
         }
 #pragma unroll
-        for (int r = 0; r < 16; ++r) XL[(o + r) + (o + l) * DN_LD] = x[r];
-      } else {                                    // upper
+        for (int r = 0; r < 16; ++r)
+          if (r > l) X[(o + r) + (o + l) * DN_LD] = x[r];
+      } else {                                    // upper: column l, on and above the diagonal
 #pragma unroll
         for (int r = 14; r >= 0; --r) {
           if (r < l) {
@@ -582,42 +586,42 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
           }
         }
 #pragma unroll
-        for (int r = 0; r < 16; ++r) XU[(o + r) + (o + l) * DN_LD] = x[r];
+        for (int r = 0; r < 16; ++r)
+          if (r <= l) X[(o + r) + (o + l) * DN_LD] = x[r];
       }
     }
   }
   __syncthreads();
   for (int st = 1; st < 4; ++st) {
     const int bl = st, bu = 3 - st;               // block row of L^-1 / U^-1 filled in this round
-    for (int e = t; e < 512 * st; e += 256) {     // S = sum of block products
-      const int blk = e >> 8, r = e & 15, c = (e >> 4) & 15;
+    // L: S_bj = sum_{bk=bj}^{bl-1} L(bl,bk) L^-1(bk,bj), then L^-1(bl,bj) = -L^-1(bl,bl) S_bj
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = e >> 8, r = e & 15, c = (e >> 4) & 15;
       T s = zero;
-      if (blk < st) {                             // L: S_bj = sum_{bk=bj}^{bl-1} L(bl,bk) XL(bk,bj), bj = blk
-        const int bj = blk;
-        for (int m = 16 * bj; m < 16 * bl; ++m)
-          cfma(s, D[(16 * bl + r) + m * DN_LD], XL[m + (16 * bj + c) * DN_LD]);
-        S[blk * 256 + r + 16 * c] = s;
-      } else {                                    // U: S_bj = sum_{bk=bu+1}^{bj} U(bu,bk) XU(bk,bj)
-        const int bj = bu + 1 + (blk - st);
-        for (int m = 16 * (bu + 1); m < 16 * (bj + 1); ++m)
-          cfma(s, D[(16 * bu + r) + m * DN_LD], XU[m + (16 * bj + c) * DN_LD]);
-        S[(3 + blk - st) * 256 + r + 16 * c] = s;
-      }
+      for (int m = 16 * bj; m < 16 * bl; ++m) cfma(s, D[(16 * bl + r) + m * DN_LD], lval(m, 16 * bj + c));
+      S[bj * 256 + r + 16 * c] = s;
     }
     __syncthreads();
-    for (int e = t; e < 512 * st; e += 256) {     // X(bi,bj) = -X(bi,bi) S_bj
-      const int blk = e >> 8, r = e & 15, c = (e >> 4) & 15;
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = e >> 8, r = e & 15, c = (e >> 4) & 15;
       T s = zero;
-      if (blk < st) {
-        const int bj = blk;
-        for (int m = 0; m < 16; ++m) cfma(s, XL[(16 * bl + r) + (16 * bl + m) * DN_LD], S[blk * 256 + m + 16 * c]);
-        XL[(16 * bl + r) + (16 * bj + c) * DN_LD] = cneg(s);
-      } else {
-        const int bj = bu + 1 + (blk - st);
-        for (int m = 0; m < 16; ++m)
-          cfma(s, XU[(16 * bu + r) + (16 * bu + m) * DN_LD], S[(3 + blk - st) * 256 + m + 16 * c]);
-        XU[(16 * bu + r) + (16 * bj + c) * DN_LD] = cneg(s);
-      }
+      for (int m = 0; m < 16; ++m) cfma(s, lval(16 * bl + r, 16 * bl + m), S[bj * 256 + m + 16 * c]);
+      X[(16 * bl + r) + (16 * bj + c) * DN_LD] = cneg(s);
+    }
+    __syncthreads();
+    // U: S_bj = sum_{bk=bu+1}^{bj} U(bu,bk) U^-1(bk,bj), then U^-1(bu,bj) = -U^-1(bu,bu) S_bj
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = bu + 1 + (e >> 8), r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      for (int m = 16 * (bu + 1); m < 16 * (bj + 1); ++m) cfma(s, D[(16 * bu + r) + m * DN_LD], uval(m, 16 * bj + c));
+      S[(e >> 8) * 256 + r + 16 * c] = s;
+    }
+    __syncthreads();
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = bu + 1 + (e >> 8), r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      for (int m = 0; m < 16; ++m) cfma(s, uval(16 * bu + r, 16 * bu + m), S[(e >> 8) * 256 + m + 16 * c]);
+      X[(16 * bu + r) + (16 * bj + c) * DN_LD] = cneg(s);
     }
     __syncthreads();
   }
@@ -626,9 +630,8 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
     const int i = e % NB, k = e / NB;
     T lv = zero, uv = zero;
     if (i < jb && k < jb) {
-      if (i > k) lv = XL[i + k * DN_LD];
-      else if (i == k) lv = one;
-      if (i <= k) uv = XU[i + k * DN_LD];
+      lv = lval(i, k);
+      uv = uval(i, k);
     }
     Linv[off + e] = lv;
     Uinv[off + e] = uv;
@@ -1050,7 +1053,7 @@ static cudaError_t nopiv_step_kernels(z32 *M, const LUBatch &lb, int J, int jb, 
   typedef z32 T;
   const int nsteps = lb.nsteps();
   cudaError_t e;
-  const size_t sm_di = sizeof(T) * (3 * 64 * DN_LD + DI_SCR), sm_tt = sizeof(T) * 2 * 64 * DN_LD;
+  const size_t sm_di = sizeof(T) * (2 * 64 * DN_LD + DI_SCR), sm_tt = sizeof(T) * 2 * 64 * DN_LD;
   static bool attr_np = false;
   if (!attr_np) {
     cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_di);
