@@ -17,7 +17,7 @@ import pytest
 
 from adga_b200 import Ladder, synth
 from oracle import adga_oracle as O
-from tests.helpers import problem, qw_points, rel_err, to_inputs
+from tests.helpers import library_env, problem, qw_points, rel_err, to_inputs
 
 pytestmark = pytest.mark.gpu
 KEYS = ("chi_dens", "chi_magn", "sigma")
@@ -132,3 +132,14 @@ def test_c3_subgrid_tangents_match_oracle_dense_jacobian(precision):
         wchi, wsig = jac[par]
         assert rel_err(dchi, wchi) < 1e-6, (par, "chi_m", rel_err(dchi, wchi))
         assert rel_err(dsig, wsig) < 1e-6, (par, "sigma", rel_err(dsig, wsig))
+
+
+def test_mixed_tangents_of_points_resolved_in_fp64():
+    """ADGA_MAX_REFINE=1 leaves every mixed point unconverged: each is re-solved
+    in FP64 together with its tangents, which then equal the FP64 path's."""
+    p = problem("t3m")
+    _, t64 = gpu_tangent(p, "U", "fp64")
+    with library_env({"ADGA_MAX_REFINE": "1"}):
+        _, tmx = gpu_tangent(p, "U", "mixed")
+    for k in KEYS:
+        assert rel_err(tmx[k], t64[k]) < 1e-12, (k, rel_err(tmx[k], t64[k]))
