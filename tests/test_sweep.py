@@ -3,7 +3,6 @@ points: mixed ladder + gradients in U and J per point, the FP64 check pass,
 and one point against the oracle."""
 import dataclasses
 
-import numpy as np
 import pytest
 
 from adga_b200 import sweep, synth

@@ -9,7 +9,6 @@ at fixed DMFT one-particle inputs:
     reference: every output of the small grid);
 both to 1e-6 relative (finite-difference truncation ~h^2, rounding ~1e-11).
 """
-import dataclasses
 from functools import lru_cache
 
 import numpy as np
