@@ -11,7 +11,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 // tensor-core trailing update of the mixed path (k_tc.cu)
@@ -166,6 +169,20 @@ static bool alloc_into(adga_handle *h, P *&ptr, size_t count, std::vector<void *
 static void free_list(std::vector<void *> &list) {
   for (void *p : list) cudaFree(p);
   list.clear();
+}
+
+cudaError_t smem_limit_once(const void *kernel, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> done;   // (kernel, device) -> limit set
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find({kernel, dev});
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done[{kernel, dev}] = bytes;
+  return e;
 }
 
 extern "C" const char *adga_last_error(const adga_handle *h) {

@@ -78,6 +78,14 @@ ADGA_HD z64 up64(z32 a) { return to64(a); }
 
 static inline unsigned cdiv_u(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 
+// Raise a kernel's dynamic shared-memory limit on the current device, once per
+// (kernel, device): the attribute belongs to the device's context, so a
+// process that drives several GPUs sets it on each of them.  Thread-safe.
+cudaError_t smem_limit_once(const void *kernel, int bytes);
+template <typename K> inline cudaError_t smem_limit(K *kernel, int bytes) {
+  return smem_limit_once((const void *)kernel, bytes);
+}
+
 // Host-side launch check used after every kernel launch: counts the launch
 // (reported in adga_run_stats.kernel_launches) and returns cudaError_t.
 #include <atomic>

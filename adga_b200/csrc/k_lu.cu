@@ -985,14 +985,10 @@ static cudaError_t launch_panel(T *M, const LUBatch &lb, int J, int jb, cudaStre
   const int rows = lb.N - J;
   auto nthreads = [&](int rpt) { int n = ((rows + rpt - 1) / rpt + 31) / 32 * 32; return n < 32 ? 32 : n; };
   const size_t dyn = sizeof(T) * (size_t)MAXNB * 2 * SWD;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_panel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_panel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_panel<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_panel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    attr = true;
-  }
+  smem_limit(k_panel<T, 1>, 96 * 1024);
+  smem_limit(k_panel<T, 2>, 96 * 1024);
+  smem_limit(k_panel<T, 4>, 96 * 1024);
+  smem_limit(k_panel<T, 8>, 96 * 1024);
   // fewer, fuller threads per CTA: more matrices resident per SM and cheaper
   // block-wide pivot reductions (FP32 rows cost half the registers of FP64)
   const bool f32 = sizeof(T) == sizeof(z32);
@@ -1054,13 +1050,9 @@ static cudaError_t nopiv_step_kernels(z32 *M, const LUBatch &lb, int J, int jb, 
   const int nsteps = lb.nsteps();
   cudaError_t e;
   const size_t sm_di = sizeof(T) * (2 * 64 * DN_LD + DI_SCR), sm_tt = sizeof(T) * 2 * 64 * DN_LD;
-  static bool attr_np = false;
-  if (!attr_np) {
-    cudaFuncSetAttribute(k_diag_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_di);
-    cudaFuncSetAttribute(k_tri_tile<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
-    cudaFuncSetAttribute(k_tri_tile<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tt);
-    attr_np = true;
-  }
+  smem_limit(k_diag_inv<T>, (int)sm_di);
+  smem_limit(k_tri_tile<T, true>, (int)sm_tt);
+  smem_limit(k_tri_tile<T, false>, (int)sm_tt);
   k_diag_inv<T><<<lb.batch, 256, sm_di, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps, (T *)lb.Linv,
                                               (T *)lb.Uinv, lb.ipiv, lb.rmap);
   if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
@@ -1119,13 +1111,8 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
   cudaError_t e;
   const size_t sm_tri = sizeof(T) * ((size_t)lb.NB * lb.NB + lb.NB);
   const size_t sm_trsm = sizeof(typename TrsmOp<T>::L) * 64 * 64 + sizeof(typename TrsmOp<T>::X) * TW * TS_LD;
-  static bool attr_done[2] = {false, false};
-  const int ti = sizeof(T) == sizeof(z64) ? 0 : 1;
-  if (!attr_done[ti]) {
-    cudaFuncSetAttribute(k_triinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_swap_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done[ti] = true;
-  }
+  smem_limit(k_triinv<T>, 200 * 1024);
+  smem_limit(k_swap_trsm<T>, 200 * 1024);
   const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
   if constexpr (sizeof(T) == sizeof(z32)) {
     if (nopiv) {
@@ -1177,17 +1164,10 @@ static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC,
     sm_small = stage_d + dbytes;
   }
   if (R <= 25 && sm_small <= 200 * 1024) {
-    static bool attr_small[16] = {false};
-    const int ti = (sizeof(T) == sizeof(z64) ? 0 : 1) * 8 + (upper ? 4 : 0) +
-                   (R == 9 ? 0 : R <= 4 ? 1 : R <= 16 ? 2 : 3);
     const int np = lb.nsteps();
 #define TS_LAUNCH(UP, RM)                                                                            \
     do {                                                                                             \
-      if (!attr_small[ti]) {                                                                         \
-        cudaFuncSetAttribute(k_trisolve_smem<T, UP, RM, 1>,                                          \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);               \
-        attr_small[ti] = true;                                                                       \
-      }                                                                                              \
+      smem_limit(k_trisolve_smem<T, UP, RM, 1>, 200 * 1024);                                         \
       k_trisolve_smem<T, UP, RM, 1><<<lb.batch, 512, sm_small, st>>>(                                \
           M, lb.strideM, lb.N, lb.NB, np, (const T *)(UP ? lb.Uinv : lb.Linv), C, strideC, ldc, R,   \
           lb.ipiv, stage_d);                                                                         \
@@ -1204,15 +1184,10 @@ static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC,
   }
   const int nph = 256 / lb.NB;
   size_t sm = sizeof(T) * ((size_t)nph * lb.NB * RT + (size_t)lb.NB * RT) + sizeof(int) * lb.N;
-  static bool attr_done[4] = {false, false, false, false};
-  const int ti = (sizeof(T) == sizeof(z64) ? 0 : 1) * 2 + (upper ? 1 : 0);
-  if (!attr_done[ti]) {
-    if (upper)
-      cudaFuncSetAttribute(k_trisolve<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    else
-      cudaFuncSetAttribute(k_trisolve<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done[ti] = true;
-  }
+  if (upper)
+    smem_limit(k_trisolve<T, true>, 200 * 1024);
+  else
+    smem_limit(k_trisolve<T, false>, 200 * 1024);
   if (!upper && !work) return cudaErrorInvalidValue;
   dim3 g(cdiv_u(R, RT), lb.batch);
   if (upper)

@@ -66,11 +66,7 @@ k_tan_rhs(int N, int R, int npts, int ch, const z64 *__restrict__ XS, const z64 
 
 cudaError_t launch_tan_rhs(const DevCtx &c, int npts, int ch, const z64 *XS, const z64 *Frow, const z64 *XD,
                            const z64 *Fdot, const z64 *dB, z64 *out, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_tan_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+  smem_limit(k_tan_rhs, SMEM_BYTES);
   dim3 g(cdiv_u(c.N, BN), cdiv_u((size_t)npts * c.R, BM));
   k_tan_rhs<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, ch, XS, Frow, XD, Fdot, dB, out);
   return ADGA_LAUNCH_CHECK();

@@ -361,12 +361,7 @@ cudaError_t launch_trsv_stream(const T *M, const LUBatch &lb, T *C, size_t strid
 #define TSV(UP, RGV, NGV, STG)                                                                     \
   do {                                                                                             \
     const size_t sm = ts_smem<T>(R, RGV * NGV, STG);                                                          \
-    static bool attr = false;                                                                      \
-    if (!attr) {                                                                                   \
-      cudaFuncSetAttribute(k_trsv_stream<T, UP, RGV, NGV, STG>,                                    \
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);               \
-      attr = true;                                                                                 \
-    }                                                                                              \
+    smem_limit(k_trsv_stream<T, UP, RGV, NGV, STG>, 227 * 1024);                                   \
     k_trsv_stream<T, UP, RGV, NGV, STG><<<lb.batch, 128 * NGV, sm, st>>>(                          \
         M, lb.strideM, lb.N, np, D, C, strideC, ldc, R, perm, work);                               \
   } while (0)

@@ -45,11 +45,7 @@ k_trail_z64(z64 *M, size_t strideM, int N, int ncols, int J, int jb) {
 cudaError_t lu_trail_z64(z64 *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
   const int m = lb.N - J - jb, n = lb.ncols - J - jb;
   if (m <= 0 || n <= 0) return cudaSuccess;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_trail_z64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+  smem_limit(k_trail_z64, SMEM_BYTES);
   dim3 grid(cdiv_u(n, BN), cdiv_u(m, BM), lb.batch);
   k_trail_z64<<<grid, NT, SMEM_BYTES, st>>>(M, lb.strideM, lb.N, lb.ncols, J, jb);
   return ADGA_LAUNCH_CHECK();
@@ -108,11 +104,7 @@ cudaError_t launch_resid_z64(const DevCtx &c, int npts, const z64 *XD, const z64
                              const z64 *Frow_d, const z64 *Frow_m, const z64 *opg_d,
                              const z64 *opg_m, z32 *V, const z64 *extra_d, unsigned long long *rnorm,
                              const z64 *Bpt, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_resid_z64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    attr = true;
-  }
+  smem_limit(k_resid_z64, SMEM_BYTES);
   dim3 g(cdiv_u(c.N, BN), cdiv_u((size_t)npts * c.R, BM));
   k_resid_z64<<<g, NT, SMEM_BYTES, st>>>(c.N, c.R, npts, 0, XD, X, Frow_d, opg_d, V, extra_d, rnorm, Bpt);
   cudaError_t e = ADGA_LAUNCH_CHECK();

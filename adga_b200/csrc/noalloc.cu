@@ -98,12 +98,12 @@ extern "C" int adga_inverse_matrix_z_noalloc(const adga_z *M_dev, adga_z *Minv_d
   if (e == cudaSuccess) e = lu_backsolve<z64>(T, lb, T + (size_t)n * n, strideM, n, n, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(Minv_dev, T + (size_t)n * n, sizeof(z64) * n * n, cudaMemcpyDeviceToDevice, st);
+  // the info is always read back (the call waits for the stream), so the
+  // return value reports a singular matrix whether or not ierr is given
   int hinfo = 0;
-  if (e == cudaSuccess && ierr) {
-    e = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    *ierr = hinfo;
-  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return ADGA_ECUDA;
+  if (ierr) *ierr = hinfo;
   return hinfo > 0 ? hinfo : 0;
 }

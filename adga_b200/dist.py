@@ -12,6 +12,7 @@ the CPU tests.  Complex arrays travel as real views.
 """
 from __future__ import annotations
 
+import os
 from typing import Dict, Tuple
 
 import numpy as np
@@ -79,16 +80,38 @@ def reduce_outputs(out: Dict[str, np.ndarray], nqw: int, group=None, device=None
     return res
 
 
-def run_ladder_distributed(prob, precision="fp64", group=None):
-    """Each rank runs its block of the full loop on its GPU, then the results
-    are combined; returns the assembled outputs on every rank."""
+def rank_device(group=None):
+    """The device the collectives of this rank use: under NCCL the rank's own
+    GPU (LOCAL_RANK, else rank modulo the visible GPUs), made current for the
+    calling thread so that the library's handle lives there too; None (host
+    tensors) under gloo."""
+    import torch
     import torch.distributed as dist
-    from .ladder import Ladder
+    if dist.get_backend(group) != "nccl":
+        return None
+    ngpu = torch.cuda.device_count()
+    local = int(os.environ.get("LOCAL_RANK", dist.get_rank(group) % max(ngpu, 1)))
+    torch.cuda.set_device(local)
+    return torch.device("cuda", local)
+
+
+def run_ladder_distributed(prob, precision="fp64", group=None, ladder_factory=None):
+    """Each rank runs its block of the full loop on its GPU, then the results
+    are combined; returns (assembled outputs, status, stats) on every rank.
+
+    ladder_factory(prob) makes the rank's ladder (default
+    ``Ladder.from_problem``); it is called after the rank's GPU is made
+    current."""
+    import torch.distributed as dist
     s = prob.spec
     nqw = s.nqp * (2 * s.iwb + 1)
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     qs, qe = distribute(nqw, world, rank)
-    lad = Ladder.from_problem(prob)
+    device = rank_device(group)
+    if ladder_factory is None:
+        from .ladder import Ladder
+        ladder_factory = Ladder.from_problem
+    lad = ladder_factory(prob)
     try:
         for iwb in sorted({-s.iwb + (i - 1) // s.nqp for i in range(qs, qe + 1)}):
             lad.set_vertex(iwb, *prob.vertex(iwb))
@@ -96,5 +119,25 @@ def run_ladder_distributed(prob, precision="fp64", group=None):
         out = lad.get_outputs()
     finally:
         lad.close()
-    full = reduce_outputs(out, nqw, group)
+    full = reduce_outputs(out, nqw, group, device=device)
+    full.update(assemble_outputs(full, prob, nqw))
     return full, status, stats
+
+
+def assemble_outputs(full, prob, nqw):
+    """chi(q, w) = chi_nl + bubble_nl + chi_loc(w) (chi_loc += bubble_loc) and
+    Sigma = Sigma_nl + siw on the diagonal for the whole loop
+    (src/main.F90:935-936,1050-1063,1127-1140; add_siw_dmft,
+    src/eom_module.f90:237-251)."""
+    s = prob.spec
+    widx = np.arange(nqw) // s.nqp
+    cld = full["chi_loc_dens"] + full["bubble_loc"]
+    clm = full["chi_loc_magn"] + full["bubble_loc"]
+    res = {"chi_dens": full["chi_qw_dens"] + full["bubble_nl"] + cld[:, :, widx],
+           "chi_magn": full["chi_qw_magn"] + full["bubble_nl"] + clm[:, :, widx]}
+    sig = full["sigma_nl"].copy(order="F")
+    nu = np.arange(-s.iwf, s.iwf) + prob.iwmax
+    for b in range(s.ndim):
+        sig[b, b] += np.asarray(prob.siw)[nu, b][:, None]
+    res["sigma"] = sig
+    return res

@@ -32,7 +32,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "BSE q·ω pts/s at 1e-8 rel err vs FP64 oracle: mixed-prec vs plain FP64 on B200"
 # DRAM bytes / algorithmic bytes of the k_tc_persist launches of one step pair
 # (two narrow K = 64 regions and one wide K = 128 region) measured with ncu on the
-# 160-point t2g case, 320 matrices; profiles/k_tc_persist_t2g.md
+# 160-point t2g case, 320 matrices
 TRAFFIC_OVER_ALG = 1.27
 UNIT = "qw_points/s"
 WORKLOAD = "c1"
@@ -425,7 +425,7 @@ def main():
     # the measured copy bandwidth with algorithmic bytes (C read + write, L21
     # and U12 read once per launch region); `traffic` scales them by the DRAM /
     # algorithmic ratio ncu measured on the launches of one step pair:
-    # TRAFFIC_OVER_ALG (see profiles/).
+    # TRAFFIC_OVER_ALG.
     pk, pk_kind = peaks()
     gflop = sum(s["trail_gflop"] for s in st_mixed)
     gbytes = sum(s["trail_gbytes"] for s in st_mixed)

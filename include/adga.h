@@ -311,8 +311,9 @@ int adga_inverse_matrix_z(adga_z *M, int n, int *ierr, char *erstr);
  * ADGA_EINVAL.  The first call on a device looks up that array's address
  * (cudaGetSymbolAddress): make it before any stream capture.  Calls share
  * the array, so calls that overlap on the GPU race.  stream may be NULL (the
- * default stream); when ierr is non-NULL the call waits for the stream and
- * stores the LAPACK-style info.  No counterpart in the reference. */
+ * default stream); the call waits for the stream and returns the LAPACK-style
+ * info (> 0: exactly zero pivot, the inverse is then not usable), also stored
+ * in *ierr when ierr is non-NULL.  No counterpart in the reference. */
 #define ADGA_NOALLOC_MAX_N 256
 int adga_inverse_matrix_z_noalloc(const adga_z *M_dev, adga_z *Minv_dev, int n, int *ierr,
                                   void *stream);
