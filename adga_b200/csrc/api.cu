@@ -88,6 +88,9 @@ struct adga_handle {
   z64 *sigma_nl = nullptr, *sigma_dmft = nullptr, *sigma_hf = nullptr;
   z64 *chi_qw_d = nullptr, *chi_qw_m = nullptr, *bubble_nl = nullptr;
   int out_cap = 0, last_npts = 0;
+  // first per-point output slot past the run's points: the FP64 re-solve of
+  // mixed points that did not converge writes there, then moves them to their slots
+  int fb_base = 0;
   // batch work buffers (sized on demand)
   int cap = 0, cap_prec = -1;
   std::vector<void *> work;
@@ -1117,6 +1120,24 @@ static int tan_local_update(adga_handle *h, int d, int iwb, bool do_chi, bool do
   return 0;
 }
 
+// per-point outputs (and their tangents) of slot src copied to slot dst
+static int move_point_outputs(adga_handle *h, int src, int dst, z64 *chi_d, z64 *chi_m, z64 *bub, bool do_chi) {
+  const size_t n = h->nd4, b = sizeof(z64) * n;
+  cudaStream_t st = h->st;
+  CK(cudaMemcpyAsync(chi_d + dst * n, chi_d + src * n, b, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(chi_m + dst * n, chi_m + src * n, b, cudaMemcpyDeviceToDevice, st));
+  if (bub) CK(cudaMemcpyAsync(bub + dst * n, bub + src * n, b, cudaMemcpyDeviceToDevice, st));
+  if (h->tan_on && do_chi)      // tangent per-point outputs exist only with do_chi (bubble: with dH)
+    for (TanState *t : h->tan)
+      if (t) {
+        CK(cudaMemcpyAsync(t->chi_qw_d + dst * n, t->chi_qw_d + src * n, b, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(t->chi_qw_m + dst * n, t->chi_qw_m + src * n, b, cudaMemcpyDeviceToDevice, st));
+        if (t->has_dhk)
+          CK(cudaMemcpyAsync(t->bub_nl + dst * n, t->bub_nl + src * n, b, cudaMemcpyDeviceToDevice, st));
+      }
+  return 0;
+}
+
 static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *status,
                      z64 *chi_qw_d, z64 *chi_qw_m, z64 *bub_nl, bool do_eom, bool do_chi) {
   DevCtx &c = h->c;
@@ -1291,19 +1312,32 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
     if (!(worst <= h->stats.max_refine_resid)) h->stats.max_refine_resid = worst;
   }
   if (mixed_fail) {
-    // FP64 re-solve of the points whose refinement did not converge
+    // FP64 re-solve of the points whose refinement did not converge, as batches:
+    // their per-point outputs (and tangents) go to the scratch slots from
+    // h->fb_base on, then move to their own slots.  status: -1 (re-solved), or
+    // the FP64 LU's LAPACK-style info where it met an exactly zero pivot.
     std::vector<int> q(np);
     for (int p = 0; p < np; ++p) q[p] = h->qidx_h[p];
     const int mixed_cap = h->cap;
     h->stats.mixed_fallbacks += mixed_fail;
-    int saved_points = h->stats.points;
-    for (int p : fallback) {
-      int r = ensure_work(h, ADGA_FP64, 1);
+    const int saved_points = h->stats.points;
+    const int base = h->fb_base;
+    for (size_t f0 = 0; f0 < fallback.size();) {
+      const int left = (int)(fallback.size() - f0);
+      int r = ensure_work(h, ADGA_FP64, left);
       if (r) return r;
-      h->qidx_h[0] = q[p];
-      r = run_batch(h, iwb, 1, off + p, ADGA_FP64, nullptr, chi_qw_d, chi_qw_m, bub_nl, do_eom, do_chi);
+      const int nb = std::min(h->cap, left);
+      for (int i = 0; i < nb; ++i) h->qidx_h[i] = q[fallback[f0 + i]];
+      std::vector<int> st64((size_t)base + nb, 0);
+      r = run_batch(h, iwb, nb, base, ADGA_FP64, st64.data(), chi_qw_d, chi_qw_m, bub_nl, do_eom, do_chi);
       if (r) return r;
-      if (status) status[off + p] = -1;
+      for (int i = 0; i < nb; ++i) {
+        const int slot = off + fallback[f0 + i];
+        r = move_point_outputs(h, base + i, slot, chi_qw_d, chi_qw_m, do_chi ? bub_nl : nullptr, do_chi);
+        if (r) return r;
+        if (status) status[slot] = st64[base + i] > 0 ? st64[base + i] : -1;
+      }
+      f0 += nb;
     }
     h->stats.points = saved_points;
     int r = ensure_work(h, ADGA_MIXED, mixed_cap);
@@ -1312,15 +1346,33 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   return 0;
 }
 
+// outputs of a run with npts points: the points plus as many scratch slots as a
+// batch can hold (the FP64 re-solve of unconverged mixed points writes there)
+static int out_slots(const adga_handle *h, int npts) { return npts + std::min(npts, h->c.nqp); }
+
+static void free_owned(adga_handle *h, void *p) {
+  if (!p) return;
+  auto it = std::find(h->owned.begin(), h->owned.end(), p);
+  if (it != h->owned.end()) h->owned.erase(it);
+  cudaFree(p);
+}
+
 static int ensure_outputs(adga_handle *h, int npts) {
-  if (h->out_cap >= npts) return 0;
+  const int want = out_slots(h, npts);
+  if (h->out_cap >= want) return 0;
+  // superseded buffers of earlier (smaller) runs are freed
+  cudaStreamSynchronize(h->st);
+  free_owned(h, h->chi_qw_d);
+  free_owned(h, h->chi_qw_m);
+  free_owned(h, h->bubble_nl);
+  h->chi_qw_d = h->chi_qw_m = h->bubble_nl = nullptr;
+  h->out_cap = 0;
   auto &L = h->owned;
-  // outputs of earlier runs are replaced; the old buffers stay owned until destroy
-  if (!alloc_into(h, h->chi_qw_d, (size_t)npts * h->nd4, L) ||
-      !alloc_into(h, h->chi_qw_m, (size_t)npts * h->nd4, L) ||
-      !alloc_into(h, h->bubble_nl, (size_t)npts * h->nd4, L))
+  if (!alloc_into(h, h->chi_qw_d, (size_t)want * h->nd4, L) ||
+      !alloc_into(h, h->chi_qw_m, (size_t)want * h->nd4, L) ||
+      !alloc_into(h, h->bubble_nl, (size_t)want * h->nd4, L))
     return fail(h, ADGA_ENOMEM, "per-point outputs");
-  h->out_cap = npts;
+  h->out_cap = want;
   return 0;
 }
 
@@ -1335,6 +1387,7 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   const int npts = qwstop - qwstart + 1;
   int r = ensure_outputs(h, npts);
   if (r) return r;
+  h->fb_base = npts;
   memset(&h->stats, 0, sizeof(h->stats));
   const long long launches0 = g_adga_launches.load();
   CK(cudaMemsetAsync(h->chi_qw_d, 0, sizeof(z64) * npts * h->nd4, h->st));
@@ -1403,15 +1456,17 @@ extern "C" int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, 
   const int npts = qwstop - qwstart + 1;
   for (TanState *t : h->tan) {
     if (!t) continue;
-    if (t->out_cap < npts) {
+    const int want = out_slots(h, npts);
+    if (t->out_cap < want) {
+      cudaStreamSynchronize(h->st);
       for (z64 *p : {t->chi_qw_d, t->chi_qw_m, t->bub_nl}) if (p) cudaFree(p);
       t->chi_qw_d = t->chi_qw_m = t->bub_nl = nullptr;
       t->out_cap = 0;
-      if (cudaMalloc(&t->chi_qw_d, sizeof(z64) * npts * h->nd4) != cudaSuccess ||
-          cudaMalloc(&t->chi_qw_m, sizeof(z64) * npts * h->nd4) != cudaSuccess ||
-          cudaMalloc(&t->bub_nl, sizeof(z64) * npts * h->nd4) != cudaSuccess)
+      if (cudaMalloc(&t->chi_qw_d, sizeof(z64) * want * h->nd4) != cudaSuccess ||
+          cudaMalloc(&t->chi_qw_m, sizeof(z64) * want * h->nd4) != cudaSuccess ||
+          cudaMalloc(&t->bub_nl, sizeof(z64) * want * h->nd4) != cudaSuccess)
         return fail(h, ADGA_ENOMEM, "tangent per-point outputs");
-      t->out_cap = npts;
+      t->out_cap = want;
     }
     CK(cudaMemsetAsync(t->chi_qw_d, 0, sizeof(z64) * npts * h->nd4, h->st));
     CK(cudaMemsetAsync(t->chi_qw_m, 0, sizeof(z64) * npts * h->nd4, h->st));
@@ -1600,11 +1655,21 @@ extern "C" int adga_bse_point(adga_handle *h, int iq, int iwb, int precision, ad
   if (r) return r;
   z64 *scr = nullptr;
   std::vector<void *> tmp;
-  if (!alloc_into(h, scr, (size_t)3 * h->nd4, tmp)) return fail(h, ADGA_ENOMEM, "scratch");
+  // per-point outputs: the point's slot and one scratch slot for a re-solve
+  if (!alloc_into(h, scr, (size_t)6 * h->nd4, tmp)) return fail(h, ADGA_ENOMEM, "scratch");
   h->qidx_h[0] = iq - 1;
-  int st_info = 0;
+  int st_info[2] = {0, 0};
   memset(&h->stats, 0, sizeof(h->stats));
-  r = run_batch(h, iwb, 1, 0, precision, &st_info, scr, scr + h->nd4, scr + 2 * h->nd4, false, true);
+  h->fb_base = 1;
+  r = run_batch(h, iwb, 1, 0, precision, st_info, scr, scr + 2 * h->nd4, scr + 4 * h->nd4, false, true);
+  if (!r && h->stats.mixed_fallbacks) {
+    // the mixed refinement did not converge: eta and gamma^q_d from the FP64 path
+    r = ensure_work(h, ADGA_FP64, 1);
+    if (!r) {
+      h->qidx_h[0] = iq - 1;
+      r = run_batch(h, iwb, 1, 0, ADGA_FP64, st_info, scr, scr + 2 * h->nd4, scr + 4 * h->nd4, false, true);
+    }
+  }
   if (!r) {
     const size_t n = (size_t)c.nd2 * c.N;
     if (etaqd) cudaMemcpyAsync(etaqd, h->etad, sizeof(z64) * n, cudaMemcpyDeviceToHost, h->st);
@@ -1613,7 +1678,7 @@ extern "C" int adga_bse_point(adga_handle *h, int iq, int iwb, int precision, ad
     if (cudaStreamSynchronize(h->st) != cudaSuccess) r = fail(h, ADGA_ECUDA, "copy-out");
   }
   free_list(tmp);
-  if (lu_info) *lu_info = st_info;
+  if (lu_info) *lu_info = st_info[0];
   return r;
 }
 

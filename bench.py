@@ -7,8 +7,10 @@ One step = one bosonic slice: the full (q, omega) loop body for all 1000 q
 points of one omega (chi0 bubble, both BSE channels, chi sums, EOM).
 `value` is the mixed-precision path (FP32 LU with BF16x3 tensor-core updates
 and FP64 refinement); the plain FP64 GPU path is timed on the same steps and
-reported beside it, with the relative error between the two and against the
-FP64 oracle on sampled points.
+reported beside it, with the relative error between the two, and both are
+checked against the FP64 oracle over the whole omega = 0 slice (chi_d/m(q, w)
+of every point and Sigma(k, nu) accumulated over the slice), the oracle
+running on the host cores.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -50,6 +52,9 @@ def parse():
                     help="skip the gradient arm (ladder + tangents in U, J, t, mixed and FP64)")
     ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the oracle run over the whole omega = 0 slice (errors of both GPU arms "
+                         "against the FP64 oracle for chi_d/m(q, omega) and Sigma(k, nu))")
     ap.add_argument("--full-grid", action="store_true",
                     help="also run every omega slice (the whole q x omega grid) in both precisions and "
                          "report the errors of chi_d/m(q, omega) and of the accumulated Sigma(k, nu)")
@@ -97,6 +102,21 @@ def _cpu_point(iq):
     return time.perf_counter() - t, res["chi_qw_dens"], res["chi_qw_magn"]
 
 
+# raw accumulators of the reference loop that the parity check compares
+ORACLE_KEYS = ("chi_qw_dens", "chi_qw_magn", "bubble_nl", "bubble_loc", "chi_loc_dens", "chi_loc_magn",
+               "sigma_nl", "sigma_dmft", "sigma_hf")
+
+
+def _cpu_block(rng_iq):
+    """The reference loop (src/main.F90:486-799) over the contiguous q block
+    [a, b) of the worker's omega slice, local terms included where the block
+    holds iq = 0: its raw accumulators."""
+    o, iwb = _W["o"], _W["iwb"]
+    a, b = rng_iq
+    out = o.run([(iwb, iq) for iq in range(a, b)])
+    return a, b, {k: out[k] for k in ORACLE_KEYS}
+
+
 class CpuPool:
     def __init__(self, workload, iwb, nproc):
         import multiprocessing as mp
@@ -108,6 +128,30 @@ class CpuPool:
         t = time.perf_counter()
         res = self.pool.map(_cpu_point, iqs, chunksize=1)
         return time.perf_counter() - t, res
+
+    def slice_async(self, npts):
+        """Start the oracle over q = 0..npts-1 of the slice, one contiguous block
+        per worker; returns the async iterator of the blocks."""
+        cuts = [round(i * npts / self.n) for i in range(self.n + 1)]
+        blocks = [(a, b) for a, b in zip(cuts, cuts[1:]) if b > a]
+        return self.pool.imap_unordered(_cpu_block, blocks)
+
+    @staticmethod
+    def gather_slice(it, npts):
+        """Sum the blocks' accumulators and place their per-point outputs."""
+        import numpy as np
+        tot = None
+        for a, b, out in it:
+            if tot is None:
+                tot = {k: (np.zeros(v.shape[:-1] + (npts,), complex, order="F")
+                           if k in ("chi_qw_dens", "chi_qw_magn", "bubble_nl") else np.zeros_like(v))
+                       for k, v in out.items()}
+            for k, v in out.items():
+                if k in ("chi_qw_dens", "chi_qw_magn", "bubble_nl"):
+                    tot[k][..., a:b] = v
+                else:
+                    tot[k] += v
+        return tot
 
     def close(self):
         self.pool.terminate()
@@ -157,6 +201,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
@@ -190,7 +244,8 @@ def run_reference(args, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)",
             "data": "synthetic",
             "config": config(args, spec),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                             "cpu_model": cpu_model()},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -401,24 +456,52 @@ def main():
     e2e = {"value": world * npts * args.steps / e2e_t, "unit": UNIT,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
-    # CPU baseline + oracle check on sampled points (rank 0)
+    # CPU baseline (rank 0): the oracle timed on one random point per host core
     cpu_line = None
     if cpu is not None:
         rng = np.random.default_rng(1)
         iqs = [int(x) for x in rng.integers(0, npts, cpu.n)]
-        dt, pts = cpu.step(iqs)
-        cpu.close()
+        dt, _ = cpu.step(iqs)
         cpu_line = {"value": len(iqs) / dt, "unit": UNIT, "cores": cpu.n, "kind": "port",
+                    "cpu_model": cpu_model(),
                     "sample": f"{len(iqs)} random q points of the {args.workload} omega=0 slice, one per "
                               f"process (single-threaded OpenBLAS), FP64 oracle port"}
-        lad.reset_outputs()
-        lad.ladder_run(*slice_range(0), "mixed")
-        om = lad.get_outputs()
-        q0 = slice_range(0)[0]
-        errs = []
-        for iq, (_, cd, cm) in zip(iqs, pts):
-            errs.append(max(rel(om["chi_qw_dens"][:, :, iq], cd), rel(om["chi_qw_magn"][:, :, iq], cm)))
-        acc["mixed_vs_oracle_chi_nl_sampled"] = max(errs)
+
+    # parity at the workload's size (rank 0): the oracle over the whole omega = 0
+    # slice on the host cores, against both GPU arms on the same slice -- chi_d/m(q, w)
+    # of every point and Sigma(k, nu) accumulated over the slice
+    if cpu is not None and not args.no_parity:
+        t_or = time.perf_counter()
+        job = cpu.slice_async(npts)
+        gpu_out = {}
+        for prec in ("fp64", "mixed"):
+            lad.reset_outputs()
+            _, stp = lad.ladder_run(*slice_range(0), prec)
+            o = lad.get_outputs()
+            gpu_out[prec] = (o, lad.assemble(o, p.siw), stp)
+        ref = CpuPool.gather_slice(job, npts)
+        t_or = time.perf_counter() - t_or
+        from oracle.adga_oracle import LadderInputs, assemble as oracle_assemble
+        inp = LadderInputs(ndim=spec.ndim, nk=spec.nk, nq=spec.nq, iwmax=p.iwmax, iwfmax_small=spec.iwf,
+                           iwbmax_small=spec.iwb, beta=p.beta, mu=p.mu, hk=p.hk, siw=p.siw, giw=p.giw,
+                           dc=p.dc, u=p.u, u_tilde=p.u_tilde, n_dmft=p.n_dmft, vertex=p.vertex,
+                           iw_data=p.iw_data)
+        ref["qw"] = np.array([(0, iq) for iq in range(npts)], dtype=np.int64)
+        want = oracle_assemble(inp, ref)
+        want.update({k: ref[k] for k in ("chi_qw_dens", "chi_qw_magn", "sigma_nl", "sigma_dmft")})
+        keys = ("chi_dens", "chi_magn", "chi_qw_dens", "chi_qw_magn", "sigma", "sigma_nl", "sigma_dmft")
+        for prec, (o, a, stp) in gpu_out.items():
+            got = dict(a)
+            got.update({k: o[k] for k in ("chi_qw_dens", "chi_qw_magn", "sigma_nl", "sigma_dmft")})
+            acc[f"{prec}_vs_oracle"] = {k: rel(got[k], want[k]) for k in keys}
+            acc[f"{prec}_vs_oracle"]["fallbacks"] = stp["mixed_fallbacks"]
+        acc["oracle_slice"] = {"points": npts, "omega": 0, "oracle_s": t_or, "workers": cpu.n,
+                               "what": "normwise max relative error against the FP64 oracle over the "
+                                       "whole slice; sigma = Sigma_nl + siw, sigma_nl the non-local "
+                                       "part accumulated over the slice's points"}
+        p.clear_vertex_cache()
+    if cpu is not None:
+        cpu.close()
 
     # roofline of the dominant kernel: the LU trailing update (tensor cores).
     # Its C read-modify-write makes it HBM-bound, so it is reported against

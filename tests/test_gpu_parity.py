@@ -5,6 +5,7 @@ Tolerances (normwise max-abs relative error against the oracle):
   mixed path <= 1e-8    (FP32/BF16x3 LU + FP64 refinement)
 """
 import dataclasses
+from functools import lru_cache
 
 import numpy as np
 import pytest
@@ -53,6 +54,25 @@ def test_c0_slice_matches_oracle(prec):
     got = run_ladder(p, prec, qwstart=qs, qwstop=qe)
     want = oracle_run(p, qwstart=qs, qwstop=qe)
     compare(got, want, TOL[prec])
+
+
+@lru_cache(maxsize=None)
+def _c0_full_grid_oracle():
+    return oracle_run(problem("c0"))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_c0_full_grid_matches_oracle(prec):
+    """The whole single-orbital simple-cubic workload: 125 q x 21 omega =
+    2625 points (BSE N = 40), every output against the oracle, the mixed
+    path without FP64 re-solves."""
+    p = problem("c0")
+    got = run_ladder(p, prec)
+    want = _c0_full_grid_oracle()
+    assert got["status"].shape == (2625,) and np.all(got["status"] == 0)
+    compare(got, want, TOL[prec])
+    if prec == "mixed":
+        assert got["stats"]["mixed_fallbacks"] == 0
 
 
 def test_partial_range_starting_mid_omega():
