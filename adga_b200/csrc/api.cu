@@ -22,8 +22,9 @@ cudaError_t tc_trail_setup(void **ctx, z32 *M, const LUBatch &lb, cudaStream_t s
 cudaError_t tc_trail_run_range(void *ctx, int first, int count, int J, int jb, cudaStream_t st,
                                cudaEvent_t ev0, cudaEvent_t ev1);
 
-// a matrix range of the tensor-core trailing-update context
-struct TcRange { void *ctx; int first, count; };
+// a matrix range of the tensor-core trailing-update context; staged: the step
+// kernels (tc_tri_step) write the operand staging, the updates only run the GEMMs
+struct TcRange { void *ctx; int first, count; bool staged = false; };
 static cudaError_t tc_trail_range_fn(void *r, int J, int jb, cudaStream_t st, cudaEvent_t ev0,
                                      cudaEvent_t ev1) {
   TcRange *x = (TcRange *)r;
@@ -34,18 +35,23 @@ int tc_available();
 int tc_trail_error(void *ctx);
 int tc_pair_supported(void *ctx);
 cudaError_t tc_pair_narrow(void *ctx, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                           cudaEvent_t ev0, cudaEvent_t ev1);
+                           cudaEvent_t ev0, cudaEvent_t ev1, bool staged);
 cudaError_t tc_pair_wide(void *ctx, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                         cudaEvent_t ev0, cudaEvent_t ev1);
+                         cudaEvent_t ev0, cudaEvent_t ev1, bool staged);
+cudaError_t tc_tri_step(void *ctx, int first, int count, int J, int jb, int set, cudaStream_t st);
 static cudaError_t tc_pair_narrow_fn(void *r, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0,
                                      cudaEvent_t ev1) {
   TcRange *x = (TcRange *)r;
-  return tc_pair_narrow(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1);
+  return tc_pair_narrow(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1, x->staged);
 }
 static cudaError_t tc_pair_wide_fn(void *r, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0,
                                    cudaEvent_t ev1) {
   TcRange *x = (TcRange *)r;
-  return tc_pair_wide(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1);
+  return tc_pair_wide(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1, x->staged);
+}
+static cudaError_t tc_tri_fn(void *r, int J, int jb, int set, cudaStream_t st) {
+  TcRange *x = (TcRange *)r;
+  return tc_tri_step(x->ctx, x->first, x->count, J, jb, set, st);
 }
 
 // Refinement stop on an estimate: the next correction d = r A^-1 is taken as at
@@ -746,8 +752,11 @@ static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool ap
   if constexpr (sizeof(T) == sizeof(z32)) {
     // unpivoted FP32 with the tensor cores: delayed two-step updates (ADGA_NO_PAIRS=1: step by step)
     if (!split && nopiv && tc && tc_pair_supported(h->tc) && !getenv("ADGA_NO_PAIRS")) {
-      TcRange r{h->tc, 0, lb.batch};
-      PairOps ops{tc_pair_narrow_fn, tc_pair_wide_fn, &r};
+      // L21 / U12 on the tensor cores with the staging written by the same kernel
+      // (ADGA_TRI_TILE=1: the FP32 CUDA-core tile products and the split kernels)
+      const bool tri_tc = (lb.N % 2) == 0 && !getenv("ADGA_TRI_TILE");
+      TcRange r{h->tc, 0, lb.batch, tri_tc};
+      PairOps ops{tc_pair_narrow_fn, tc_pair_wide_fn, &r, tri_tc ? tc_tri_fn : nullptr};
       return lu_factor_pairs(M, lb, ops, st, tt);
     }
   }

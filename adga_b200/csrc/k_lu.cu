@@ -1044,8 +1044,10 @@ static cudaError_t lu_trail_step(T *M, const LUBatch &lb, int J, int jb, trail_f
   return cudaSuccess;
 }
 
-// kernels of one unpivoted FP32 step: block LU + inverses, L21, U12 (k_diag_inv, k_tri_tile)
-static cudaError_t nopiv_step_kernels(z32 *M, const LUBatch &lb, int J, int jb, cudaStream_t st) {
+// kernels of one unpivoted FP32 step: block LU + inverses, L21, U12 (k_diag_inv, k_tri_tile;
+// tiles = false: the block LU only)
+static cudaError_t nopiv_step_kernels(z32 *M, const LUBatch &lb, int J, int jb, cudaStream_t st,
+                                      bool tiles = true) {
   typedef z32 T;
   const int nsteps = lb.nsteps();
   cudaError_t e;
@@ -1056,6 +1058,7 @@ static cudaError_t nopiv_step_kernels(z32 *M, const LUBatch &lb, int J, int jb, 
   k_diag_inv<T><<<lb.batch, 256, sm_di, st>>>(M, lb.strideM, lb.N, J, jb, lb.NB, nsteps, (T *)lb.Linv,
                                               (T *)lb.Uinv, lb.ipiv, lb.rmap);
   if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
+  if (!tiles) return cudaSuccess;
   if (J + jb < lb.N) {
     k_tri_tile<T, false><<<dim3(cdiv_u(lb.N - J - jb, 64), lb.batch), 256, sm_tt, st>>>(
         M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, nsteps, (const T *)lb.Uinv);
@@ -1082,7 +1085,8 @@ cudaError_t lu_factor_pairs(z32 *M, const LUBatch &lb, const PairOps &ops, cudaS
   const int nsteps = lb.nsteps();
   for (int s = 0; s < nsteps; ++s) {
     const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
-    cudaError_t e = nopiv_step_kernels(M, lb, J, jb, st);
+    cudaError_t e = nopiv_step_kernels(M, lb, J, jb, st, ops.tri == nullptr);
+    if (e == cudaSuccess && ops.tri) e = ops.tri(ops.ctx, J, jb, s % 2, st);
     if (e != cudaSuccess) return e;
     if (J + jb >= lb.N) break;
     cudaEvent_t ev0 = (tt && tt->ev) ? tt->ev[2 * tt->n] : nullptr;

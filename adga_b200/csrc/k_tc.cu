@@ -439,6 +439,267 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
   lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
+// ---------------------------------------------------------------------------
+// Panel products of one unpivoted step on the tensor cores (k_tc_tri):
+//   mode 0   L21   = A21 U11^-1     rows J+jb.. of the step's jb columns
+//   mode 1   U12^T = A12^T L11^-T   columns J+jb.. (right-hand sides included)
+//                                   of the step's jb rows
+// with U11^-1 / L11^-1 the 64 x 64 block inverses of k_diag_inv.  One CTA per
+// tile of 128 rows (mode 0) or 128 columns (mode 1) of one matrix, K = 64:
+//   * every thread loads its part of the FP32 tile from the matrix (coalesced),
+//     splits each value into bf16 hi + lo and writes the K-major, 128 B
+//     swizzled A operand [Xr_hi | Xi_hi | Xr_lo | Xi_lo] (four 64-wide K blocks);
+//   * the block inverse W becomes the B operand, real-part rows
+//     [Wr | -Wi] and imaginary-part rows [Wi | Wr], hi and lo K blocks;
+//   * one thread issues 24 MMAs (M = 128, N = 128, K = 16): the (hi, hi),
+//     (hi, lo) and (lo, hi) products of the 3-term split into one TMEM
+//     accumulator (columns 0..63 real, 64..127 imaginary parts);
+//   * the epilogue (thread = row of the tile) writes the FP32 result into the
+//     matrix and the step's operand staging of the trailing update
+//     (k_split_a's layout for L21, k_split_b's for U12), so no split kernel
+//     runs for the step.
+// The wait on the MMAs is bounded (WAIT_NS); on a timeout the CTA records an
+// error and skips its epilogue.
+// ---------------------------------------------------------------------------
+constexpr int TT_THREADS = 256;
+constexpr int TT_ROWS = 128;                       // tile rows (MMA M)
+constexpr int TT_KBLK = TT_ROWS * 128;             // one K block: 128 rows x 64 bf16
+constexpr int TT_SMEM_BYTES = 8 * TT_KBLK + 1024 + 64;
+constexpr int TT_TMEM_COLS = 128;
+// kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
+constexpr uint32_t IDESC_N128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 / 8) << 17) |
+                                ((uint32_t)(TT_ROWS / 16) << 24);
+
+__device__ __forceinline__ void mma_bf16_n128(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(IDESC_N128), "r"(acc));
+}
+// byte offset of 16-byte chunk c (0..7) of row r in a 128 B swizzled K block
+__device__ __forceinline__ uint32_t sw128(int r, int c) {
+  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
+}
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+// 8 consecutive K values of one row -> the four K blocks (re hi, im hi, re lo, im lo), chunk c
+__device__ __forceinline__ void put_chunk(unsigned char *base, int r, int c, const float2 *v, bool neg_im,
+                                          bool swap) {
+  uint32_t w[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    __nv_bfloat16 h[4][2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      float re = v[2 * j + u].x, im = v[2 * j + u].y;
+      if (neg_im) im = -im;
+      if (swap) { const float x = re; re = im; im = x; }
+      __nv_bfloat16 rh, rl, ih, il;
+      split2(re, rh, rl);
+      split2(im, ih, il);
+      h[0][u] = rh; h[1][u] = ih; h[2][u] = rl; h[3][u] = il;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[q][j] = pack_bf16(h[q][0], h[q][1]);
+  }
+  const uint32_t off = sw128(r, c);
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    *reinterpret_cast<uint4 *>(base + q * TT_KBLK + off) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+}
+
+__global__ void __launch_bounds__(TT_THREADS, 1)
+k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
+         const z32 *Uinv, __nv_bfloat16 *Astage, __nv_bfloat16 *Bstage, int Ncap, int b0, int ntA, int ntU,
+         int *err) {
+  extern __shared__ unsigned char smraw[];
+  const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
+  unsigned char *gA = smraw + (sbase - smem_u32(smraw));
+  unsigned char *gB = gA + 4 * TT_KBLK;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(gA + 8 * TT_KBLK);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const uint32_t sA = sbase, sB = sbase + 4 * TT_KBLK, sbar = smem_u32(bar);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int per = ntA + ntU;
+  const int b = b0 + blockIdx.x / per, tile = blockIdx.x % per;
+  const bool lower = tile < ntA;                       // mode 0: L21
+  const int m0 = (lower ? tile : tile - ntA) * TT_ROWS;
+  const int nrows = lower ? N - J - jb : ncols - J - jb;
+  z32 *Am = M + (size_t)b * strideM;
+  const size_t woff = ((size_t)b * nsteps + J / NB) * NB * NB;
+
+  if (t == 0) {
+    mbar_init(sbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(TT_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+
+  // ---- A operand: the tile, 128 rows x 64 K (zero outside the matrix / beyond jb)
+  {
+    float2 v[32];
+    int r, kh;
+    if (lower) {
+      // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
+      r = t & 127;
+      kh = t >> 7;
+      const bool rv = m0 + r < nrows;
+      const z32 *src = Am + (size_t)(J + jb + m0 + r);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int k = kh * 32 + i;
+        v[i] = (rv && k < jb) ? src[(size_t)(J + k) * N] : make_float2(0.f, 0.f);
+      }
+    } else {
+      // columns J+jb+m0+r, rows J+k: two threads per column, 256 contiguous bytes each
+      r = t >> 1;
+      kh = t & 1;
+      const bool rv = m0 + r < nrows;
+      const z32 *src = Am + (size_t)(J + jb + m0 + r) * N + J;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int k = kh * 32 + 2 * i;            // jb is even: k, k+1 are both in or both out
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (rv && k < jb) q = *reinterpret_cast<const float4 *>(src + k);
+        v[2 * i] = make_float2(q.x, q.y);
+        v[2 * i + 1] = make_float2(q.z, q.w);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) put_chunk(gA, r, kh * 4 + j, v + 8 * j, false, false);
+  }
+  // ---- B operand: W = U11^-1 (mode 0) or L11^-T (mode 1); real-part row n
+  //      [Wr(:, n) | -Wi(:, n)], imaginary-part row 64 + n [Wi(:, n) | Wr(:, n)]
+  {
+    const int n = t & 63, kq = t >> 6;            // K values kq*16 .. kq*16+15 of column n
+    float2 w[16];
+    const z32 *W = (lower ? Uinv : Linv) + woff;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int k = kq * 16 + i;
+      w[i] = lower ? W[k + n * NB] : W[n + k * NB];
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      put_chunk(gB, n, kq * 2 + j, w + 8 * j, true, false);        // [Wr | -Wi]
+      put_chunk(gB, 64 + n, kq * 2 + j, w + 8 * j, false, true);   // [Wi | Wr]
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+
+  if (t == 32) {
+    // (hi, hi), (hi, lo), (lo, hi): K blocks {0,1} are the hi parts, {2,3} the lo parts
+    const int ap[3] = {0, 0, 2}, bp[3] = {0, 2, 0};
+#pragma unroll
+    for (int term = 0; term < 3; ++term)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint32_t a = sA + (ap[term] + j / 4) * TT_KBLK + (j % 4) * 32;
+        const uint32_t bb = sB + (bp[term] + j / 4) * TT_KBLK + (j % 4) * 32;
+        mma_bf16_n128(tmem, smem_desc(a), smem_desc(bb), (term > 0 || j > 0) ? 1u : 0u);
+      }
+    mma_commit(sbar);
+  }
+
+  // ---- epilogue: warp w reads TMEM lanes 32 (w % 4).. (tile rows), output columns 32 (w / 4)..
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(sbar, 0, err, 21));
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (ok) {
+    const int quad = warp & 3, half = warp >> 2;
+    const int r = quad * 32 + lane;
+    const int mr = m0 + r;
+    const bool rv = mr < nrows;
+    // 8 bf16 of x[8 c .. 8 c + 7], negated when neg
+    auto chunk = [](const __nv_bfloat16 (&x)[16], int c, bool neg) {
+      uint32_t w[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        __nv_bfloat16 p = x[8 * c + 2 * u], q = x[8 * c + 2 * u + 1];
+        if (neg) { p = __hneg(p); q = __hneg(q); }
+        w[u] = pack_bf16(p, q);
+      }
+      return make_uint4(w[0], w[1], w[2], w[3]);
+    };
+#pragma unroll 1
+    for (int piece = 0; piece < 2; ++piece) {
+      const int n0 = half * 32 + piece * 16;        // output columns n0 .. n0 + 15
+      const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)n0;
+      float re[16], im[16];
+      tmem_ld16(tl, re);
+      tmem_ld16(tl + 64, im);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (!rv) continue;
+      __nv_bfloat16 rh[16], rl[16], ih[16], il[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        split2(re[j], rh[j], rl[j]);
+        split2(im[j], ih[j], il[j]);
+      }
+      if (lower) {
+        // L21 into the matrix: row J+jb+mr, columns J+n
+        z32 *dst = Am + (size_t)(J + jb + mr);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (n0 + j < jb) dst[(size_t)(J + n0 + j) * N] = make_float2(re[j], im[j]);
+        // k_split_a's row: [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo], NB each
+        __nv_bfloat16 *row = Astage + ((size_t)b * N + mr) * 6 * NB + n0;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const uint4 xrh = chunk(rh, c, false), xih = chunk(ih, c, false);
+          *reinterpret_cast<uint4 *>(row + 0 * NB + 8 * c) = xrh;
+          *reinterpret_cast<uint4 *>(row + 1 * NB + 8 * c) = xih;
+          *reinterpret_cast<uint4 *>(row + 2 * NB + 8 * c) = xrh;
+          *reinterpret_cast<uint4 *>(row + 3 * NB + 8 * c) = xih;
+          *reinterpret_cast<uint4 *>(row + 4 * NB + 8 * c) = chunk(rl, c, false);
+          *reinterpret_cast<uint4 *>(row + 5 * NB + 8 * c) = chunk(il, c, false);
+        }
+      } else {
+        // U12 into the matrix: column J+jb+mr, rows J+n (pairs: jb is even)
+        z32 *dst = Am + (size_t)(J + jb + mr) * N + J;
+#pragma unroll
+        for (int j = 0; j < 16; j += 2)
+          if (n0 + j < jb)
+            *reinterpret_cast<float4 *>(dst + n0 + j) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
+        // k_split_b's rows: real [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo, Ur_hi, -Ui_hi],
+        //                   imaginary [Ui_hi, Ur_hi, Ui_lo, Ur_lo, Ui_hi, Ur_hi]
+        __nv_bfloat16 *rr = Bstage + ((size_t)b * 2 * Ncap + mr) * 6 * NB + n0;
+        __nv_bfloat16 *ri = Bstage + ((size_t)b * 2 * Ncap + Ncap + mr) * 6 * NB + n0;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const uint4 xrh = chunk(rh, c, false), nih = chunk(ih, c, true), xih = chunk(ih, c, false);
+          *reinterpret_cast<uint4 *>(rr + 0 * NB + 8 * c) = xrh;
+          *reinterpret_cast<uint4 *>(rr + 1 * NB + 8 * c) = nih;
+          *reinterpret_cast<uint4 *>(rr + 2 * NB + 8 * c) = chunk(rl, c, false);
+          *reinterpret_cast<uint4 *>(rr + 3 * NB + 8 * c) = chunk(il, c, true);
+          *reinterpret_cast<uint4 *>(rr + 4 * NB + 8 * c) = xrh;
+          *reinterpret_cast<uint4 *>(rr + 5 * NB + 8 * c) = nih;
+          *reinterpret_cast<uint4 *>(ri + 0 * NB + 8 * c) = xih;
+          *reinterpret_cast<uint4 *>(ri + 1 * NB + 8 * c) = xrh;
+          *reinterpret_cast<uint4 *>(ri + 2 * NB + 8 * c) = chunk(il, c, false);
+          *reinterpret_cast<uint4 *>(ri + 3 * NB + 8 * c) = chunk(rl, c, false);
+          *reinterpret_cast<uint4 *>(ri + 4 * NB + 8 * c) = xih;
+          *reinterpret_cast<uint4 *>(ri + 5 * NB + 8 * c) = xrh;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TT_TMEM_COLS));
+  }
+}
+
 // A[b][m][6*NB]: rows m = 0..Mrows-1 are matrix rows J+jb+m, k = 0..NB-1 (zero for k >= jb)
 __global__ void __launch_bounds__(256)
 k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB, __nv_bfloat16 *A,
@@ -683,11 +944,28 @@ cudaError_t stage_step(TcCtx *c, __nv_bfloat16 *A, __nv_bfloat16 *B, int first, 
 
 int tc_pair_supported(void *ctxp) { return ctxp && ((TcCtx *)ctxp)->persist && ((TcCtx *)ctxp)->lb.NB == 64; }
 
-cudaError_t tc_pair_narrow(void *ctxp, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                           cudaEvent_t ev0, cudaEvent_t ev1) {
+// L21 and U12 of unpivoted step (J, jb) on the tensor cores (k_tc_tri), which also
+// writes the step's operand staging: set 0 (the first step of a pair) or 1 (the second)
+cudaError_t tc_tri_step(void *ctxp, int first, int count, int J, int jb, int set, cudaStream_t st) {
   TcCtx *c = (TcCtx *)ctxp;
   const LUBatch &lb = c->lb;
-  cudaError_t e = stage_step(c, c->A, c->B, first, count, J0, jb, st);
+  if (!c->persist || lb.NB != 64 || (jb & 1)) return cudaErrorInvalidValue;
+  const int ntA = (int)cdiv_u(std::max(lb.N - J - jb, 0), TT_ROWS);
+  const int ntU = (int)cdiv_u(std::max(lb.ncols - J - jb, 0), TT_ROWS);
+  if (ntA + ntU == 0 || count <= 0) return cudaSuccess;
+  cudaError_t e = smem_limit(k_tc_tri, TT_SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  k_tc_tri<<<(unsigned)((ntA + ntU) * count), TT_THREADS, TT_SMEM_BYTES, st>>>(
+      c->M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, lb.nsteps(), (const z32 *)lb.Linv, (const z32 *)lb.Uinv,
+      set ? c->A2 : c->A, set ? c->B2 : c->B, c->Ncap, first, ntA, ntU, c->err);
+  return ADGA_LAUNCH_CHECK();
+}
+
+cudaError_t tc_pair_narrow(void *ctxp, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
+                           cudaEvent_t ev0, cudaEvent_t ev1, bool staged) {
+  TcCtx *c = (TcCtx *)ctxp;
+  const LUBatch &lb = c->lb;
+  cudaError_t e = staged ? cudaSuccess : stage_step(c, c->A, c->B, first, count, J0, jb, st);
   if (e != cudaSuccess) return e;
   const int J1 = J0 + jb;
   if (ev0) cudaEventRecord(ev0, st);
@@ -701,13 +979,13 @@ cudaError_t tc_pair_narrow(void *ctxp, int first, int count, int J0, int jb, int
 }
 
 cudaError_t tc_pair_wide(void *ctxp, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                         cudaEvent_t ev0, cudaEvent_t ev1) {
+                         cudaEvent_t ev0, cudaEvent_t ev1, bool staged) {
   TcCtx *c = (TcCtx *)ctxp;
   const LUBatch &lb = c->lb;
   const int J1 = J0 + jb, R0 = J1 + jb2;
   if (lb.N - R0 <= 0) return cudaSuccess;
-  // step J0's staging (from tc_pair_narrow, rows / columns from J1) is still valid
-  cudaError_t e = stage_step(c, c->A2, c->B2, first, count, J1, jb2, st);
+  // step J0's staging (rows / columns from J1) is still valid
+  cudaError_t e = staged ? cudaSuccess : stage_step(c, c->A2, c->B2, first, count, J1, jb2, st);
   if (e != cudaSuccess) return e;
   if (ev0) cudaEventRecord(ev0, st);
   e = persist_region(c, true, first, count, R0, R0, jb2, jb2, 0, 0, lb.N - R0, lb.ncols - R0, st);

@@ -55,10 +55,13 @@ cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn tr
 // Delayed updates of the unpivoted FP32 factorisation (tensor cores): after step
 // J0 (width jb) `narrow` applies its update to what step J1 = J0 + jb (width jb2)
 // reads; after step J1 `wide` applies both steps' updates to the rest.
+// tri (optional): L21 and U12 of step (J, jb) in place of the CUDA-core tile
+// products, also writing the operand staging set (0: first step of a pair, 1: second)
 struct PairOps {
   cudaError_t (*narrow)(void *ctx, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
   cudaError_t (*wide)(void *ctx, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
   void *ctx;
+  cudaError_t (*tri)(void *ctx, int J, int jb, int set, cudaStream_t st) = nullptr;
 };
 cudaError_t lu_factor_pairs(z32 *M, const LUBatch &lb, const PairOps &ops, cudaStream_t st,
                             TrailTiming *tt = nullptr);
