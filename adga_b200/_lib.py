@@ -24,7 +24,8 @@ EXPORTS = [
     "adga_inverse_matrix_z_noalloc", "adga_set_vertex_g4", "adga_vertex_transform",
     "adga_index2component_band", "adga_post_loop", "adga_set_threeleg", "adga_set_chi_loc_ext",
     "adga_set_vq", "adga_set_tangent", "adga_set_vertex_tangent", "adga_ladder_run_tangent",
-    "adga_get_tangent_outputs", "adga_clear_tangents",
+    "adga_get_tangent_outputs", "adga_clear_tangents", "adga_set_tune", "adga_get_tune",
+    "adga_autotune",
 ]
 
 
@@ -47,6 +48,17 @@ class RunStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tune(C.Structure):
+    _fields_ = [("factor", C.c_int), ("pairs", C.c_int), ("tri_tc", C.c_int), ("batch", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneTrial(C.Structure):
+    _fields_ = [("tune", Tune), ("ms", C.c_double), ("err", C.c_double), ("accepted", C.c_int)]
 
 
 class Outputs(C.Structure):
@@ -102,6 +114,9 @@ def load():
         "adga_ladder_run_tangent": [vp, i, i, i, ip, C.POINTER(RunStats)],
         "adga_get_tangent_outputs": [vp, i, C.POINTER(Outputs)],
         "adga_clear_tangents": [vp],
+        "adga_set_tune": [vp, C.POINTER(Tune)],
+        "adga_get_tune": [vp, C.POINTER(Tune)],
+        "adga_autotune": [vp, i, i, d, C.POINTER(TuneTrial), i, ip, C.POINTER(Tune)],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

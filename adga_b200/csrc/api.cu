@@ -115,6 +115,7 @@ struct adga_handle {
   bool refine_estimate = true;   // stop on the bounded next correction (ADGA_REFINE_EXACT=1: on a solved one)
   bool mixed_nopiv = true;   // FP32 factorisation without row interchanges (ADGA_MIXED_PIVOT=1: with)
   double tol = 1e-10;   // stop when max|dX| <= tol * max|X| (the error is then far below)
+  adga_tune tune{0, 1, 1, 0};   // mixed-path kernel choices (adga_set_tune / adga_autotune)
   // last-run statistics
   adga_run_stats stats{};
 };
@@ -308,6 +309,8 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   if (const char *mpv = getenv("ADGA_MIXED_PIVOT")) h->mixed_nopiv = atoi(mpv) == 0;
   if (const char *mr = getenv("ADGA_MAX_REFINE")) h->max_iter = std::max(1, atoi(mr));
   if (const char *re = getenv("ADGA_REFINE_EXACT")) h->refine_estimate = atoi(re) == 0;
+  if (getenv("ADGA_NO_PAIRS")) h->tune.pairs = 0;
+  if (getenv("ADGA_TRI_TILE")) h->tune.tri_tc = 0;
   const char *ev = getenv("ADGA_NB");
   if (ev) h->NB = std::max(16, std::min(64, atoi(ev) / 8 * 8));   // the LU kernels assume NB <= 64
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -674,7 +677,8 @@ static size_t bytes_per_point(const adga_handle *h, int prec, int NB) {
 
 static int ensure_work(adga_handle *h, int prec, int want) {
   const DevCtx &c = h->c;
-  if (h->cap_prec == prec && h->cap >= want) return 0;
+  if (h->tune.batch > 0) want = std::min(want, h->tune.batch);
+  if (h->cap_prec == prec && h->cap >= want && (h->tune.batch <= 0 || h->cap <= h->tune.batch)) return 0;
   cudaStreamSynchronize(h->st);
   if (h->tc) { tc_trail_free(h->tc); h->tc = nullptr; }
   free_list(h->work);
@@ -750,11 +754,11 @@ static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool ap
   // overlap on the t2g workload; kept as an option (ADGA_TWO_STREAMS=1)
   const bool split = h->st2 && lb.batch >= 8 && getenv("ADGA_TWO_STREAMS");
   if constexpr (sizeof(T) == sizeof(z32)) {
-    // unpivoted FP32 with the tensor cores: delayed two-step updates (ADGA_NO_PAIRS=1: step by step)
-    if (!split && nopiv && tc && tc_pair_supported(h->tc) && !getenv("ADGA_NO_PAIRS")) {
+    // unpivoted FP32 with the tensor cores: delayed two-step updates (tune.pairs = 0: step by step)
+    if (!split && nopiv && tc && tc_pair_supported(h->tc) && h->tune.pairs) {
       // L21 / U12 on the tensor cores with the staging written by the same kernel
-      // (ADGA_TRI_TILE=1: the FP32 CUDA-core tile products and the split kernels)
-      const bool tri_tc = (lb.N % 2) == 0 && !getenv("ADGA_TRI_TILE");
+      // (tune.tri_tc = 0: the FP32 CUDA-core tile products and the split kernels)
+      const bool tri_tc = (lb.N % 2) == 0 && h->tune.tri_tc;
       TcRange r{h->tc, 0, lb.batch, tri_tc};
       PairOps ops{tc_pair_narrow_fn, tc_pair_wide_fn, &r, tri_tc ? tc_tri_fn : nullptr};
       return lu_factor_pairs(M, lb, ops, st, tt);
@@ -1393,6 +1397,8 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   if (qwstart < 1 || qwstop > total || qwstop < qwstart)
     return fail(h, ADGA_EINVAL, "qw range outside 1..nqp*(2*iwbmax_small+1)");
   if (precision != ADGA_FP64 && precision != ADGA_MIXED) return fail(h, ADGA_EINVAL, "precision");
+  // the tuned mixed path may factor in FP64 (tune.factor = 1: faster at this size)
+  if (precision == ADGA_MIXED && h->tune.factor == 1) precision = ADGA_FP64;
   const int npts = qwstop - qwstart + 1;
   int r = ensure_outputs(h, npts);
   if (r) return r;
@@ -1451,6 +1457,102 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
   h->last_npts = npts;
   if (stats) *stats = h->stats;
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// kernel choices of the mixed path and the autotuner
+// ---------------------------------------------------------------------------
+extern "C" int adga_set_tune(adga_handle *h, const adga_tune *t) {
+  if (!h || !t) return ADGA_EINVAL;
+  if (t->factor < 0 || t->factor > 1 || t->pairs < 0 || t->pairs > 1 || t->tri_tc < 0 || t->tri_tc > 1 ||
+      t->batch < 0)
+    return fail(h, ADGA_EINVAL, "adga_set_tune: factor, pairs, tri_tc in {0, 1}, batch >= 0");
+  h->tune = *t;
+  return 0;
+}
+
+extern "C" int adga_get_tune(const adga_handle *h, adga_tune *t) {
+  if (!h || !t) return ADGA_EINVAL;
+  *t = h->tune;
+  return 0;
+}
+
+// one run of qwstart..qwstop from zeroed accumulators; host copies of the
+// per-point chi and of Sigma_nl
+static int tune_sample(adga_handle *h, int qwstart, int qwstop, int prec, std::vector<z64> &chi,
+                       std::vector<z64> &sig, double *ms) {
+  int r = adga_reset_outputs(h);
+  if (r) return r;
+  adga_run_stats st{};
+  if ((r = adga_ladder_run(h, qwstart, qwstop, prec, nullptr, &st))) return r;
+  const size_t nc = (size_t)(qwstop - qwstart + 1) * h->nd4;
+  const size_t ns = (size_t)h->c.nd2 * 2 * h->c.iwf * h->c.nkp_eom;
+  chi.resize(2 * nc);
+  sig.resize(ns);
+  CK(cudaMemcpy(chi.data(), h->chi_qw_d, nc * sizeof(z64), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(chi.data() + nc, h->chi_qw_m, nc * sizeof(z64), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sig.data(), h->sigma_nl, ns * sizeof(z64), cudaMemcpyDeviceToHost));
+  *ms = st.ms_total;
+  return 0;
+}
+
+static double rel_diff(const std::vector<z64> &a, const std::vector<z64> &b, size_t lo, size_t hi) {
+  double num = 0.0, den = 0.0;
+  for (size_t i = lo; i < hi; ++i) {
+    const double d = std::max(std::fabs(a[i].x - b[i].x), std::fabs(a[i].y - b[i].y));
+    const double m = std::max(std::fabs(b[i].x), std::fabs(b[i].y));
+    if (!(d <= num)) num = d;    // NaN propagates
+    den = std::max(den, m);
+  }
+  return den > 0 ? num / den : num;
+}
+
+extern "C" int adga_autotune(adga_handle *h, int qwstart, int qwstop, double tol, adga_tune_trial *trials,
+                             int max_trials, int *ntrials, adga_tune *best) {
+  if (!h) return ADGA_EINVAL;
+  const DevCtx &c = h->c;
+  if (qwstart < 1 || qwstop > c.nqp * h->nw || qwstop < qwstart)
+    return fail(h, ADGA_EINVAL, "adga_autotune: qw range outside 1..nqp*(2*iwbmax_small+1)");
+  if (h->tan_on) return fail(h, ADGA_ESTATE, "adga_autotune: not inside a tangent run");
+  if (!(tol > 0)) tol = 1e-8;
+  const adga_tune start = h->tune;
+  // candidates: the tensor-core variants (when the tensor cores serve this size), then
+  // the FP64 factorisation
+  std::vector<adga_tune> cand;
+  auto with = [&](int f, int p, int t) { adga_tune x = start; x.factor = f; x.pairs = p; x.tri_tc = t; return x; };
+  const bool tc = tc_available() && !getenv("ADGA_NO_TC");
+  if (tc) {
+    if (c.N % 2 == 0) cand.push_back(with(0, 1, 1));
+    cand.push_back(with(0, 1, 0));
+    cand.push_back(with(0, 0, 0));
+  } else {
+    cand.push_back(with(0, 0, 0));
+  }
+  cand.push_back(with(1, 0, 0));
+  std::vector<z64> ref_chi, ref_sig, chi, sig;
+  double ms = 0.0;
+  h->tune = start;
+  int r = tune_sample(h, qwstart, qwstop, ADGA_FP64, ref_chi, ref_sig, &ms);
+  const size_t nc = ref_chi.size() / 2;
+  int nt = 0, ibest = -1;
+  double best_ms = 0.0;
+  for (size_t i = 0; !r && i < cand.size(); ++i) {
+    h->tune = cand[i];
+    double ms_warm = 0.0;
+    if ((r = tune_sample(h, qwstart, qwstop, ADGA_MIXED, chi, sig, &ms_warm))) break;
+    if ((r = tune_sample(h, qwstart, qwstop, ADGA_MIXED, chi, sig, &ms))) break;
+    const double err = std::max({rel_diff(chi, ref_chi, 0, nc), rel_diff(chi, ref_chi, nc, 2 * nc),
+                                 rel_diff(sig, ref_sig, 0, sig.size())});
+    const bool ok = err <= tol;
+    if (trials && nt < max_trials) trials[nt] = adga_tune_trial{cand[i], ms, err, ok ? 1 : 0};
+    ++nt;
+    if (ok && (ibest < 0 || ms < best_ms)) { ibest = (int)i; best_ms = ms; }
+  }
+  h->tune = (!r && ibest >= 0) ? cand[ibest] : start;
+  if (ntrials) *ntrials = nt;
+  if (best) *best = h->tune;
+  int r2 = adga_reset_outputs(h);
+  return r ? r : r2;
 }
 
 extern "C" int adga_ladder_run_tangent(adga_handle *h, int qwstart, int qwstop, int precision, int *status,

@@ -464,8 +464,14 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
 constexpr int TT_THREADS = 256;
 constexpr int TT_ROWS = 128;                       // tile rows (MMA M)
 constexpr int TT_KBLK = TT_ROWS * 128;             // one K block: 128 rows x 64 bf16
-constexpr int TT_SMEM_BYTES = 8 * TT_KBLK + 1024 + 64;
+constexpr int TT_WLD = 65;                         // padded column stride of the staged block inverse
+constexpr int TT_W_BYTES = 64 * TT_WLD * 8;        // 33,280 B
+constexpr int TT_SROW = 784;                       // padded stride of a staged 768 B operand row
+constexpr int TT_FROW = 528;                       // padded stride of a staged 512 B matrix column
+constexpr int TT_SMEM_BYTES = 8 * TT_KBLK + TT_W_BYTES + 1024 + 64;
 constexpr int TT_TMEM_COLS = 128;
+static_assert(TT_ROWS * TT_SROW <= 8 * TT_KBLK && TT_ROWS * TT_FROW <= 8 * TT_KBLK,
+              "the epilogue staging reuses the operand buffers");
 // kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
 constexpr uint32_t IDESC_N128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 / 8) << 17) |
                                 ((uint32_t)(TT_ROWS / 16) << 24);
@@ -509,6 +515,32 @@ __device__ __forceinline__ void put_chunk(unsigned char *base, int r, int c, con
   for (int q = 0; q < 4; ++q)
     *reinterpret_cast<uint4 *>(base + q * TT_KBLK + off) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
 }
+// 8 bf16 of the values x[0..7] (split part `part`: 0 re hi, 1 re lo, 2 im hi, 3 im lo), negated when neg
+__device__ __forceinline__ uint4 pack8(const float *re, const float *im, int part, bool neg) {
+  uint32_t w[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    __nv_bfloat16 p2[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      __nv_bfloat16 hi, lo;
+      split2(part < 2 ? re[2 * u + e] : im[2 * u + e], hi, lo);
+      p2[e] = (part & 1) ? lo : hi;
+      if (neg) p2[e] = __hneg(p2[e]);
+    }
+    w[u] = pack_bf16(p2[0], p2[1]);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+// nrow rows of 768 B, staged with stride TT_SROW, to nrow contiguous global rows
+__device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat16 *dst, int nrow, int t) {
+  unsigned char *d = reinterpret_cast<unsigned char *>(dst);
+  for (int e = t; e < nrow * 48; e += TT_THREADS) {
+    const int r = e / 48, c = e % 48;
+    *reinterpret_cast<uint4 *>(d + (size_t)r * 768 + c * 16) =
+        *reinterpret_cast<const uint4 *>(stg + r * TT_SROW + c * 16);
+  }
+}
 
 __global__ void __launch_bounds__(TT_THREADS, 1)
 k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
@@ -518,7 +550,8 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gA = smraw + (sbase - smem_u32(smraw));
   unsigned char *gB = gA + 4 * TT_KBLK;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(gA + 8 * TT_KBLK);
+  z32 *Wsh = reinterpret_cast<z32 *>(gA + 8 * TT_KBLK);            // [64][TT_WLD]
+  uint64_t *bar = reinterpret_cast<uint64_t *>(gA + 8 * TT_KBLK + TT_W_BYTES);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
   const uint32_t sA = sbase, sB = sbase + 4 * TT_KBLK, sbar = smem_u32(bar);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -527,9 +560,18 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   const bool lower = tile < ntA;                       // mode 0: L21
   const int m0 = (lower ? tile : tile - ntA) * TT_ROWS;
   const int nrows = lower ? N - J - jb : ncols - J - jb;
+  const int nv = min(TT_ROWS, nrows - m0);             // valid rows of the tile
   z32 *Am = M + (size_t)b * strideM;
-  const size_t woff = ((size_t)b * nsteps + J / NB) * NB * NB;
 
+  // the block inverse W (U11^-1, or L11^-1 for mode 1) into shared memory, coalesced
+  {
+    const z32 *W = (lower ? Uinv : Linv) + ((size_t)b * nsteps + J / NB) * NB * NB;
+    for (int e = t; e < 64 * 64; e += TT_THREADS) {
+      const uint32_t d = smem_u32(Wsh + (e & 63) + (e >> 6) * TT_WLD);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(W + e));
+    }
+    asm volatile("cp.async.commit_group;");
+  }
   if (t == 0) {
     mbar_init(sbar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -548,7 +590,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
       r = t & 127;
       kh = t >> 7;
-      const bool rv = m0 + r < nrows;
+      const bool rv = r < nv;
       const z32 *src = Am + (size_t)(J + jb + m0 + r);
 #pragma unroll
       for (int i = 0; i < 32; ++i) {
@@ -559,7 +601,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       // columns J+jb+m0+r, rows J+k: two threads per column, 256 contiguous bytes each
       r = t >> 1;
       kh = t & 1;
-      const bool rv = m0 + r < nrows;
+      const bool rv = r < nv;
       const z32 *src = Am + (size_t)(J + jb + m0 + r) * N + J;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
@@ -573,16 +615,17 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
 #pragma unroll
     for (int j = 0; j < 4; ++j) put_chunk(gA, r, kh * 4 + j, v + 8 * j, false, false);
   }
-  // ---- B operand: W = U11^-1 (mode 0) or L11^-T (mode 1); real-part row n
-  //      [Wr(:, n) | -Wi(:, n)], imaginary-part row 64 + n [Wi(:, n) | Wr(:, n)]
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+  // ---- B operand from W: real-part row n [Wr(:, n) | -Wi(:, n)], imaginary-part row
+  //      64 + n [Wi(:, n) | Wr(:, n)]; mode 0: W(k, n) = U11^-1(k, n), mode 1: L11^-1(n, k)
   {
     const int n = t & 63, kq = t >> 6;            // K values kq*16 .. kq*16+15 of column n
     float2 w[16];
-    const z32 *W = (lower ? Uinv : Linv) + woff;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int k = kq * 16 + i;
-      w[i] = lower ? W[k + n * NB] : W[n + k * NB];
+      w[i] = lower ? Wsh[k + n * TT_WLD] : Wsh[n + k * TT_WLD];
     }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -610,85 +653,92 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
     mma_commit(sbar);
   }
 
-  // ---- epilogue: warp w reads TMEM lanes 32 (w % 4).. (tile rows), output columns 32 (w / 4)..
-  const bool ok = __all_sync(0xffffffffu, mbar_wait(sbar, 0, err, 21));
+  // ---- epilogue: warp w reads TMEM lanes 32 (w % 4).. (tile rows) and output columns
+  //      32 (w / 4) .. + 31; the results reach global memory through shared memory (the
+  //      operand buffers, free once the MMAs completed) so that every store is coalesced
+  // CTA-uniform: the epilogue below has block barriers
+  const bool ok = __syncthreads_and(mbar_wait(sbar, 0, err, 21));
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (ok) {
     const int quad = warp & 3, half = warp >> 2;
     const int r = quad * 32 + lane;
-    const int mr = m0 + r;
-    const bool rv = mr < nrows;
-    // 8 bf16 of x[8 c .. 8 c + 7], negated when neg
-    auto chunk = [](const __nv_bfloat16 (&x)[16], int c, bool neg) {
-      uint32_t w[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        __nv_bfloat16 p = x[8 * c + 2 * u], q = x[8 * c + 2 * u + 1];
-        if (neg) { p = __hneg(p); q = __hneg(q); }
-        w[u] = pack_bf16(p, q);
-      }
-      return make_uint4(w[0], w[1], w[2], w[3]);
-    };
-#pragma unroll 1
-    for (int piece = 0; piece < 2; ++piece) {
-      const int n0 = half * 32 + piece * 16;        // output columns n0 .. n0 + 15
+    const int n0 = half * 32;
+    float re[32], im[32];
+    {
       const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)n0;
-      float re[16], im[16];
-      tmem_ld16(tl, re);
-      tmem_ld16(tl + 64, im);
+      tmem_ld16(tl, *reinterpret_cast<float(*)[16]>(re));
+      tmem_ld16(tl + 16, *reinterpret_cast<float(*)[16]>(re + 16));
+      tmem_ld16(tl + 64, *reinterpret_cast<float(*)[16]>(im));
+      tmem_ld16(tl + 80, *reinterpret_cast<float(*)[16]>(im + 16));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (!rv) continue;
-      __nv_bfloat16 rh[16], rl[16], ih[16], il[16];
+    }
+    unsigned char *stg = gA;
+    if (lower) {
+      // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
+      if (r < nv) {
+        z32 *dst = Am + (size_t)(J + jb + m0 + r);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        split2(re[j], rh[j], rl[j]);
-        split2(im[j], ih[j], il[j]);
-      }
-      if (lower) {
-        // L21 into the matrix: row J+jb+mr, columns J+n
-        z32 *dst = Am + (size_t)(J + jb + mr);
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
+        for (int j = 0; j < 32; ++j)
           if (n0 + j < jb) dst[(size_t)(J + n0 + j) * N] = make_float2(re[j], im[j]);
-        // k_split_a's row: [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo], NB each
-        __nv_bfloat16 *row = Astage + ((size_t)b * N + mr) * 6 * NB + n0;
+      }
+      // k_split_a's rows [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
+      unsigned char *row = stg + r * TT_SROW + n0 * 2;
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const uint4 xrh = chunk(rh, c, false), xih = chunk(ih, c, false);
-          *reinterpret_cast<uint4 *>(row + 0 * NB + 8 * c) = xrh;
-          *reinterpret_cast<uint4 *>(row + 1 * NB + 8 * c) = xih;
-          *reinterpret_cast<uint4 *>(row + 2 * NB + 8 * c) = xrh;
-          *reinterpret_cast<uint4 *>(row + 3 * NB + 8 * c) = xih;
-          *reinterpret_cast<uint4 *>(row + 4 * NB + 8 * c) = chunk(rl, c, false);
-          *reinterpret_cast<uint4 *>(row + 5 * NB + 8 * c) = chunk(il, c, false);
+      for (int c = 0; c < 4; ++c) {
+        const uint4 rh = pack8(re + 8 * c, im + 8 * c, 0, false), ih = pack8(re + 8 * c, im + 8 * c, 2, false);
+        *reinterpret_cast<uint4 *>(row + 0 * 128 + 16 * c) = rh;
+        *reinterpret_cast<uint4 *>(row + 1 * 128 + 16 * c) = ih;
+        *reinterpret_cast<uint4 *>(row + 2 * 128 + 16 * c) = rh;
+        *reinterpret_cast<uint4 *>(row + 3 * 128 + 16 * c) = ih;
+        *reinterpret_cast<uint4 *>(row + 4 * 128 + 16 * c) = pack8(re + 8 * c, im + 8 * c, 1, false);
+        *reinterpret_cast<uint4 *>(row + 5 * 128 + 16 * c) = pack8(re + 8 * c, im + 8 * c, 3, false);
+      }
+      __syncthreads();
+      copy_rows(stg, Astage + ((size_t)b * N + m0) * 6 * NB, nv, t);
+    } else {
+      // U12 (column J+jb+m0+r, rows J..J+jb): the tile's columns staged, then 512 B per column
+      {
+        unsigned char *col = stg + r * TT_FROW + n0 * 8;
+#pragma unroll
+        for (int j = 0; j < 32; j += 2)
+          *reinterpret_cast<float4 *>(col + j * 8) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
+      }
+      __syncthreads();
+      const int pc = jb / 2;                       // 16-byte pieces of a column (jb is even)
+      for (int e = t; e < nv * pc; e += TT_THREADS) {
+        const int cc = e / pc, pp = e % pc;
+        *reinterpret_cast<float4 *>(Am + (size_t)(J + jb + m0 + cc) * N + J + 2 * pp) =
+            *reinterpret_cast<const float4 *>(stg + cc * TT_FROW + pp * 16);
+      }
+      // k_split_b's rows: real [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo, Ur_hi, -Ui_hi],
+      //                   imaginary [Ui_hi, Ur_hi, Ui_lo, Ur_lo, Ui_hi, Ur_hi]
+#pragma unroll 1
+      for (int part = 0; part < 2; ++part) {
+        __syncthreads();
+        unsigned char *row = stg + r * TT_SROW + n0 * 2;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const float *xr = re + 8 * c, *xi = im + 8 * c;
+          if (part == 0) {
+            const uint4 rh = pack8(xr, xi, 0, false), nih = pack8(xr, xi, 2, true);
+            *reinterpret_cast<uint4 *>(row + 0 * 128 + 16 * c) = rh;
+            *reinterpret_cast<uint4 *>(row + 1 * 128 + 16 * c) = nih;
+            *reinterpret_cast<uint4 *>(row + 2 * 128 + 16 * c) = pack8(xr, xi, 1, false);
+            *reinterpret_cast<uint4 *>(row + 3 * 128 + 16 * c) = pack8(xr, xi, 3, true);
+            *reinterpret_cast<uint4 *>(row + 4 * 128 + 16 * c) = rh;
+            *reinterpret_cast<uint4 *>(row + 5 * 128 + 16 * c) = nih;
+          } else {
+            const uint4 ih = pack8(xr, xi, 2, false), rh = pack8(xr, xi, 0, false);
+            *reinterpret_cast<uint4 *>(row + 0 * 128 + 16 * c) = ih;
+            *reinterpret_cast<uint4 *>(row + 1 * 128 + 16 * c) = rh;
+            *reinterpret_cast<uint4 *>(row + 2 * 128 + 16 * c) = pack8(xr, xi, 3, false);
+            *reinterpret_cast<uint4 *>(row + 3 * 128 + 16 * c) = pack8(xr, xi, 1, false);
+            *reinterpret_cast<uint4 *>(row + 4 * 128 + 16 * c) = ih;
+            *reinterpret_cast<uint4 *>(row + 5 * 128 + 16 * c) = rh;
+          }
         }
-      } else {
-        // U12 into the matrix: column J+jb+mr, rows J+n (pairs: jb is even)
-        z32 *dst = Am + (size_t)(J + jb + mr) * N + J;
-#pragma unroll
-        for (int j = 0; j < 16; j += 2)
-          if (n0 + j < jb)
-            *reinterpret_cast<float4 *>(dst + n0 + j) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
-        // k_split_b's rows: real [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo, Ur_hi, -Ui_hi],
-        //                   imaginary [Ui_hi, Ur_hi, Ui_lo, Ur_lo, Ui_hi, Ur_hi]
-        __nv_bfloat16 *rr = Bstage + ((size_t)b * 2 * Ncap + mr) * 6 * NB + n0;
-        __nv_bfloat16 *ri = Bstage + ((size_t)b * 2 * Ncap + Ncap + mr) * 6 * NB + n0;
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const uint4 xrh = chunk(rh, c, false), nih = chunk(ih, c, true), xih = chunk(ih, c, false);
-          *reinterpret_cast<uint4 *>(rr + 0 * NB + 8 * c) = xrh;
-          *reinterpret_cast<uint4 *>(rr + 1 * NB + 8 * c) = nih;
-          *reinterpret_cast<uint4 *>(rr + 2 * NB + 8 * c) = chunk(rl, c, false);
-          *reinterpret_cast<uint4 *>(rr + 3 * NB + 8 * c) = chunk(il, c, true);
-          *reinterpret_cast<uint4 *>(rr + 4 * NB + 8 * c) = xrh;
-          *reinterpret_cast<uint4 *>(rr + 5 * NB + 8 * c) = nih;
-          *reinterpret_cast<uint4 *>(ri + 0 * NB + 8 * c) = xih;
-          *reinterpret_cast<uint4 *>(ri + 1 * NB + 8 * c) = xrh;
-          *reinterpret_cast<uint4 *>(ri + 2 * NB + 8 * c) = chunk(il, c, false);
-          *reinterpret_cast<uint4 *>(ri + 3 * NB + 8 * c) = chunk(rl, c, false);
-          *reinterpret_cast<uint4 *>(ri + 4 * NB + 8 * c) = xih;
-          *reinterpret_cast<uint4 *>(ri + 5 * NB + 8 * c) = xrh;
-        }
+        __syncthreads();
+        copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (size_t)part * Ncap + m0) * 6 * NB, nv, t);
       }
     }
   }
@@ -700,6 +750,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   }
 }
 
+// ---------------------------------------------------------------------------
 // A[b][m][6*NB]: rows m = 0..Mrows-1 are matrix rows J+jb+m, k = 0..NB-1 (zero for k >= jb)
 __global__ void __launch_bounds__(256)
 k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB, __nv_bfloat16 *A,

@@ -15,7 +15,7 @@ from typing import Dict, Optional
 import numpy as np
 
 from . import _lib
-from ._lib import ADGA_FP64, ADGA_MIXED, Dims, Outputs, RunStats, ptr
+from ._lib import ADGA_FP64, ADGA_MIXED, Dims, Outputs, RunStats, Tune, TuneTrial, ptr
 
 PRECISION = {"fp64": ADGA_FP64, "mixed": ADGA_MIXED, ADGA_FP64: ADGA_FP64, ADGA_MIXED: ADGA_MIXED}
 
@@ -213,6 +213,33 @@ class Ladder:
         self.last_npts = n
         self.last_range = (qwstart, qwstop)
         return status, st.as_dict()
+
+    # ---- kernel choices of the mixed path ------------------------------
+    @property
+    def tune(self) -> Dict[str, int]:
+        """The mixed path's kernel choices (adga_get_tune): factor (0: FP32 LU
+        + FP64 refinement, 1: FP64 LU), pairs, tri_tc, batch."""
+        t = Tune()
+        self._check(self._lib.adga_get_tune(self._h, C.byref(t)), "get_tune")
+        return t.as_dict()
+
+    @tune.setter
+    def tune(self, cfg: Dict[str, int]):
+        t = Tune(**{**self.tune, **cfg})
+        self._check(self._lib.adga_set_tune(self._h, C.byref(t)), "set_tune")
+
+    def autotune(self, qwstart, qwstop, tol=1e-8):
+        """Measure the mixed path's configurations on points qwstart..qwstop
+        against the FP64 path and keep the fastest one within tol
+        (adga_autotune; resets the accumulators).  Returns (choice, trials)."""
+        trials = (TuneTrial * 16)()
+        n = C.c_int()
+        best = Tune()
+        self._check(self._lib.adga_autotune(self._h, int(qwstart), int(qwstop), float(tol), trials, 16,
+                                            C.byref(n), C.byref(best)), "autotune")
+        out = [dict(**trials[i].tune.as_dict(), ms=trials[i].ms, err=trials[i].err,
+                    accepted=bool(trials[i].accepted)) for i in range(n.value)]
+        return best.as_dict(), out
 
     def output_shapes(self, npts=None) -> Dict[str, tuple]:
         """Shapes of the accumulators get_outputs returns (npts: points of the run)."""

@@ -9,7 +9,9 @@ while a host thread builds the next point's inputs (H(k), G, the local
 vertex).  Per point: the mixed-precision ladder with the tangents of U and J
 in the same pass (`adga_ladder_run_tangent`), then, on the same handle, the
 FP64 ladder with the same tangents, which gives the per-point error of the
-mixed outputs and gradients.  Throughput counts mixed device time only.
+mixed outputs and gradients.  Throughput counts mixed device time only.  The
+mixed path's kernel choices come from the autotuner, measured once per
+(orbital count, BSE size) on the first point of that size and reused.
 
     python -m adga_b200.sweep [--points 64] [--omegas all|0] [--no-fp64] [--json FILE]
 """
@@ -69,18 +71,29 @@ def _run_pass(lad, prob, ranges, precision):
     return ms, iters, fallbacks, res
 
 
-def run_point(prepared, omegas, check_fp64=True, keep=False) -> Dict:
+def run_point(prepared, omegas, check_fp64=True, keep=False, tune_cache=None) -> Dict:
     """One parameter point: mixed ladder + tangents of U and J on the omega
     slices `omegas`, then (check_fp64) the FP64 pass; keep: also return the
-    mixed outputs (chi_dens, chi_magn per point, sigma, dchi_magn, dsigma)."""
+    mixed outputs (chi_dens, chi_magn per point, sigma, dchi_magn, dsigma).
+    tune_cache: dict of the mixed path's kernel choices per (ndim, N); a
+    missing entry is measured with the autotuner on the first omega slice."""
     prob, verts, tans = prepared
     s = prob.spec
     N = s.ndim ** 2 * 2 * s.iwf
     ranges = _ranges(s.nqp, s.iwb, omegas)
     npts = s.nqp * len(omegas)
+    tuned = None
     with Ladder.from_problem(prob) as lad:
         for iwb, (d, m) in verts.items():
             lad.set_vertex(iwb, d, m)
+        if tune_cache is not None:
+            key = (s.ndim, N)
+            if key not in tune_cache:
+                t0 = time.perf_counter()
+                best, trials = lad.autotune(*ranges[0])
+                tune_cache[key] = best
+                tuned = dict(choice=best, trials=trials, wall_s=time.perf_counter() - t0)
+            lad.tune = tune_cache[key]
         for dr, (dhk, du, dut, dv) in enumerate(tans):
             lad.set_tangent(dhk, du, dut, direction=dr)
             if dv:
@@ -88,7 +101,10 @@ def run_point(prepared, omegas, check_fp64=True, keep=False) -> Dict:
                     lad.set_vertex_tangent(iwb, a, b, direction=dr)
         ms, iters, fb, mx = _run_pass(lad, prob, ranges, "mixed")
         rec = dict(name=s.name, ndim=s.ndim, iwf=s.iwf, beta=s.beta, U=s.U, J=s.J, N=N, points=npts,
-                   ms_mixed=ms, pts_per_s=npts / (ms * 1e-3), max_refine_iters=iters, mixed_fallbacks=fb)
+                   ms_mixed=ms, pts_per_s=npts / (ms * 1e-3), max_refine_iters=iters, mixed_fallbacks=fb,
+                   tune=lad.tune)
+        if tuned:
+            rec["autotune"] = tuned
         if check_fp64:
             ms64, _, _, f64 = _run_pass(lad, prob, ranges, "fp64")
             rec["ms_fp64"] = ms64
@@ -103,19 +119,22 @@ def run_point(prepared, omegas, check_fp64=True, keep=False) -> Dict:
 
 
 def run_sweep(specs: Sequence, omegas: Optional[Sequence[int]] = None, check_fp64: bool = True,
-              log=None) -> Dict:
+              log=None, autotune: bool = True) -> Dict:
     """Run every parameter point (largest BSE dimension first); the next
-    point's host inputs are prepared while the current one runs."""
+    point's host inputs are prepared while the current one runs.  autotune:
+    the mixed path's kernel choices are measured once per (ndim, N) and
+    reused by every point of that size."""
     order = sorted(specs, key=lambda sp: -(sp.ndim ** 2 * 2 * sp.iwf))
     om = lambda sp: list(range(-sp.iwb, sp.iwb + 1)) if omegas is None else list(omegas)
     recs: List[Dict] = []
+    tune_cache = {} if autotune else None
     t0 = time.perf_counter()
     with cf.ThreadPoolExecutor(max_workers=1) as pool:
         nxt = pool.submit(_prepare, order[0], om(order[0])) if order else None
         for i, sp in enumerate(order):
             prepared = nxt.result()
             nxt = pool.submit(_prepare, order[i + 1], om(order[i + 1])) if i + 1 < len(order) else None
-            rec = run_point(prepared, om(sp), check_fp64)
+            rec = run_point(prepared, om(sp), check_fp64, tune_cache=tune_cache)
             recs.append(rec)
             if log:
                 log(rec)
@@ -124,7 +143,13 @@ def run_sweep(specs: Sequence, omegas: Optional[Sequence[int]] = None, check_fp6
     ms = sum(r["ms_mixed"] for r in recs)
     summary = dict(parameter_points=len(recs), qw_points=pts, ms_mixed=ms,
                    pts_per_s_device=pts / (ms * 1e-3) if ms else None, wall_s=wall,
-                   gradient=list(GRAD_PARAMS), precision="mixed")
+                   gradient=list(GRAD_PARAMS), precision="mixed",
+                   tune={f"ndim{k[0]}_N{k[1]}": v for k, v in (tune_cache or {}).items()},
+                   autotune_wall_s=sum(r["autotune"]["wall_s"] for r in recs if "autotune" in r))
+    if check_fp64 and recs:
+        ms64 = sum(r["ms_fp64"] for r in recs)
+        summary["ms_fp64"] = ms64
+        summary["mixed_over_fp64"] = ms64 / ms if ms else None
     if check_fp64 and recs:
         keys = recs[0]["err_vs_fp64"].keys()
         summary["max_err_vs_fp64"] = {k: max(r["err_vs_fp64"][k] for r in recs) for k in keys}
@@ -137,13 +162,14 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=4321)
     ap.add_argument("--omegas", default="all", help="'all' or comma-separated bosonic indices, e.g. 0")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 check pass")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel choices")
     ap.add_argument("--json", default=None, help="write the full record to this file")
     args = ap.parse_args(argv)
     specs = synth.sweep_specs(args.points, args.seed)
     omegas = None if args.omegas == "all" else [int(x) for x in args.omegas.split(",")]
     res = run_sweep(specs, omegas, not args.no_fp64,
                     log=lambda r: print(json.dumps({k: v for k, v in r.items() if k != "err_vs_fp64"}),
-                                        flush=True))
+                                        flush=True), autotune=not args.no_autotune)
     print(json.dumps(res["summary"]), flush=True)
     if args.json:
         with open(args.json, "w") as f:

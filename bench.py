@@ -54,6 +54,8 @@ def parse():
                     help="skip the gradient arm (ladder + tangents in U, J, t, mixed and FP64)")
     ap.add_argument("--cpu-points", type=int, default=0, help="CPU baseline sample (0 = one per core)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default kernel choices instead of tuning them on the first slice")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the oracle run over the whole omega = 0 slice (errors of both GPU arms "
                          "against the FP64 oracle for chi_d/m(q, omega) and Sigma(k, nu))")
@@ -360,6 +362,13 @@ def main():
             barrier()
         return allmax(ms), stats, clk.summary()
 
+    # kernel choices of the mixed path, measured on the first warm-up slice (set-up, untimed)
+    tuned = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        best, trials = lad.autotune(*slice_range(omegas[0]))
+        tuned = {"choice": best, "trials": trials, "sample": "the first warm-up omega slice",
+                 "wall_s": time.perf_counter() - t0}
     ms_mixed, st_mixed, clk = timed("mixed")
     v_mixed = world * npts * args.steps / (ms_mixed * 1e-3)
     res = {}
@@ -564,7 +573,7 @@ def main():
             "accuracy": acc, "stage_ms_per_step": stage, "fp64_stage_ms_per_step": stage64,
             "refine": {"max_iters": max(s["max_refine_iters"] for s in st_mixed),
                        "fallbacks": sum(s["mixed_fallbacks"] for s in st_mixed)},
-            "gradient": grad, "library_lu": library_lu, "full_grid": full_grid,
+            "gradient": grad, "library_lu": library_lu, "full_grid": full_grid, "autotune": tuned,
             "roofline": roof, "cpu_baseline": cpu_line, "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in st_mixed)),
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}

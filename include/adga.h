@@ -212,6 +212,43 @@ typedef struct adga_run_stats {
 int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
                     int *status, adga_run_stats *stats);
 
+/*
+ * Tunable choices of the ADGA_MIXED path, per handle, and the autotuner that
+ * picks them by measurement.  No counterpart in the reference (it has no GPU
+ * path); they select kernel variants, never the arithmetic's result beyond
+ * the mixed path's tolerance.
+ *   factor  0: complex FP32 LU with BF16x3 tensor-core updates and FP64
+ *              refinement; 1: the FP64 LU (no refinement), for sizes where
+ *              it is the faster way to the same accuracy
+ *   pairs   1: delayed two-step tensor-core updates (K = 128 per C pass);
+ *           0: one update per step (K = 64)
+ *   tri_tc  1: the L21 / U12 panel products on the tensor cores, writing the
+ *              update operands directly; 0: FP32 CUDA-core tile products and
+ *              separate operand-split kernels
+ *   batch   points per batch (0: as many as 60% of the free memory holds)
+ * A new handle starts at {0, 1, 1, 0} (the environment switches
+ * ADGA_NO_PAIRS, ADGA_TRI_TILE and ADGA_BATCH override it).
+ */
+typedef struct adga_tune {
+  int factor, pairs, tri_tc, batch;
+} adga_tune;
+typedef struct adga_tune_trial {
+  adga_tune tune;
+  double ms;        /* device time of the sample run (CUDA events)                 */
+  double err;       /* max relative difference of chi_d, chi_m, Sigma from FP64    */
+  int accepted;     /* err <= tol                                                   */
+} adga_tune_trial;
+int adga_set_tune(adga_handle *h, const adga_tune *t);
+int adga_get_tune(const adga_handle *h, adga_tune *t);
+/* Run the candidate configurations of the mixed path on the points
+ * qwstart..qwstop (each once to warm up, once timed), compare chi_qw_dens,
+ * chi_qw_magn and sigma_nl with the FP64 path on the same points, and keep on
+ * the handle the fastest configuration within tol (<= 0: 1e-8).  trials
+ * (room for max_trials, may be NULL) receives every measurement, *ntrials
+ * their count, *best the choice.  The accumulators are reset afterwards. */
+int adga_autotune(adga_handle *h, int qwstart, int qwstop, double tol, adga_tune_trial *trials,
+                  int max_trials, int *ntrials, adga_tune *best);
+
 /* Host copies of the accumulators; any pointer may be NULL. */
 typedef struct adga_outputs {
   adga_z *chi_qw_dens;     /* (ndim2, ndim2, qwstart:qwstop) of the last run   */

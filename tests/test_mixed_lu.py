@@ -1,9 +1,10 @@
 """The FP32 factorisation of the mixed path: without row interchanges (the
 default; the BSE matrices have growth factor ~1), with them
-(ADGA_MIXED_PIVOT=1), and the FP64 re-solve of points whose refinement does
-not converge (ADGA_MAX_REFINE=1 leaves every point unconverged); the
-refinement's two stopping rules: the bounded next correction (default) and a
-solved one (ADGA_REFINE_EXACT=1)."""
+(ADGA_MIXED_PIVOT=1), its panel products L21 / U12 on the tensor cores (the
+default) or as FP32 CUDA-core tiles (ADGA_TRI_TILE=1), and the FP64 re-solve
+of points whose refinement does not converge (ADGA_MAX_REFINE=1 leaves every
+point unconverged); the refinement's two stopping rules: the bounded next
+correction (default) and a solved one (ADGA_REFINE_EXACT=1)."""
 import pytest
 
 from adga_b200 import Ladder
@@ -35,6 +36,22 @@ def test_mixed_factorisation_matches_oracle(name, pivot):
     want = oracle_run(p)
     assert stats["mixed_fallbacks"] == 0 and not status.any()
     for k in ("chi_dens", "chi_magn", "sigma"):
+        assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
+
+
+@pytest.mark.parametrize("name", ["t3b", "t3m", "t2", "c3s"])
+@pytest.mark.parametrize("tri", ["tensor", "tile"])
+def test_panel_products_match_oracle(name, tri):
+    """L21 = A21 U11^-1 and U12 = L11^-1 A12 of every unpivoted step on the
+    tensor cores (k_tc_tri, writing the update operands itself) or as FP32
+    CUDA-core tiles with separate operand-split kernels: the same converged
+    outputs, N = 144 .. 320 (partial last steps included)."""
+    p = problem(name)
+    status, stats, got = run_mixed(p, {"ADGA_TRI_TILE": "1"} if tri == "tile" else {})
+    want = oracle_run(p)
+    assert stats["mixed_fallbacks"] == 0 and not status.any()
+    assert stats["max_refine_iters"] <= 3
+    for k in ("chi_dens", "chi_magn", "sigma", "chi_qw_magn"):
         assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
 
 

@@ -27,6 +27,10 @@ def test_sweep_runs_uneven_points_with_gradients():
     assert s["qw_points"] == sum(sp.nqp * (2 * sp.iwb + 1) for sp in specs)
     Ns = [r["N"] for r in res["points"]]
     assert Ns == sorted(Ns, reverse=True)                 # largest BSE dimension first
+    # kernel choices tuned once per (orbital count, BSE size), every point runs with its size's choice
+    assert set(s["tune"]) == {f"ndim{r['ndim']}_N{r['N']}" for r in res["points"]}
+    for r in res["points"]:
+        assert r["tune"] == s["tune"][f"ndim{r['ndim']}_N{r['N']}"]
     for r in res["points"]:
         assert r["mixed_fallbacks"] == 0
         for k, e in r["err_vs_fp64"].items():
