@@ -464,14 +464,13 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
 constexpr int TT_THREADS = 256;
 constexpr int TT_ROWS = 128;                       // tile rows (MMA M)
 constexpr int TT_KBLK = TT_ROWS * 128;             // one K block: 128 rows x 64 bf16
-constexpr int TT_WLD = 65;                         // padded column stride of the staged block inverse
-constexpr int TT_W_BYTES = 64 * TT_WLD * 8;        // 33,280 B
+constexpr int TT_OPER = 4 * TT_KBLK;               // A hi, A lo, B hi, B lo of one K half: 64 KB
 constexpr int TT_SROW = 784;                       // padded stride of a staged 768 B operand row
 constexpr int TT_FROW = 528;                       // padded stride of a staged 512 B matrix column
-constexpr int TT_SMEM_BYTES = 8 * TT_KBLK + TT_W_BYTES + 1024 + 64;
+constexpr int TT_SMEM_BYTES = TT_OPER + 1024 + 64;
 constexpr int TT_TMEM_COLS = 128;
-static_assert(TT_ROWS * TT_SROW <= 8 * TT_KBLK && TT_ROWS * TT_FROW <= 8 * TT_KBLK,
-              "the epilogue staging reuses the operand buffers");
+static_assert(64 * TT_SROW <= TT_OPER && 64 * TT_FROW <= TT_OPER,
+              "the epilogue stages 64 rows at a time in the operand buffers");
 // kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
 constexpr uint32_t IDESC_N128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 / 8) << 17) |
                                 ((uint32_t)(TT_ROWS / 16) << 24);
@@ -490,30 +489,21 @@ __device__ __forceinline__ uint32_t sw128(int r, int c) {
 __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
   return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
 }
-// 8 consecutive K values of one row -> the four K blocks (re hi, im hi, re lo, im lo), chunk c
-__device__ __forceinline__ void put_chunk(unsigned char *base, int r, int c, const float2 *v, bool neg_im,
-                                          bool swap) {
-  uint32_t w[4][4];
+// 8 consecutive K values of one row -> chunk c of the hi block (at base) and of the lo block
+// (at base + TT_KBLK), scaled by sgn
+__device__ __forceinline__ void put8(unsigned char *base, int r, int c, const float *x, float sgn) {
+  uint32_t hw[4], lw[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    __nv_bfloat16 h[4][2];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      float re = v[2 * j + u].x, im = v[2 * j + u].y;
-      if (neg_im) im = -im;
-      if (swap) { const float x = re; re = im; im = x; }
-      __nv_bfloat16 rh, rl, ih, il;
-      split2(re, rh, rl);
-      split2(im, ih, il);
-      h[0][u] = rh; h[1][u] = ih; h[2][u] = rl; h[3][u] = il;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) w[q][j] = pack_bf16(h[q][0], h[q][1]);
+  for (int u = 0; u < 4; ++u) {
+    __nv_bfloat16 h0, l0, h1, l1;
+    split2(sgn * x[2 * u], h0, l0);
+    split2(sgn * x[2 * u + 1], h1, l1);
+    hw[u] = pack_bf16(h0, h1);
+    lw[u] = pack_bf16(l0, l1);
   }
   const uint32_t off = sw128(r, c);
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-    *reinterpret_cast<uint4 *>(base + q * TT_KBLK + off) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+  *reinterpret_cast<uint4 *>(base + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+  *reinterpret_cast<uint4 *>(base + TT_KBLK + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
 }
 // 8 bf16 of the values x[0..7] (split part `part`: 0 re hi, 1 re lo, 2 im hi, 3 im lo), negated when neg
 __device__ __forceinline__ uint4 pack8(const float *re, const float *im, int part, bool neg) {
@@ -542,18 +532,22 @@ __device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat1
   }
 }
 
-__global__ void __launch_bounds__(TT_THREADS, 1)
+// Panel products (see the block comment above).  The complex product
+// [Cr | Ci] = Xr [Wr | Wi] + Xi [-Wi | Wr] runs as two MMA phases over the
+// real and the imaginary part of X (64 KB of operands at a time, so three
+// CTAs share an SM and the load, MMA and store phases of different tiles
+// overlap); the epilogue stages 64 tile rows at a time.
+__global__ void __launch_bounds__(TT_THREADS, 3)
 k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
          const z32 *Uinv, __nv_bfloat16 *Astage, __nv_bfloat16 *Bstage, int Ncap, int b0, int ntA, int ntU,
          int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
-  unsigned char *gA = smraw + (sbase - smem_u32(smraw));
-  unsigned char *gB = gA + 4 * TT_KBLK;
-  z32 *Wsh = reinterpret_cast<z32 *>(gA + 8 * TT_KBLK);            // [64][TT_WLD]
-  uint64_t *bar = reinterpret_cast<uint64_t *>(gA + 8 * TT_KBLK + TT_W_BYTES);
+  unsigned char *gA = smraw + (sbase - smem_u32(smraw));    // A hi, A lo, B hi, B lo
+  unsigned char *gB = gA + 2 * TT_KBLK;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(gA + TT_OPER);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
-  const uint32_t sA = sbase, sB = sbase + 4 * TT_KBLK, sbar = smem_u32(bar);
+  const uint32_t sA = sbase, sB = sbase + 2 * TT_KBLK, sbar = smem_u32(bar);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int per = ntA + ntU;
   const int b = b0 + blockIdx.x / per, tile = blockIdx.x % per;
@@ -562,16 +556,8 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   const int nrows = lower ? N - J - jb : ncols - J - jb;
   const int nv = min(TT_ROWS, nrows - m0);             // valid rows of the tile
   z32 *Am = M + (size_t)b * strideM;
+  const z32 *W = (lower ? Uinv : Linv) + ((size_t)b * nsteps + J / NB) * NB * NB;
 
-  // the block inverse W (U11^-1, or L11^-1 for mode 1) into shared memory, coalesced
-  {
-    const z32 *W = (lower ? Uinv : Linv) + ((size_t)b * nsteps + J / NB) * NB * NB;
-    for (int e = t; e < 64 * 64; e += TT_THREADS) {
-      const uint32_t d = smem_u32(Wsh + (e & 63) + (e >> 6) * TT_WLD);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(W + e));
-    }
-    asm volatile("cp.async.commit_group;");
-  }
   if (t == 0) {
     mbar_init(sbar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -581,164 +567,204 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
                  "r"(TT_TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-
-  // ---- A operand: the tile, 128 rows x 64 K (zero outside the matrix / beyond jb)
-  {
-    float2 v[32];
-    int r, kh;
-    if (lower) {
-      // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
-      r = t & 127;
-      kh = t >> 7;
-      const bool rv = r < nv;
-      const z32 *src = Am + (size_t)(J + jb + m0 + r);
-#pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        const int k = kh * 32 + i;
-        v[i] = (rv && k < jb) ? src[(size_t)(J + k) * N] : make_float2(0.f, 0.f);
-      }
-    } else {
-      // columns J+jb+m0+r, rows J+k: two threads per column, 256 contiguous bytes each
-      r = t >> 1;
-      kh = t & 1;
-      const bool rv = r < nv;
-      const z32 *src = Am + (size_t)(J + jb + m0 + r) * N + J;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int k = kh * 32 + 2 * i;            // jb is even: k, k+1 are both in or both out
-        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (rv && k < jb) q = *reinterpret_cast<const float4 *>(src + k);
-        v[2 * i] = make_float2(q.x, q.y);
-        v[2 * i + 1] = make_float2(q.z, q.w);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) put_chunk(gA, r, kh * 4 + j, v + 8 * j, false, false);
-  }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
-  __syncthreads();
-  // ---- B operand from W: real-part row n [Wr(:, n) | -Wi(:, n)], imaginary-part row
-  //      64 + n [Wi(:, n) | Wr(:, n)]; mode 0: W(k, n) = U11^-1(k, n), mode 1: L11^-1(n, k)
-  {
-    const int n = t & 63, kq = t >> 6;            // K values kq*16 .. kq*16+15 of column n
-    float2 w[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int k = kq * 16 + i;
-      w[i] = lower ? Wsh[k + n * TT_WLD] : Wsh[n + k * TT_WLD];
-    }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      put_chunk(gB, n, kq * 2 + j, w + 8 * j, true, false);        // [Wr | -Wi]
-      put_chunk(gB, 64 + n, kq * 2 + j, w + 8 * j, false, true);   // [Wi | Wr]
-    }
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tslot;
 
-  if (t == 32) {
-    // (hi, hi), (hi, lo), (lo, hi): K blocks {0,1} are the hi parts, {2,3} the lo parts
-    const int ap[3] = {0, 0, 2}, bp[3] = {0, 2, 0};
+  bool ok = true;
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    if (h == 1) {
+      // the phase-0 MMAs must have read the operands before they are overwritten
+      ok = __syncthreads_and(mbar_wait(sbar, 0, err, 21));
+      if (!ok) break;
+    }
+    // ---- A operand: part h (0 real, 1 imaginary) of the tile, 128 rows x 64 K, hi and lo
+    if (lower) {
+      // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
+      const int r = t & 127, kh = t >> 7;
+      const z32 *src = Am + (size_t)(J + jb + m0 + r);
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) {
+        float x[8];
 #pragma unroll
-    for (int term = 0; term < 3; ++term)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const uint32_t a = sA + (ap[term] + j / 4) * TT_KBLK + (j % 4) * 32;
-        const uint32_t bb = sB + (bp[term] + j / 4) * TT_KBLK + (j % 4) * 32;
-        mma_bf16_n128(tmem, smem_desc(a), smem_desc(bb), (term > 0 || j > 0) ? 1u : 0u);
+        for (int i = 0; i < 8; ++i) {
+          const int k = kh * 32 + q * 8 + i;
+          const z32 v = (r < nv && k < jb) ? src[(size_t)(J + k) * N] : make_float2(0.f, 0.f);
+          x[i] = h ? v.y : v.x;
+        }
+        put8(gA, r, kh * 4 + q, x, 1.f);
       }
-    mma_commit(sbar);
+    } else {
+      // columns J+jb+m0+r, rows J+k: two threads per column, 256 contiguous bytes each
+      const int r = t >> 1, kh = t & 1;
+      const z32 *src = Am + (size_t)(J + jb + m0 + r) * N + J;
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) {
+        float x[8];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int k = kh * 32 + q * 8 + 2 * i;  // jb is even: k, k+1 are both in or both out
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (r < nv && k < jb) v = *reinterpret_cast<const float4 *>(src + k);
+          x[2 * i] = h ? v.y : v.x;
+          x[2 * i + 1] = h ? v.w : v.z;
+        }
+        put8(gA, r, kh * 4 + q, x, 1.f);
+      }
+    }
+    // ---- B operand: rows n (real part of the output) and 64 + n (imaginary part):
+    //      phase 0 [Wr(:, n)], [Wi(:, n)]; phase 1 [-Wi(:, n)], [Wr(:, n)];
+    //      mode 0 W(k, n) = U11^-1(k, n), mode 1 W(k, n) = L11^-1(n, k)
+    {
+      const int n = t & 63, kq = t >> 6;          // K values kq*16 .. kq*16+15 of column n
+#pragma unroll 1
+      for (int j = 0; j < 2; ++j) {
+        float wr[8], wi[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int k = kq * 16 + j * 8 + i;
+          const z32 w = lower ? W[k + n * NB] : W[n + k * NB];
+          wr[i] = w.x;
+          wi[i] = w.y;
+        }
+        put8(gB, n, kq * 2 + j, h ? wi : wr, h ? -1.f : 1.f);
+        put8(gB, 64 + n, kq * 2 + j, h ? wr : wi, 1.f);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (t == 32) {
+      // (hi, hi), (hi, lo), (lo, hi) over this K half
+#pragma unroll
+      for (int term = 0; term < 3; ++term)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t a = sA + (term == 2 ? TT_KBLK : 0) + 32 * k;
+          const uint32_t bb = sB + (term == 1 ? TT_KBLK : 0) + 32 * k;
+          mma_bf16_n128(tmem, smem_desc(a), smem_desc(bb), (h > 0 || term > 0 || k > 0) ? 1u : 0u);
+        }
+      mma_commit(sbar);
+    }
   }
+  // CTA-uniform: the epilogue below has block barriers
+  if (ok) ok = __syncthreads_and(mbar_wait(sbar, 1, err, 22));
+  asm volatile("tcgen05.fence::after_thread_sync;");
 
   // ---- epilogue: warp w reads TMEM lanes 32 (w % 4).. (tile rows) and output columns
   //      32 (w / 4) .. + 31; the results reach global memory through shared memory (the
-  //      operand buffers, free once the MMAs completed) so that every store is coalesced
-  // CTA-uniform: the epilogue below has block barriers
-  const bool ok = __syncthreads_and(mbar_wait(sbar, 0, err, 21));
-  asm volatile("tcgen05.fence::after_thread_sync;");
+  //      operand buffers, free once the MMAs completed), 64 tile rows per round, so that
+  //      every store is coalesced
   if (ok) {
     const int quad = warp & 3, half = warp >> 2;
     const int r = quad * 32 + lane;
     const int n0 = half * 32;
-    float re[32], im[32];
-    {
-      const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)n0;
-      tmem_ld16(tl, *reinterpret_cast<float(*)[16]>(re));
-      tmem_ld16(tl + 16, *reinterpret_cast<float(*)[16]>(re + 16));
-      tmem_ld16(tl + 64, *reinterpret_cast<float(*)[16]>(im));
-      tmem_ld16(tl + 80, *reinterpret_cast<float(*)[16]>(im + 16));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    }
     unsigned char *stg = gA;
+    const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)n0;
+    // the thread's 32 output values of part `piece` (16 columns each), re then im
+    auto tload = [&](int piece, float (&re)[16], float (&im)[16]) {
+      tmem_ld16(tl + 16 * piece, re);
+      tmem_ld16(tl + 64 + 16 * piece, im);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    };
     if (lower) {
-      // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
-      if (r < nv) {
-        z32 *dst = Am + (size_t)(J + jb + m0 + r);
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-          if (n0 + j < jb) dst[(size_t)(J + n0 + j) * N] = make_float2(re[j], im[j]);
-      }
-      // k_split_a's rows [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
-      unsigned char *row = stg + r * TT_SROW + n0 * 2;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const uint4 rh = pack8(re + 8 * c, im + 8 * c, 0, false), ih = pack8(re + 8 * c, im + 8 * c, 2, false);
-        *reinterpret_cast<uint4 *>(row + 0 * 128 + 16 * c) = rh;
-        *reinterpret_cast<uint4 *>(row + 1 * 128 + 16 * c) = ih;
-        *reinterpret_cast<uint4 *>(row + 2 * 128 + 16 * c) = rh;
-        *reinterpret_cast<uint4 *>(row + 3 * 128 + 16 * c) = ih;
-        *reinterpret_cast<uint4 *>(row + 4 * 128 + 16 * c) = pack8(re + 8 * c, im + 8 * c, 1, false);
-        *reinterpret_cast<uint4 *>(row + 5 * 128 + 16 * c) = pack8(re + 8 * c, im + 8 * c, 3, false);
-      }
-      __syncthreads();
-      copy_rows(stg, Astage + ((size_t)b * N + m0) * 6 * NB, nv, t);
-    } else {
-      // U12 (column J+jb+m0+r, rows J..J+jb): the tile's columns staged, then 512 B per column
-      {
-        unsigned char *col = stg + r * TT_FROW + n0 * 8;
-#pragma unroll
-        for (int j = 0; j < 32; j += 2)
-          *reinterpret_cast<float4 *>(col + j * 8) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
-      }
-      __syncthreads();
-      const int pc = jb / 2;                       // 16-byte pieces of a column (jb is even)
-      for (int e = t; e < nv * pc; e += TT_THREADS) {
-        const int cc = e / pc, pp = e % pc;
-        *reinterpret_cast<float4 *>(Am + (size_t)(J + jb + m0 + cc) * N + J + 2 * pp) =
-            *reinterpret_cast<const float4 *>(stg + cc * TT_FROW + pp * 16);
-      }
-      // k_split_b's rows: real [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo, Ur_hi, -Ui_hi],
-      //                   imaginary [Ui_hi, Ur_hi, Ui_lo, Ur_lo, Ui_hi, Ur_hi]
 #pragma unroll 1
-      for (int part = 0; part < 2; ++part) {
-        __syncthreads();
-        unsigned char *row = stg + r * TT_SROW + n0 * 2;
+      for (int rnd = 0; rnd < 2; ++rnd) {
+        if (rnd) __syncthreads();
+        if ((quad >> 1) == rnd) {
+          unsigned char *row = stg + (r - 64 * rnd) * TT_SROW + n0 * 2;
+#pragma unroll 1
+          for (int piece = 0; piece < 2; ++piece) {
+            float re[16], im[16];
+            tload(piece, re, im);
+            // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
+            if (r < nv) {
+              z32 *dst = Am + (size_t)(J + jb + m0 + r);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const float *xr = re + 8 * c, *xi = im + 8 * c;
-          if (part == 0) {
-            const uint4 rh = pack8(xr, xi, 0, false), nih = pack8(xr, xi, 2, true);
-            *reinterpret_cast<uint4 *>(row + 0 * 128 + 16 * c) = rh;
-            *reinterpret_cast<uint4 *>(row + 1 * 128 + 16 * c) = nih;
-            *reinterpret_cast<uint4 *>(row + 2 * 128 + 16 * c) = pack8(xr, xi, 1, false);
-            *reinterpret_cast<uint4 *>(row + 3 * 128 + 16 * c) = pack8(xr, xi, 3, true);
-            *reinterpret_cast<uint4 *>(row + 4 * 128 + 16 * c) = rh;
-            *reinterpret_cast<uint4 *>(row + 5 * 128 + 16 * c) = nih;
-          } else {
-            const uint4 ih = pack8(xr, xi, 2, false), rh = pack8(xr, xi, 0, false);
-            *reinterpret_cast<uint4 *>(row + 0 * 128 + 16 * c) = ih;
-            *reinterpret_cast<uint4 *>(row + 1 * 128 + 16 * c) = rh;
-            *reinterpret_cast<uint4 *>(row + 2 * 128 + 16 * c) = pack8(xr, xi, 3, false);
-            *reinterpret_cast<uint4 *>(row + 3 * 128 + 16 * c) = pack8(xr, xi, 1, false);
-            *reinterpret_cast<uint4 *>(row + 4 * 128 + 16 * c) = ih;
-            *reinterpret_cast<uint4 *>(row + 5 * 128 + 16 * c) = rh;
+              for (int j = 0; j < 16; ++j)
+                if (n0 + 16 * piece + j < jb)
+                  dst[(size_t)(J + n0 + 16 * piece + j) * N] = make_float2(re[j], im[j]);
+            }
+            // k_split_a's rows [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const int o = 32 * piece + 16 * c;
+              const uint4 rh = pack8(re + 8 * c, im + 8 * c, 0, false), ih = pack8(re + 8 * c, im + 8 * c, 2, false);
+              *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = rh;
+              *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = ih;
+              *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = rh;
+              *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = ih;
+              *reinterpret_cast<uint4 *>(row + 4 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 1, false);
+              *reinterpret_cast<uint4 *>(row + 5 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 3, false);
+            }
           }
         }
         __syncthreads();
-        copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (size_t)part * Ncap + m0) * 6 * NB, nv, t);
+        copy_rows(stg, Astage + ((size_t)b * N + m0 + 64 * rnd) * 6 * NB, min(64, nv - 64 * rnd), t);
+      }
+    } else {
+      const int pc = jb / 2;                       // 16-byte pieces of a U12 column (jb is even)
+      // rounds 0, 1: U12 columns (rows 64 rnd ..); 2..5: k_split_b's real rows [Ur_hi, -Ui_hi,
+      // Ur_lo, -Ui_lo, Ur_hi, -Ui_hi] and imaginary rows [Ui_hi, Ur_hi, Ui_lo, Ur_lo, Ui_hi, Ur_hi]
+#pragma unroll 1
+      for (int rnd = 0; rnd < 6; ++rnd) {
+        const int rh64 = rnd & 1;                  // tile rows 64 rh64 .. 64 rh64 + 63
+        if (rnd) __syncthreads();
+        if ((quad >> 1) == rh64) {
+          const int rr = r - 64 * rh64;
+#pragma unroll 1
+          for (int piece = 0; piece < 2; ++piece) {
+            float re[16], im[16];
+            tload(piece, re, im);
+            const int nn = n0 + 16 * piece;
+            if (rnd < 2) {
+              unsigned char *col = stg + rr * TT_FROW + nn * 8;
+#pragma unroll
+              for (int j = 0; j < 16; j += 2)
+                *reinterpret_cast<float4 *>(col + j * 8) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
+            } else {
+              unsigned char *row = stg + rr * TT_SROW + nn * 2;
+              const bool imag = rnd >= 4;
+#pragma unroll
+              for (int c = 0; c < 2; ++c) {
+                const float *xr = re + 8 * c, *xi = im + 8 * c;
+                const int o = 16 * c;
+                if (!imag) {
+                  const uint4 a = pack8(xr, xi, 0, false), nb = pack8(xr, xi, 2, true);
+                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = a;
+                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = nb;
+                  *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 1, false);
+                  *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 3, true);
+                  *reinterpret_cast<uint4 *>(row + 4 * 128 + o) = a;
+                  *reinterpret_cast<uint4 *>(row + 5 * 128 + o) = nb;
+                } else {
+                  const uint4 a = pack8(xr, xi, 2, false), bb = pack8(xr, xi, 0, false);
+                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = a;
+                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = bb;
+                  *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 3, false);
+                  *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 1, false);
+                  *reinterpret_cast<uint4 *>(row + 4 * 128 + o) = a;
+                  *reinterpret_cast<uint4 *>(row + 5 * 128 + o) = bb;
+                }
+              }
+            }
+          }
+        }
+        __syncthreads();
+        const int nrw = min(64, nv - 64 * rh64);
+        if (rnd < 2) {
+          for (int e = t; e < nrw * pc; e += TT_THREADS) {
+            const int cc = e / pc, pp = e % pc;
+            *reinterpret_cast<float4 *>(Am + (size_t)(J + jb + m0 + 64 * rh64 + cc) * N + J + 2 * pp) =
+                *reinterpret_cast<const float4 *>(stg + cc * TT_FROW + pp * 16);
+          }
+        } else {
+          copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (rnd >= 4 ? (size_t)Ncap : 0) + m0 + 64 * rh64) * 6 * NB,
+                    nrw, t);
+        }
       }
     }
   }

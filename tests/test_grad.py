@@ -86,3 +86,61 @@ def test_vjp_matches_oracle_dense_jacobian():
         v = np.concatenate([vc.ravel(), vs.ravel()])
         want = np.real(np.conj(v) @ jac)
         assert rel_err(g.numpy(), want) < 1e-6, (g.numpy(), want)
+
+
+class SplitModel:
+    """A caller model: the synthetic couplings (U, J), the hopping scale t and
+    on-site shifts d_a of the first orbitals (H_aa(k) += d_a).  Its input
+    tangents: the synthetic model's for U, J, t; dH/dd_a = E_aa for the shifts."""
+
+    def __init__(self, base, nshift):
+        self.base, self.nshift = base, nshift
+
+    def problem(self, theta):
+        import dataclasses
+        s = self.base.spec
+        p = synth.perturbed_problem(self.base, dU=theta[0] - s.U, dJ=theta[1] - s.J, dt=theta[2] - s.hop["t"])
+        hk = p.hk.copy(order="F")
+        for a in range(self.nshift):
+            hk[a, a, :] += theta[3 + a]
+        return dataclasses.replace(p, hk=hk, _vcache={})
+
+    def tangents(self, theta, i):
+        if i < 3:
+            return synth.tangent_inputs(self.problem(theta), synth.PARAMS[i])
+        p = self.base
+        dhk = np.zeros_like(p.hk, order="F")
+        dhk[i - 3, i - 3, :] = 1.0
+        return dhk, None, None, None
+
+
+@pytest.mark.parametrize("nshift", [1, 2])
+def test_caller_model_gradient_matches_finite_differences(nshift):
+    """ladder_outputs with a caller's model and its own input tangents: 4 or 5
+    parameters (the latter in two tangent passes), every output of the full
+    grid in a scalar loss, against central differences of the loss."""
+    from adga_b200.grad import ladder_outputs
+    p = problem("t2")
+    model = SplitModel(p, nshift)
+    s = p.spec
+    theta = torch.tensor([s.U, s.J, s.hop["t"]] + [0.01 * (a + 1) for a in range(nshift)],
+                         dtype=torch.float64, requires_grad=True)
+    rng = np.random.default_rng(3)
+    chi_d, chi_m, sig = ladder_outputs(theta, model)
+    w = [torch.from_numpy(rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+         for x in (chi_d, chi_m, sig)]
+
+    def loss(*ys):
+        return sum((wi * y).real.sum() + (y.abs() ** 2).sum() for wi, y in zip(w, ys))
+
+    loss(chi_d, chi_m, sig).backward()
+    want = []
+    with torch.no_grad():
+        for i in range(len(theta)):
+            e = torch.zeros(len(theta), dtype=torch.float64)
+            e[i] = H
+            lp = loss(*ladder_outputs(theta.detach() + e, model))
+            lm = loss(*ladder_outputs(theta.detach() - e, model))
+            want.append(float((lp - lm) / (2 * H)))
+    got = theta.grad.numpy()
+    assert np.max(np.abs(got - want)) < 1e-6 * max(1.0, np.max(np.abs(want))), (got, want)
