@@ -534,10 +534,10 @@ __device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat1
 
 // Panel products (see the block comment above).  The complex product
 // [Cr | Ci] = Xr [Wr | Wi] + Xi [-Wi | Wr] runs as two MMA phases over the
-// real and the imaginary part of X (64 KB of operands at a time, so three
+// real and the imaginary part of X (64 KB of operands at a time, so two
 // CTAs share an SM and the load, MMA and store phases of different tiles
 // overlap); the epilogue stages 64 tile rows at a time.
-__global__ void __launch_bounds__(TT_THREADS, 3)
+__global__ void __launch_bounds__(TT_THREADS, 2)
 k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
          const z32 *Uinv, __nv_bfloat16 *Astage, __nv_bfloat16 *Bstage, int Ncap, int b0, int ntA, int ntU,
          int *err) {
@@ -572,6 +572,44 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tslot;
 
+  // ---- the tile, 128 rows x 64 K (zero outside the matrix / beyond jb), loaded once with all of
+  //      a thread's loads in flight: real parts feed phase 0, imaginary parts (kept) phase 1
+  float xi[32];
+  int ar, akh;
+  {
+    float xr[32];
+    if (lower) {
+      // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
+      ar = t & 127;
+      akh = t >> 7;
+      const z32 *src = Am + (size_t)(J + jb + m0 + ar);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int k = akh * 32 + i;
+        const z32 v = (ar < nv && k < jb) ? src[(size_t)(J + k) * N] : make_float2(0.f, 0.f);
+        xr[i] = v.x;
+        xi[i] = v.y;
+      }
+    } else {
+      // columns J+jb+m0+r, rows J+k: two threads per column, 256 contiguous bytes each
+      ar = t >> 1;
+      akh = t & 1;
+      const z32 *src = Am + (size_t)(J + jb + m0 + ar) * N + J;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int k = akh * 32 + 2 * i;            // jb is even: k, k+1 are both in or both out
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ar < nv && k < jb) v = *reinterpret_cast<const float4 *>(src + k);
+        xr[2 * i] = v.x;
+        xi[2 * i] = v.y;
+        xr[2 * i + 1] = v.z;
+        xi[2 * i + 1] = v.w;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) put8(gA, ar, akh * 4 + q, xr + 8 * q, 1.f);
+  }
+
   bool ok = true;
 #pragma unroll 1
   for (int h = 0; h < 2; ++h) {
@@ -579,40 +617,9 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       // the phase-0 MMAs must have read the operands before they are overwritten
       ok = __syncthreads_and(mbar_wait(sbar, 0, err, 21));
       if (!ok) break;
-    }
-    // ---- A operand: part h (0 real, 1 imaginary) of the tile, 128 rows x 64 K, hi and lo
-    if (lower) {
-      // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
-      const int r = t & 127, kh = t >> 7;
-      const z32 *src = Am + (size_t)(J + jb + m0 + r);
-#pragma unroll 1
-      for (int q = 0; q < 4; ++q) {
-        float x[8];
+      // ---- A operand of phase 1: the imaginary part of the tile
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int k = kh * 32 + q * 8 + i;
-          const z32 v = (r < nv && k < jb) ? src[(size_t)(J + k) * N] : make_float2(0.f, 0.f);
-          x[i] = h ? v.y : v.x;
-        }
-        put8(gA, r, kh * 4 + q, x, 1.f);
-      }
-    } else {
-      // columns J+jb+m0+r, rows J+k: two threads per column, 256 contiguous bytes each
-      const int r = t >> 1, kh = t & 1;
-      const z32 *src = Am + (size_t)(J + jb + m0 + r) * N + J;
-#pragma unroll 1
-      for (int q = 0; q < 4; ++q) {
-        float x[8];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int k = kh * 32 + q * 8 + 2 * i;  // jb is even: k, k+1 are both in or both out
-          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (r < nv && k < jb) v = *reinterpret_cast<const float4 *>(src + k);
-          x[2 * i] = h ? v.y : v.x;
-          x[2 * i + 1] = h ? v.w : v.z;
-        }
-        put8(gA, r, kh * 4 + q, x, 1.f);
-      }
+      for (int q = 0; q < 4; ++q) put8(gA, ar, akh * 4 + q, xi + 8 * q, 1.f);
     }
     // ---- B operand: rows n (real part of the output) and 64 + n (imaginary part):
     //      phase 0 [Wr(:, n)], [Wi(:, n)]; phase 1 [-Wi(:, n)], [Wr(:, n)];
