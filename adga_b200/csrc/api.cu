@@ -115,7 +115,9 @@ struct adga_handle {
   bool refine_estimate = true;   // stop on the bounded next correction (ADGA_REFINE_EXACT=1: on a solved one)
   bool mixed_nopiv = true;   // FP32 factorisation without row interchanges (ADGA_MIXED_PIVOT=1: with)
   double tol = 1e-10;   // stop when max|dX| <= tol * max|X| (the error is then far below)
-  adga_tune tune{0, 1, 1, 0};   // mixed-path kernel choices (adga_set_tune / adga_autotune)
+  adga_tune tune{0, 1, 1, 0, 1};   // mixed-path kernel choices (adga_set_tune / adga_autotune)
+  void *ri8 = nullptr;            // int8-slice residual context (k_resid_i8.cu), with the mixed work
+  long long frow_gen = 0;         // bumped whenever F~ is recomputed (its residual slices go stale)
   // last-run statistics
   adga_run_stats stats{};
 };
@@ -311,6 +313,7 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   if (const char *re = getenv("ADGA_REFINE_EXACT")) h->refine_estimate = atoi(re) == 0;
   if (getenv("ADGA_NO_PAIRS")) h->tune.pairs = 0;
   if (getenv("ADGA_TRI_TILE")) h->tune.tri_tc = 0;
+  if (getenv("ADGA_RESID_FP64")) h->tune.resid = 0;
   const char *ev = getenv("ADGA_NB");
   if (ev) h->NB = std::max(16, std::min(64, atoi(ev) / 8 * 8));   // the LU kernels assume NB <= 64
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -385,6 +388,7 @@ extern "C" int adga_destroy(adga_handle *h) {
   if (!h) return 0;
   if (h->st) cudaStreamSynchronize(h->st);
   if (h->tc) tc_trail_free(h->tc);
+  if (h->ri8) ri8_free(h->ri8);
   free_list(h->work);
   free_list(h->owned);
   for (auto p : h->vd) if (p) cudaFree(p);
@@ -644,6 +648,7 @@ static int ensure_local(adga_handle *h, int iwb) {
   CK(launch_local_F(h->c, h->vd[w], h->c0inv, h->Frow_d, h->st));
   CK(launch_local_F(h->c, h->vm[w], h->c0inv, h->Frow_m, h->st));
   h->f32_iwb = INT_MIN;
+  ++h->frow_gen;
   if (h->tl_d[w]) {
     // external three-leg vertex (src/main.F90:560-561), then 1 + gamma^w
     const size_t ng = (size_t)h->c.nd2 * h->c.N;
@@ -671,6 +676,7 @@ static size_t bytes_per_point(const adga_handle *h, int prec, int NB) {
   } else {
     b += 2 * N * (N + R) * 8 + 2 * 2 * nsteps * NB * NB * 8;
     b += 2 * 2 * R * N * 16 + 2 * R * N * 8 + 2 * ((R + 15) / 16) * 16 * N * 8 + 2 * N * 4 + 64;
+    b += 2 * 7 * R * ((2 * N + 63) / 64 * 64) + 2 * R * 4;   // int8 residual slices and scales
   }
   return b;
 }
@@ -681,6 +687,7 @@ static int ensure_work(adga_handle *h, int prec, int want) {
   if (h->cap_prec == prec && h->cap >= want && (h->tune.batch <= 0 || h->cap <= h->tune.batch)) return 0;
   cudaStreamSynchronize(h->st);
   if (h->tc) { tc_trail_free(h->tc); h->tc = nullptr; }
+  if (h->ri8) { ri8_free(h->ri8); h->ri8 = nullptr; }
   free_list(h->work);
   h->cap = 0;
   h->cap_prec = -1;
@@ -732,6 +739,8 @@ static int ensure_work(adga_handle *h, int prec, int want) {
   if (prec == ADGA_MIXED && tc_available() && !getenv("ADGA_NO_TC")) {
     LUBatch lb{(int)N, (int)(N + R), 2 * cap, NB, N * (N + R), h->ipiv, h->info, h->Linv, h->Uinv, h->rmap};
     if (tc_trail_setup(&h->tc, (z32 *)h->Tm, lb, h->st) != cudaSuccess) h->tc = nullptr;
+    // the int8-slice residual (its slices and maps for this batch size)
+    if (ri8_setup(&h->ri8, (int)N, (int)R, cap) != cudaSuccess) h->ri8 = nullptr;
   }
   return 0;
 }
@@ -987,7 +996,7 @@ static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 
     CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
     CK(cudaMemsetAsync(rnorm, 0, sizeof(unsigned long long) * nmat, st));
     CK(launch_residual(c, np, dX, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, h->XD, h->V32,
-                       nullptr, rnorm, st, r));
+                       nullptr, rnorm, st, r, h->tune.resid ? h->ri8 : nullptr, h->frow_gen));
     if (it > 0 && h->refine_estimate) {
       CK(cudaMemcpyAsync(nh.data() + 2 * nmat, rnorm, sizeof(unsigned long long) * nmat, cudaMemcpyDeviceToHost,
                          st));
@@ -1227,7 +1236,8 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
         CK(launch_vq_resid_extra(c, np, h->qidx_d, h->X64, chi0q, h->opg_d, extra, st));
       }
       CK(launch_residual(c, np, h->X64, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m,
-                         h->XD, h->V32, extra, rnorm, st));
+                         h->XD, h->V32, extra, rnorm, st, nullptr, h->tune.resid ? h->ri8 : nullptr,
+                         h->frow_gen));
       if (it > 0 && h->refine_estimate) {
         // after a correction: its successor d = r A^-1 is bounded by kEstSafety * rho * max|r|,
         // rho = max|d_1| / max|r_1| of the first sweep (the solve's amplification, at least 1);
@@ -1302,6 +1312,8 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
   CK(cudaStreamSynchronize(st));
   if (prec == ADGA_MIXED && h->tc && tc_trail_error(h->tc))
     return fail(h, ADGA_ETIMEOUT, "tensor-core trailing update: a bounded wait gave up");
+  if (prec == ADGA_MIXED && h->ri8 && ri8_error(h->ri8))
+    return fail(h, ADGA_ETIMEOUT, "int8-slice residual: a bounded wait gave up");
   stage_ms(h, &h->stats.ms_chi0, ev[0], ev[1]);
   stage_ms(h, &h->stats.ms_bse, ev[1], ev[2]);
   stage_ms(h, &h->stats.ms_lu, ev[2], ev[3]);
@@ -1465,8 +1477,8 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
 extern "C" int adga_set_tune(adga_handle *h, const adga_tune *t) {
   if (!h || !t) return ADGA_EINVAL;
   if (t->factor < 0 || t->factor > 1 || t->pairs < 0 || t->pairs > 1 || t->tri_tc < 0 || t->tri_tc > 1 ||
-      t->batch < 0)
-    return fail(h, ADGA_EINVAL, "adga_set_tune: factor, pairs, tri_tc in {0, 1}, batch >= 0");
+      t->batch < 0 || t->resid < 0 || t->resid > 1)
+    return fail(h, ADGA_EINVAL, "adga_set_tune: factor, pairs, tri_tc, resid in {0, 1}, batch >= 0");
   h->tune = *t;
   return 0;
 }
@@ -1519,16 +1531,21 @@ extern "C" int adga_autotune(adga_handle *h, int qwstart, int qwstop, double tol
   // candidates: the tensor-core variants (when the tensor cores serve this size), then
   // the FP64 factorisation
   std::vector<adga_tune> cand;
-  auto with = [&](int f, int p, int t) { adga_tune x = start; x.factor = f; x.pairs = p; x.tri_tc = t; return x; };
+  auto with = [&](int f, int p, int t, int rs) {
+    adga_tune x = start; x.factor = f; x.pairs = p; x.tri_tc = t; x.resid = rs; return x;
+  };
   const bool tc = tc_available() && !getenv("ADGA_NO_TC");
   if (tc) {
-    if (c.N % 2 == 0) cand.push_back(with(0, 1, 1));
-    cand.push_back(with(0, 1, 0));
-    cand.push_back(with(0, 0, 0));
+    if (c.N % 2 == 0) {
+      cand.push_back(with(0, 1, 1, 1));
+      cand.push_back(with(0, 1, 1, 0));
+    }
+    cand.push_back(with(0, 1, 0, 1));
+    cand.push_back(with(0, 0, 0, 1));
   } else {
-    cand.push_back(with(0, 0, 0));
+    cand.push_back(with(0, 0, 0, 0));
   }
-  cand.push_back(with(1, 0, 0));
+  cand.push_back(with(1, 0, 0, 0));
   std::vector<z64> ref_chi, ref_sig, chi, sig;
   double ms = 0.0;
   h->tune = start;

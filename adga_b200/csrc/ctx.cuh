@@ -135,10 +135,22 @@ cudaError_t launch_eom_dynamic(const DevCtx &c, int iwb, const int *qidx, int np
 cudaError_t launch_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat, z64 *X, cudaStream_t st);
 // rnorm (nullable): per-matrix max |re| + |im| of the FP64 residual, atomicMax on the bit patterns;
 // Bpt (nullable): per-point right-hand sides in X's layout instead of (1+gamma^w) (tangent solves)
+// ri8 (k_resid_i8.cu context, or null for the FP64 CUDA-core GEMM): the product
+// X D F~ from exact int8 slices on the tensor cores; fgen names the current F~
+// (its slices are cut again when it changes)
 cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q,
                             const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
                             const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, const z64 *extra_d,
-                            unsigned long long *rnorm, cudaStream_t st, const z64 *Bpt = nullptr);
+                            unsigned long long *rnorm, cudaStream_t st, const z64 *Bpt = nullptr,
+                            void *ri8 = nullptr, long long fgen = 0);
+// the int8-slice residual (k_resid_i8.cu)
+cudaError_t ri8_setup(void **ctx, int N, int R, int cap);
+void ri8_free(void *ctx);
+int ri8_error(void *ctx);
+cudaError_t ri8_residual(void *ctx, const DevCtx &dc, int npts, const z64 *XD, const z64 *X,
+                         const z64 *Frow_d, const z64 *Frow_m, long long fgen, const z64 *opg_d,
+                         const z64 *opg_m, z32 *V, const z64 *extra_d, unsigned long long *rnorm, const z64 *Bpt,
+                         cudaStream_t st);
 cudaError_t launch_xd(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q, const z64 *c0inv, z64 *XD,
                       bool minus_one, cudaStream_t st);
 cudaError_t launch_update(int per, int nmat, const z32 *V, z64 *X, unsigned long long *norms,

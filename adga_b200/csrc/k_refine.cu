@@ -51,72 +51,6 @@ __global__ void k_xd(DevCtx c, int npts, const z64 *X, const z64 *chi0q, const z
   XD[m * per + e] = s;
 }
 
-// residual GEMM for one channel: rows (p, i1), K = N, columns c:
-//   r(p,i1,c) = B(i1,c) - X(p,i1,c) + sum_m XD(p,i1,m) F~(m,c)  -> V32 (FP32)
-// 64 x 64 tiles, BK = 16, 256 threads, 4 x 4 complex outputs per thread.
-__global__ void __launch_bounds__(256)
-k_resid(int N, int R, int npts, int ch, const z64 *__restrict__ XD, const z64 *__restrict__ X,
-        const z64 *__restrict__ Frow, const z64 *__restrict__ opg, z32 *V) {
-  __shared__ z64 As[16][64];
-  __shared__ z64 Bs[16][64];
-  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-  const int rows = npts * R;
-  const int r0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
-  z64 acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
-  const size_t per = (size_t)R * N;
-  for (int k0 = 0; k0 < N; k0 += 16) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      int e = t + 256 * i;
-      int kk = e & 15, rr = e >> 4;
-      int row = r0 + rr, k = k0 + kk;
-      z64 v = make_double2(0.0, 0.0);
-      if (row < rows && k < N) {
-        int p = row / R, i1 = row % R;
-        v = XD[(size_t)(2 * p + ch) * per + (size_t)i1 * N + k];
-      }
-      As[kk][rr] = v;
-      int cc = e & 63, kk2 = e >> 6;
-      int cl = c0 + cc, k2 = k0 + kk2;
-      Bs[kk2][cc] = (cl < N && k2 < N) ? Frow[(size_t)k2 * N + cl] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      z64 av[4], bv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) cfma(acc[i][j], av[i], bv[j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int row = r0 + ty + 16 * i;
-    if (row >= rows) continue;
-    int p = row / R, i1 = row % R;
-    size_t m = (size_t)(2 * p + ch);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int cl = c0 + tx + 16 * j;
-      if (cl >= N) continue;
-      z64 b = opg[i1 + (size_t)cl * R];
-      z64 x = X[m * per + (size_t)i1 * N + cl];
-      z64 r = make_double2(b.x - x.x + acc[i][j].x, b.y - x.y + acc[i][j].y);
-      V[m * per + (size_t)i1 * N + cl] = to32(r);
-    }
-  }
-}
-
 // X += up(V); per-matrix max |d| and max |X| (|re|+|im|) into norms[2*m], norms[2*m+1]
 __global__ void k_update(int per, const z32 *V, z64 *X, unsigned long long *norms, const int *active) {
   const int m = blockIdx.y;
@@ -154,11 +88,14 @@ cudaError_t launch_init_x(const z32 *T32, size_t strideM, int N, int R, int nmat
 cudaError_t launch_residual(const DevCtx &c, int npts, const z64 *X, const z64 *chi0q,
                             const z64 *c0inv, const z64 *Frow_d, const z64 *Frow_m,
                             const z64 *opg_d, const z64 *opg_m, z64 *XD, z32 *V, const z64 *extra_d,
-                            unsigned long long *rnorm, cudaStream_t st, const z64 *Bpt) {
+                            unsigned long long *rnorm, cudaStream_t st, const z64 *Bpt, void *ri8,
+                            long long fgen) {
   size_t total = (size_t)c.nd2 * c.N * 2 * npts;
   k_xd<<<cdiv_u(total, 256), 256, 0, st>>>(c, npts, X, chi0q, c0inv, XD, 1);
   cudaError_t e = ADGA_LAUNCH_CHECK();
   if (e != cudaSuccess) return e;
+  if (ri8)
+    return ri8_residual(ri8, c, npts, XD, X, Frow_d, Frow_m, fgen, opg_d, opg_m, V, extra_d, rnorm, Bpt, st);
   return launch_resid_z64(c, npts, XD, X, Frow_d, Frow_m, opg_d, opg_m, V, extra_d, rnorm, Bpt, st);
 }
 

@@ -22,12 +22,15 @@
 // Every mbarrier wait is bounded; on timeout the kernel records an error and
 // leaves.  Loads use no cluster multicast.
 #include "lu.cuh"
+#include "umma.cuh"
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <algorithm>
 #include <cstdio>
 
 namespace {
+
+using namespace umma;
 
 constexpr int BM = 128;          // rows per tile (MMA M)
 constexpr int BN = 128;          // complex columns per tile (MMA N = 2*BN)
@@ -38,54 +41,6 @@ constexpr int B_BYTES = 2 * BN * BK * 2;       // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 2 * BN;              // 256 fp32 columns
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s bound on any wait
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.b32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait: returns false (and records the error) after WAIT_NS
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *err, int code) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer();
-  for (;;) {
-    for (int i = 0; i < 64; ++i)
-      if (mbar_try(bar, parity)) return true;
-    if (gtimer() - t0 > WAIT_NS) {
-      atomicCAS(err, 0, code);
-      return false;
-    }
-  }
-}
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
-                                            int x, int y, int z) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
-      "l"((unsigned long long)map), "r"(bar), "r"(x), "r"(y), "r"(z)
-      : "memory");
-}
 // K-major, 128 B swizzle: LBO = 16 B (unused), SBO = 1024 B between 8-row groups
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   uint64_t d = 0;
@@ -107,22 +62,6 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, 
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
       "l"(a), "l"(b), "r"(IDESC), "r"(acc));
 }
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(192, 2)
 k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
@@ -262,9 +201,6 @@ constexpr int P_TMEM_COLS = 2 * TMEM_COLS;            // two accumulators
 constexpr int P_THREADS = 384;
 constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + 2 * P_CH_BYTES + 1024 + 256;
 
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
 
 __global__ void __launch_bounds__(P_THREADS, 1)
 k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,

@@ -226,11 +226,13 @@ int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
  *              update operands directly; 0: FP32 CUDA-core tile products and
  *              separate operand-split kernels
  *   batch   points per batch (0: as many as 60% of the free memory holds)
- * A new handle starts at {0, 1, 1, 0} (the environment switches
- * ADGA_NO_PAIRS, ADGA_TRI_TILE and ADGA_BATCH override it).
+ *   resid   1: the FP64 refinement residual's product X D F~ formed exactly
+ *              from int8 slices on the tensor cores; 0: FP64 CUDA-core GEMM
+ * A new handle starts at {0, 1, 1, 0, 1} (the environment switches
+ * ADGA_NO_PAIRS, ADGA_TRI_TILE, ADGA_BATCH and ADGA_RESID_FP64 override it).
  */
 typedef struct adga_tune {
-  int factor, pairs, tri_tc, batch;
+  int factor, pairs, tri_tc, batch, resid;
 } adga_tune;
 typedef struct adga_tune_trial {
   adga_tune tune;

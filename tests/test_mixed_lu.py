@@ -55,6 +55,22 @@ def test_panel_products_match_oracle(name, tri):
         assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
 
 
+@pytest.mark.parametrize("name", ["t3b", "t3m", "t2", "c3s", "t5"])
+@pytest.mark.parametrize("resid", ["int8", "fp64"])
+def test_refinement_residual_matches_oracle(name, resid):
+    """The FP64 refinement residual r = B - X + (X D) F~ with its product formed
+    exactly from int8 slices on the tensor cores (the default) or by the FP64
+    CUDA-core GEMM (ADGA_RESID_FP64=1): the refinement converges without FP64
+    re-solves to the same outputs."""
+    p = problem(name)
+    status, stats, got = run_mixed(p, {"ADGA_RESID_FP64": "1"} if resid == "fp64" else {})
+    want = oracle_run(p)
+    assert stats["mixed_fallbacks"] == 0 and not status.any()
+    assert stats["max_refine_iters"] <= 3 and stats["max_refine_resid"] <= 1e-10
+    for k in ("chi_dens", "chi_magn", "sigma", "chi_qw_dens", "chi_qw_magn"):
+        assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
+
+
 @pytest.mark.parametrize("name", ["t3b", "t3m"])
 def test_step_by_step_updates_match_oracle(name):
     """ADGA_NO_PAIRS=1: the unpivoted FP32 factorisation with one tensor-core
