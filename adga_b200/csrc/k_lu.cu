@@ -1156,11 +1156,6 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
 template <typename T>
 static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
                             bool upper, T *work, cudaStream_t st) {
-  // FP32 factors, R <= 9, N in 640..1152: the register-resident solve (ADGA_TRSV_STREAM=1: streaming)
-  if constexpr (sizeof(T) == sizeof(z32)) {
-    if (trsv_reg_supported(lb, R) && (upper || lb.perm) && !getenv("ADGA_TRSV_STREAM"))
-      return launch_trsv_reg((const z32 *)M, lb, (z32 *)C, strideC, ldc, R, upper, lb.perm, st);
-  }
   // few right-hand sides and NB = 64: the streaming solve (k_trsv.cu)
   if (trsv_stream_supported<T>(lb, strideC, R, upper, lb.perm, work))
     return launch_trsv_stream<T>(M, lb, C, strideC, ldc, R, upper, lb.perm, work, st);

@@ -330,170 +330,6 @@ k_trsv_stream(const T *__restrict__ M, size_t strideM, int N, int nsteps, const 
   }
 }
 
-// ---------------------------------------------------------------------------
-// Register-resident solve of the FP32 factors (the mixed path's refinement):
-// one CTA per matrix, thread t owns rows 4t .. 4t+3 and keeps their R <= 9
-// right-hand sides in registers for the whole solve.  Per block step (NB = 64):
-// the owners of the step's rows hand them to shared memory, Y = D^-1 B_J (D the
-// inverted diagonal block) is formed there and packed as the two pairs
-// (-y_re, -y_im), (y_im, -y_re), and every thread applies B_rows -= L(rows, J)
-// Y to its rows with packed FMAs, the panel's columns read straight from global
-// memory (32 contiguous bytes per thread and column, four columns in flight): each
-// triangle element is read once, with no shared-memory ring.
-// ---------------------------------------------------------------------------
-constexpr int TR_RPT = 4;               // rows per thread
-constexpr int TR_RMAX = 9;              // right-hand sides held per row
-constexpr int TR_MAXT = 288;            // threads: N <= 1152
-constexpr int TR_DLD = 65;              // padded stride of the staged diagonal block
-
-template <bool UPPER>
-__global__ void __launch_bounds__(TR_MAXT, 1)
-k_trsv_reg(const z32 *__restrict__ M, size_t strideM, int N, int nsteps, const z32 *__restrict__ Dinv, z32 *C,
-           size_t strideC, int ldc, int R, const int *__restrict__ perm) {
-  __shared__ __align__(16) float4 Ys[TS_NB][TR_RMAX];     // packed -Y per (k, rhs)
-  __shared__ __align__(16) z32 Bj[TS_NB][TR_RMAX];        // the step's rows; then their solution
-  __shared__ __align__(16) z32 Ds[TS_NB * TR_DLD];        // D^-1 of the step
-  const int b = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
-  const z32 *A = M + (size_t)b * strideM;
-  z32 *Cb = C + (size_t)b * strideC;
-  const int r0 = TR_RPT * t;
-  float2 acc[TR_RPT][TR_RMAX];
-#pragma unroll
-  for (int i = 0; i < TR_RPT; ++i) {
-    const int row = r0 + i;
-    const int src = (!UPPER && perm && row < N) ? perm[(size_t)b * N + row] : row;
-#pragma unroll
-    for (int r = 0; r < TR_RMAX; ++r)
-      acc[i][r] = (row < N && r < R) ? Cb[(size_t)src + (size_t)r * ldc] : make_float2(0.f, 0.f);
-  }
-  for (int s = 0; s < nsteps; ++s) {
-    const int blk = UPPER ? nsteps - 1 - s : s;
-    const int J = blk * TS_NB, jb = min(TS_NB, N - J);
-    __syncthreads();                     // the previous step is done with Bj, Ys and Ds
-    {
-      const z32 *D = Dinv + ((size_t)b * nsteps + blk) * TS_NB * TS_NB;
-      for (int e = t; e < TS_NB * TS_NB; e += nt) Ds[(e % TS_NB) * TR_DLD + e / TS_NB] = D[e];   // Ds[i][k]
-    }
-#pragma unroll
-    for (int i = 0; i < TR_RPT; ++i) {
-      const int k = r0 + i - J;
-      if (k >= 0 && k < jb)
-#pragma unroll
-        for (int r = 0; r < TR_RMAX; ++r) Bj[k][r] = acc[i][r];
-    }
-    __syncthreads();
-    // Y = D^-1 B_J (outputs (i, r)), kept as the solution rows and packed negated for the update
-    for (int e = t; e < TS_NB * TR_RMAX; e += nt) {
-      const int i = e % TS_NB, r = e / TS_NB;
-      float2 y = make_float2(0.f, 0.f);
-      if (i < jb && r < R) {
-        const z32 *d = Ds + i * TR_DLD;
-        float2 y2 = make_float2(0.f, 0.f);
-        for (int k = 0; k < jb; k += 2) {
-          cfma(y, d[k], Bj[k][r]);
-          if (k + 1 < jb) cfma(y2, d[k + 1], Bj[k + 1][r]);
-        }
-        y = cadd(y, y2);
-      }
-      Ys[i][r] = make_float4(-y.x, -y.y, y.y, -y.x);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < TR_RPT; ++i) {
-      const int k = r0 + i - J;
-      if (k >= 0 && k < jb)
-#pragma unroll
-        for (int r = 0; r < TR_RMAX; ++r) {
-          const float4 q = Ys[k][r];
-          acc[i][r] = make_float2(-q.x, -q.y);
-        }
-    }
-    // B_rows -= L(rows, J..J+jb) Y for the rows still to solve
-    const int lo = UPPER ? 0 : J + jb, hi = UPPER ? J : N;
-    if (r0 + TR_RPT > lo && r0 < hi) {
-      const float4 *col = reinterpret_cast<const float4 *>(A + (size_t)J * N + r0);   // rows r0..r0+3
-      const size_t cs = (size_t)N / 2;                                                 // float4 per column
-      bool inr[TR_RPT];
-#pragma unroll
-      for (int i = 0; i < TR_RPT; ++i) inr[i] = r0 + i >= lo && r0 + i < hi;
-      const bool full = inr[0] && inr[TR_RPT - 1];
-      auto ld = [&](int k, float4 (&a)[2]) {
-        if (k < jb && r0 + TR_RPT <= N) {
-          a[0] = __ldg(col + (size_t)k * cs);
-          a[1] = __ldg(col + (size_t)k * cs + 1);
-        } else {
-          a[0] = a[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (k < jb) {                      // the matrix's last rows: element by element
-            const z32 *c1 = A + (size_t)(J + k) * N + r0;
-            const float2 v0 = c1[0], v1 = r0 + 1 < N ? c1[1] : make_float2(0.f, 0.f);
-            const float2 v2 = r0 + 2 < N ? c1[2] : make_float2(0.f, 0.f), v3 = r0 + 3 < N ? c1[3] : make_float2(0.f, 0.f);
-            a[0] = make_float4(v0.x, v0.y, v1.x, v1.y);
-            a[1] = make_float4(v2.x, v2.y, v3.x, v3.y);
-          }
-        }
-        if (!full) {                         // rows outside [lo, hi) take no update
-          if (!inr[0]) { a[0].x = 0.f; a[0].y = 0.f; }
-          if (!inr[1]) { a[0].z = 0.f; a[0].w = 0.f; }
-          if (!inr[2]) { a[1].x = 0.f; a[1].y = 0.f; }
-          if (!inr[3]) { a[1].z = 0.f; a[1].w = 0.f; }
-        }
-      };
-      auto apply = [&](int k, const float4 (&a)[2]) {
-        const float ar[4] = {a[0].x, a[0].z, a[1].x, a[1].z}, ai[4] = {a[0].y, a[0].w, a[1].y, a[1].w};
-#pragma unroll
-        for (int r = 0; r < TR_RMAX; ++r) {
-          const float4 q = Ys[k][r];
-          const float2 y1 = make_float2(q.x, q.y), y2 = make_float2(q.z, q.w);
-#pragma unroll
-          for (int i = 0; i < TR_RPT; ++i) {
-            acc[i][r] = __ffma2_rn(make_float2(ar[i], ar[i]), y1, acc[i][r]);
-            acc[i][r] = __ffma2_rn(make_float2(ai[i], ai[i]), y2, acc[i][r]);
-          }
-        }
-      };
-      // four columns in flight while four are applied
-      float4 cur[4][2], nxt[4][2];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) ld(u, cur[u]);
-      for (int k = 0; k < jb; k += 4) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) ld(k + 4 + u, nxt[u]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (k + u < jb) apply(k + u, cur[u]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u) { cur[u][0] = nxt[u][0]; cur[u][1] = nxt[u][1]; }
-      }
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < TR_RPT; ++i) {
-    const int row = r0 + i;
-    if (row < N)
-#pragma unroll
-      for (int r = 0; r < TR_RMAX; ++r)
-        if (r < R) Cb[(size_t)row + (size_t)r * ldc] = acc[i][r];
-  }
-}
-
-bool trsv_reg_supported(const LUBatch &lb, int R) {
-  return lb.NB == TS_NB && R >= 1 && R <= TR_RMAX && lb.N >= 640 && lb.N <= TR_RPT * TR_MAXT &&
-         (lb.N % 2) == 0 && (lb.strideM % 2) == 0;
-}
-
-cudaError_t launch_trsv_reg(const z32 *M, const LUBatch &lb, z32 *C, size_t strideC, int ldc, int R, bool upper,
-                            const int *perm, cudaStream_t st) {
-  const int nt = (lb.N + TR_RPT - 1) / TR_RPT;
-  const int threads = (nt + 31) / 32 * 32;
-  if (upper)
-    k_trsv_reg<true><<<lb.batch, threads, 0, st>>>(M, lb.strideM, lb.N, lb.nsteps(), (const z32 *)lb.Uinv, C,
-                                                   strideC, ldc, R, nullptr);
-  else
-    k_trsv_reg<false><<<lb.batch, threads, 0, st>>>(M, lb.strideM, lb.N, lb.nsteps(), (const z32 *)lb.Linv, C,
-                                                    strideC, ldc, R, perm);
-  return ADGA_LAUNCH_CHECK();
-}
-
 cudaError_t lu_build_perm(const LUBatch &lb, int *perm, cudaStream_t st) {
   if (!perm || lb.N > 8192) return cudaErrorInvalidValue;
   k_build_perm<<<lb.batch, 128, sizeof(int) * 2 * lb.N, st>>>(lb.ipiv, lb.N, perm);

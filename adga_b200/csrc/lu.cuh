@@ -100,8 +100,3 @@ bool trsv_stream_supported(const LUBatch &lb, size_t strideC, int R, bool upper,
 template <typename T>
 cudaError_t launch_trsv_stream(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
                                bool upper, const int *perm, T *work, cudaStream_t st);
-// register-resident FP32 solve (k_trsv.cu): NB = 64, R <= 9, 640 <= N <= 1152, N even;
-// the forward one applies perm (may be null) as it loads the right-hand sides
-bool trsv_reg_supported(const LUBatch &lb, int R);
-cudaError_t launch_trsv_reg(const z32 *M, const LUBatch &lb, z32 *C, size_t strideC, int ldc, int R, bool upper,
-                            const int *perm, cudaStream_t st);

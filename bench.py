@@ -549,15 +549,18 @@ def main():
     nlaunch = max(sum(s["trail_launches"] for s in st_mixed), 1)
     achieved = gbytes / mst * 1e3 if mst else 0.0          # GB/s
     peak = pk.get("hbm_gbs")
-    roof = {"kernel": "k_tc_persist: tensor-core LU trailing updates of the mixed path (narrow K=64 and "
-                      "wide K=128 regions of each step pair; GEMM launches only)",
+    bf16_tf = 3 * gflop / mst if mst else 0.0
+    roof = {"kernel": "k_tc_persist: tensor-core LU trailing updates of the mixed path (per step pair: the "
+                      "narrow K=64 update, two launches, and the wide K=128 update, one launch; GEMMs only)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if peak else None,
             "traffic": TRAFFIC_OVER_ALG * gbytes * 1e9 / nlaunch,
             "peak_kind": f"hbm copy bandwidth, {pk_kind}",
-            "alg_bytes_per_launch": gbytes * 1e9 / nlaunch, "avg_launch_ms": mst / nlaunch,
-            "complex_tflops": gflop / mst if mst else 0.0,
-            "bf16_tensor_tflops": 3 * gflop / mst if mst else 0.0}
+            "alg_bytes_per_update": gbytes * 1e9 / nlaunch, "avg_update_ms": mst / nlaunch,
+            "updates": nlaunch, "complex_tflops": gflop / mst if mst else 0.0,
+            "bf16_tensor_tflops": bf16_tf,
+            "tensor_frac": bf16_tf / pk["bf16_tflops_sustained"] if pk.get("bf16_tflops_sustained") else None,
+            "tensor_peak_kind": f"bf16 sustained, {pk_kind}"}
     stage_keys = ("ms_chi0", "ms_bse", "ms_lu", "ms_trail", "ms_post", "ms_eom", "ms_total")
     stage = {k: sum(s[k] for s in st_mixed) / args.steps for k in stage_keys}
     stage64 = {k: sum(s[k] for s in st64) / args.steps for k in stage_keys} if not args.no_fp64 else None
