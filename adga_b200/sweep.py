@@ -53,25 +53,30 @@ def _ranges(nqp, iwbmax, omegas):
     return [((iwb + iwbmax) * nqp + 1, (iwb + iwbmax + 1) * nqp) for iwb in sorted(omegas)]
 
 
-def _run_pass(lad, prob, ranges, precision):
+def _run_pass(lad, prob, ranges, precision, probe=None):
+    """One pass over the ranges; probe: a 1-based compound point whose raw
+    chi_qw_dens / chi_qw_magn are returned as well (in the result's 'probe')."""
     lad.reset_outputs()
-    ms, iters, fallbacks, outs, touts = 0.0, 0, 0, [], []
+    ms, iters, fallbacks, outs, touts, got = 0.0, 0, 0, [], [], None
     for qs, qe in ranges:
         _, st = lad.ladder_run_tangent(qs, qe, precision)
         ms += st["ms_total"]
         iters = max(iters, st["max_refine_iters"])
         fallbacks += st["mixed_fallbacks"]
-        outs.append(lad.assemble(lad.get_outputs(), prob.siw))
+        raw = lad.get_outputs()
+        if probe is not None and qs <= probe <= qe:
+            got = {k: raw[k][:, :, probe - qs].copy() for k in ("chi_qw_dens", "chi_qw_magn")}
+        outs.append(lad.assemble(raw, prob.siw))
         touts.append([lad.assemble_tangent(lad.get_tangent_outputs(d)) for d in range(len(GRAD_PARAMS))])
     # chi per point of every range, Sigma after the last range (it accumulates)
     chi = {k: np.concatenate([o[k] for o in outs], axis=-1) for k in ("chi_dens", "chi_magn")}
     dchi = [np.concatenate([t[d]["chi_magn"] for t in touts], axis=-1) for d in range(len(GRAD_PARAMS))]
     res = dict(chi_dens=chi["chi_dens"], chi_magn=chi["chi_magn"], sigma=outs[-1]["sigma"],
-               dchi_magn=dchi, dsigma=[touts[-1][d]["sigma"] for d in range(len(GRAD_PARAMS))])
+               dchi_magn=dchi, dsigma=[touts[-1][d]["sigma"] for d in range(len(GRAD_PARAMS))], probe=got)
     return ms, iters, fallbacks, res
 
 
-def run_point(prepared, omegas, check_fp64=True, keep=False, tune_cache=None) -> Dict:
+def run_point(prepared, omegas, check_fp64=True, keep=False, tune_cache=None, probe=None) -> Dict:
     """One parameter point: mixed ladder + tangents of U and J on the omega
     slices `omegas`, then (check_fp64) the FP64 pass; keep: also return the
     mixed outputs (chi_dens, chi_magn per point, sigma, dchi_magn, dsigma).
@@ -99,12 +104,14 @@ def run_point(prepared, omegas, check_fp64=True, keep=False, tune_cache=None) ->
             if dv:
                 for iwb, (a, b) in dv.items():
                     lad.set_vertex_tangent(iwb, a, b, direction=dr)
-        ms, iters, fb, mx = _run_pass(lad, prob, ranges, "mixed")
+        ms, iters, fb, mx = _run_pass(lad, prob, ranges, "mixed", probe)
         rec = dict(name=s.name, ndim=s.ndim, iwf=s.iwf, beta=s.beta, U=s.U, J=s.J, N=N, points=npts,
                    ms_mixed=ms, pts_per_s=npts / (ms * 1e-3), max_refine_iters=iters, mixed_fallbacks=fb,
                    tune=lad.tune)
         if tuned:
             rec["autotune"] = tuned
+        if mx["probe"] is not None:
+            rec["probe"] = mx["probe"]
         if check_fp64:
             ms64, _, _, f64 = _run_pass(lad, prob, ranges, "fp64")
             rec["ms_fp64"] = ms64
@@ -119,11 +126,12 @@ def run_point(prepared, omegas, check_fp64=True, keep=False, tune_cache=None) ->
 
 
 def run_sweep(specs: Sequence, omegas: Optional[Sequence[int]] = None, check_fp64: bool = True,
-              log=None, autotune: bool = True) -> Dict:
+              log=None, autotune: bool = True, probes: Optional[Dict[str, int]] = None) -> Dict:
     """Run every parameter point (largest BSE dimension first); the next
     point's host inputs are prepared while the current one runs.  autotune:
     the mixed path's kernel choices are measured once per (ndim, N) and
-    reused by every point of that size."""
+    reused by every point of that size.  probes: {point name: 1-based compound
+    point} whose raw chi_qw the records keep ('probe')."""
     order = sorted(specs, key=lambda sp: -(sp.ndim ** 2 * 2 * sp.iwf))
     om = lambda sp: list(range(-sp.iwb, sp.iwb + 1)) if omegas is None else list(omegas)
     recs: List[Dict] = []
@@ -134,7 +142,8 @@ def run_sweep(specs: Sequence, omegas: Optional[Sequence[int]] = None, check_fp6
         for i, sp in enumerate(order):
             prepared = nxt.result()
             nxt = pool.submit(_prepare, order[i + 1], om(order[i + 1])) if i + 1 < len(order) else None
-            rec = run_point(prepared, om(sp), check_fp64, tune_cache=tune_cache)
+            rec = run_point(prepared, om(sp), check_fp64, tune_cache=tune_cache,
+                            probe=(probes or {}).get(sp.name))
             recs.append(rec)
             if log:
                 log(rec)

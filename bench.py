@@ -162,6 +162,90 @@ class CpuPool:
 
 
 # ---------------------------------------------------------------------------
+# Config 4, the uneven-size parameter sweep: the oracle on one (q, omega = 0)
+# point of every distinct (ndim, N), in spawned workers on the host cores
+# ---------------------------------------------------------------------------
+def _c4_cpu_point(spec):
+    """Seconds of the FP64 oracle (zgetrf + zgetri inversions, on-the-fly G,
+    EOM) for point iq = 1 (0-based) of the omega = 0 slice, single-threaded,
+    and its chi_qw_dens / chi_qw_magn."""
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import numpy as np
+    from adga_b200 import synth
+    from oracle.adga_oracle import LadderInputs, Oracle
+    p = synth.make_problem(spec)
+    s = p.spec
+    inp = LadderInputs(ndim=s.ndim, nk=s.nk, nq=s.nq, iwmax=p.iwmax, iwfmax_small=s.iwf, iwbmax_small=s.iwb,
+                       beta=p.beta, mu=p.mu, hk=p.hk, siw=p.siw, giw=p.giw, dc=p.dc, u=p.u, u_tilde=p.u_tilde,
+                       n_dmft=p.n_dmft, vertex=p.vertex, iw_data=p.iw_data)
+    o = Oracle(inp)
+    scratch = {k: np.zeros((p.ndim2, p.ndim2, 2 * s.iwb + 1), complex)
+               for k in ("bubble_loc", "chi_loc_dens", "chi_loc_magn")}
+    loc = o.local_block(0, 1, scratch)
+    o.point(0, 0, loc)                                # warm the G caches
+    t = time.perf_counter()
+    res = o.point(1, 0, loc)
+    sig = np.zeros((p.ndim, p.ndim, 2 * s.iwf, s.nkp), complex, order="F")
+    o.calc_eom_dynamic(res["etaqd"], res["etaqm"], res["gammaqd"], 0, 1, sig)
+    return time.perf_counter() - t, res["chi_qw_dens"], res["chi_qw_magn"]
+
+
+def run_c4(args):
+    """The 64 seeded parameter points (ndim 1/3/5, BSE 40..4000) over all 11
+    bosonic frequencies, mixed ladder with the gradients in U and J per point,
+    then the FP64 pass (adga_b200.sweep); per-size CPU baseline and oracle probes."""
+    import multiprocessing as mp
+    import numpy as np
+    from adga_b200 import synth
+    specs = synth.sweep_specs(64)
+    sizes = {}
+    for sp in specs:
+        sizes.setdefault((sp.ndim, sp.ndim ** 2 * 2 * sp.iwf), []).append(sp)
+    keys = sorted(sizes)
+    reps = [sizes[k][0] for k in keys]
+    cores = os.cpu_count() or 1
+    pool = mp.get_context("spawn").Pool(min(len(reps), cores))   # before any GPU call
+    job = pool.map_async(_c4_cpu_point, reps, chunksize=1)
+    from adga_b200 import sweep
+    probes = {sp.name: (0 + sp.iwb) * sp.nqp + 2 for sp in reps}  # omega = 0, iq = 1 (0-based)
+    res = sweep.run_sweep(specs, None, check_fp64=True, autotune=True, probes=probes)
+    cpu = job.get()
+    pool.close()
+    summ, recs = res["summary"], {r["name"]: r for r in res["points"]}
+    rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    per_size, core_s = {}, 0.0
+    for k, sp, (sec, cd, cm) in zip(keys, reps, cpu):
+        pts = sum(x.nqp * (2 * x.iwb + 1) for x in sizes[k])
+        core_s += pts * sec
+        pr = recs[sp.name]["probe"]
+        per_size[f"ndim{k[0]}_N{k[1]}"] = {
+            "parameter_points": len(sizes[k]), "qw_points": pts, "cpu_s_per_point": sec,
+            "tune": recs[sp.name]["tune"],
+            "mixed_vs_oracle_probe": max(rel(pr["chi_qw_dens"], cd), rel(pr["chi_qw_magn"], cm)),
+            "mixed_pts_per_s": sum(recs[x.name]["points"] for x in sizes[k]) /
+                               (1e-3 * sum(recs[x.name]["ms_mixed"] for x in sizes[k])),
+            "fp64_over_mixed": sum(recs[x.name]["ms_fp64"] for x in sizes[k]) /
+                               sum(recs[x.name]["ms_mixed"] for x in sizes[k])}
+    cpu_v = summ["qw_points"] / core_s * cores
+    line = {"metric": METRIC, "value": summ["pts_per_s_device"], "unit": UNIT, "n_gpus": 1, "steps": 1,
+            "warmup": 0, "ms_per_step": summ["ms_mixed"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "mixed: c64 LU (bf16x3 tensor-core updates) + c128 refinement, "
+                                          "tangents of U and J in the same pass",
+            "data": "synthetic (64 seeded parameter points)",
+            "config": {"workload": "c4: uneven-size sweep, 64 parameter points, ndim 1/3/5, BSE N 40..4000, "
+                                   "12^3 k, 6^3 q, 11 bosonic frequencies, gradients in U and J per point",
+                       "step": "the whole sweep once (each size's kernel choices tuned first, untimed)"},
+            "fp64_ms": summ.get("ms_fp64"), "mixed_over_fp64": summ.get("mixed_over_fp64"),
+            "max_err_vs_fp64": summ.get("max_err_vs_fp64"), "per_size": per_size,
+            "sweep_wall_s": summ["wall_s"], "autotune_wall_s": summ["autotune_wall_s"],
+            "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": cores, "kind": "port", "cpu_model": cpu_model(),
+                             "sample": "one (q, omega=0) point per distinct (ndim, N), FP64 oracle port single-"
+                                       "threaded, weighted by each size's share of the points, scaled to all cores"}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi samples during the timed region."""
 
@@ -279,6 +363,10 @@ def main():
     if world > 1:
         # one GPU per process: the library's runtime and torch both see device 0
         os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    if args.workload == "c4" and args.impl == "ours":
+        if rank == 0:
+            run_c4(args)
+        return
     if args.impl == "reference":
         if world > 1:
             import torch.distributed as dist
