@@ -6,12 +6,14 @@
 // Complex arithmetic is embedded as
 //     [Re C | Im C] = [Lr | Li] . [[Ur, Ui], [-Ui, Ur]]
 // so one MMA with N = 2*BN produces the real (columns 0..BN) and imaginary
-// (BN..2BN) parts of BN complex columns.  Operands are staged per step by
-// k_split_a / k_split_b in K-major BF16 with every 3-term segment NB long:
-//     A[m]     = [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo]
-//     Bre[n]   = [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo, Ur_hi, -Ui_hi]
-//     Bim[n]   = [Ui_hi,  Ur_hi, Ui_lo,  Ur_lo, Ui_hi,  Ur_hi]
-// (K = 6*NB).  Two GEMM kernels share the operand path (TMA loads with
+// (BN..2BN) parts of BN complex columns.  Operands are staged per step in
+// K-major BF16, four segments of NB each (K4 = 4*NB per step):
+//     A[m]     = [Lr_hi, Li_hi, Lr_lo, Li_lo]
+//     Bre[n]   = [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo]
+//     Bim[n]   = [Ui_hi,  Ur_hi, Ui_lo,  Ur_lo]
+// and the GEMMs run six segment pairs per step (A, B) = (0,0), (1,1), (0,2),
+// (1,3), (2,0), (3,1): the hi*hi, hi*lo and lo*hi products of the real and
+// imaginary parts (K = 6*NB of MMAs from 4*NB of staging).
 // 128B swizzle into a ring of shared-memory stages, tcgen05.mma M=128,
 // N=256, K=16 issued by one thread, FP32 accumulators in TMEM):
 //   k_tc_persist  (used when the C strides are 16-byte multiples) one CTA per
@@ -41,6 +43,12 @@ constexpr int B_BYTES = 2 * BN * BK * 2;       // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 2 * BN;              // 256 fp32 columns
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+// the staging segments of MMA k-segment j (0..5) of a step: A and B segment indices
+__device__ __forceinline__ int seg_a(int j) { return j < 4 ? (j & 1) : j - 2; }
+__device__ __forceinline__ int seg_b(int j) { return j < 4 ? j : j - 4; }
+// x coordinate (bf16) in the four-segment staging of k-block kb of a step (nbk = NB / BK)
+__device__ __forceinline__ int kx_a(int kb, int nbk) { return (seg_a(kb / nbk) * nbk + kb % nbk) * BK; }
+__device__ __forceinline__ int kx_b(int kb, int nbk) { return (seg_b(kb / nbk) * nbk + kb % nbk) * BK; }
 // K-major, 128 B swizzle: LBO = 16 B (unused), SBO = 1024 B between 8-row groups
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   uint64_t d = 0;
@@ -66,7 +74,7 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, 
 __global__ void __launch_bounds__(192, 2)
 k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int Ncols, int Ncap, int nkb,
-            int b0, int *err) {
+            int b0, int nbk, int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
@@ -104,9 +112,9 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         if (!ok) break;
         const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
         mbar_expect_tx(bar_full + 8 * s, STAGE_BYTES);
-        tma_load_3d(sa, &mapA, bar_full + 8 * s, kb * BK, m0, b);
-        tma_load_3d(sb, &mapB, bar_full + 8 * s, kb * BK, n0, b);
-        tma_load_3d(sb + B_BYTES / 2, &mapB, bar_full + 8 * s, kb * BK, Ncap + n0, b);
+        tma_load_3d(sa, &mapA, bar_full + 8 * s, kx_a(kb, nbk), m0, b);
+        tma_load_3d(sb, &mapB, bar_full + 8 * s, kx_b(kb, nbk), n0, b);
+        tma_load_3d(sb + B_BYTES / 2, &mapB, bar_full + 8 * s, kx_b(kb, nbk), Ncap + n0, b);
       }
     }
   } else if (warp == 1) {
@@ -207,7 +215,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
              const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB2,
              const __grid_constant__ CUtensorMap mapC, z32 *M, size_t strideM, int N, int crow0, int ccol0,
              int arow0, int bcol0, int arow2, int bcol2, int nkb1, int Mrows, int Ncols, int Ncap, int nkb, int b0,
-             int count, int *err) {
+             int count, int nbk, int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
@@ -262,10 +270,11 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           // k-blocks [0, nkb1) from the first staging, the rest from the second
           const bool second = kb >= nkb1;
           const CUtensorMap *ma = second ? &mapA2 : &mapA, *mb = second ? &mapB2 : &mapB;
-          const int kx = (second ? kb - nkb1 : kb) * BK, ar = second ? arow2 : arow0, bc = second ? bcol2 : bcol0;
-          tma_load_3d(sa, ma, bar_full + 8 * s, kx, ar + tm * BM, b);
-          tma_load_3d(sb, mb, bar_full + 8 * s, kx, bc + tn * BN, b);
-          tma_load_3d(sb + B_BYTES / 2, mb, bar_full + 8 * s, kx, Ncap + bc + tn * BN, b);
+          const int kl = second ? kb - nkb1 : kb, ar = second ? arow2 : arow0, bc = second ? bcol2 : bcol0;
+          const int xa = kx_a(kl, nbk), xb = kx_b(kl, nbk);
+          tma_load_3d(sa, ma, bar_full + 8 * s, xa, ar + tm * BM, b);
+          tma_load_3d(sb, mb, bar_full + 8 * s, xb, bc + tn * BN, b);
+          tma_load_3d(sb + B_BYTES / 2, mb, bar_full + 8 * s, xb, Ncap + bc + tn * BN, b);
         }
         if (!ok) break;
       }
@@ -401,7 +410,7 @@ constexpr int TT_THREADS = 256;
 constexpr int TT_ROWS = 128;                       // tile rows (MMA M)
 constexpr int TT_KBLK = TT_ROWS * 128;             // one K block: 128 rows x 64 bf16
 constexpr int TT_OPER = 4 * TT_KBLK;               // A hi, A lo, B hi, B lo of one K half: 64 KB
-constexpr int TT_SROW = 784;                       // padded stride of a staged 768 B operand row
+constexpr int TT_SROW = 528;                       // padded stride of a staged 512 B operand row
 constexpr int TT_FROW = 528;                       // padded stride of a staged 512 B matrix column
 constexpr int TT_SMEM_BYTES = TT_OPER + 1024 + 64;
 constexpr int TT_TMEM_COLS = 128;
@@ -458,12 +467,13 @@ __device__ __forceinline__ uint4 pack8(const float *re, const float *im, int par
   }
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
-// nrow rows of 768 B, staged with stride TT_SROW, to nrow contiguous global rows
+// nrow operand rows of 512 B (four segments of 64 bf16), staged with stride TT_SROW, to nrow
+// contiguous global rows
 __device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat16 *dst, int nrow, int t) {
   unsigned char *d = reinterpret_cast<unsigned char *>(dst);
-  for (int e = t; e < nrow * 48; e += TT_THREADS) {
-    const int r = e / 48, c = e % 48;
-    *reinterpret_cast<uint4 *>(d + (size_t)r * 768 + c * 16) =
+  for (int e = t; e < nrow * 32; e += TT_THREADS) {
+    const int r = e / 32, c = e % 32;
+    *reinterpret_cast<uint4 *>(d + (size_t)r * 512 + c * 16) =
         *reinterpret_cast<const uint4 *>(stg + r * TT_SROW + c * 16);
   }
 }
@@ -631,27 +641,24 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
                 if (n0 + 16 * piece + j < jb)
                   dst[(size_t)(J + n0 + 16 * piece + j) * N] = make_float2(re[j], im[j]);
             }
-            // k_split_a's rows [Lr_hi, Li_hi, Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
+            // k_split_a's rows [Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
               const int o = 32 * piece + 16 * c;
-              const uint4 rh = pack8(re + 8 * c, im + 8 * c, 0, false), ih = pack8(re + 8 * c, im + 8 * c, 2, false);
-              *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = rh;
-              *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = ih;
-              *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = rh;
-              *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = ih;
-              *reinterpret_cast<uint4 *>(row + 4 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 1, false);
-              *reinterpret_cast<uint4 *>(row + 5 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 3, false);
+              *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 0, false);
+              *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 2, false);
+              *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 1, false);
+              *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 3, false);
             }
           }
         }
         __syncthreads();
-        copy_rows(stg, Astage + ((size_t)b * N + m0 + 64 * rnd) * 6 * NB, min(64, nv - 64 * rnd), t);
+        copy_rows(stg, Astage + ((size_t)b * N + m0 + 64 * rnd) * 4 * NB, min(64, nv - 64 * rnd), t);
       }
     } else {
       const int pc = jb / 2;                       // 16-byte pieces of a U12 column (jb is even)
       // rounds 0, 1: U12 columns (rows 64 rnd ..); 2..5: k_split_b's real rows [Ur_hi, -Ui_hi,
-      // Ur_lo, -Ui_lo, Ur_hi, -Ui_hi] and imaginary rows [Ui_hi, Ur_hi, Ui_lo, Ur_lo, Ui_hi, Ur_hi]
+      // Ur_lo, -Ui_lo] and imaginary rows [Ui_hi, Ur_hi, Ui_lo, Ur_lo]
 #pragma unroll 1
       for (int rnd = 0; rnd < 6; ++rnd) {
         const int rh64 = rnd & 1;                  // tile rows 64 rh64 .. 64 rh64 + 63
@@ -676,21 +683,15 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
                 const float *xr = re + 8 * c, *xi = im + 8 * c;
                 const int o = 16 * c;
                 if (!imag) {
-                  const uint4 a = pack8(xr, xi, 0, false), nb = pack8(xr, xi, 2, true);
-                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = a;
-                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = nb;
+                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 0, false);
+                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 2, true);
                   *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 1, false);
                   *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 3, true);
-                  *reinterpret_cast<uint4 *>(row + 4 * 128 + o) = a;
-                  *reinterpret_cast<uint4 *>(row + 5 * 128 + o) = nb;
                 } else {
-                  const uint4 a = pack8(xr, xi, 2, false), bb = pack8(xr, xi, 0, false);
-                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = a;
-                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = bb;
+                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 2, false);
+                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 0, false);
                   *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 3, false);
                   *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 1, false);
-                  *reinterpret_cast<uint4 *>(row + 4 * 128 + o) = a;
-                  *reinterpret_cast<uint4 *>(row + 5 * 128 + o) = bb;
                 }
               }
             }
@@ -705,7 +706,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
                 *reinterpret_cast<const float4 *>(stg + cc * TT_FROW + pp * 16);
           }
         } else {
-          copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (rnd >= 4 ? (size_t)Ncap : 0) + m0 + 64 * rh64) * 6 * NB,
+          copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (rnd >= 4 ? (size_t)Ncap : 0) + m0 + 64 * rh64) * 4 * NB,
                     nrw, t);
         }
       }
@@ -720,7 +721,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
 }
 
 // ---------------------------------------------------------------------------
-// A[b][m][6*NB]: rows m = 0..Mrows-1 are matrix rows J+jb+m, k = 0..NB-1 (zero for k >= jb)
+// A[b][m][4*NB]: rows m = 0..Mrows-1 are matrix rows J+jb+m, k = 0..NB-1 (zero for k >= jb)
 __global__ void __launch_bounds__(256)
 k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB, __nv_bfloat16 *A,
           int b0) {
@@ -743,17 +744,16 @@ k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB,
         __nv_bfloat16 rh, rl, ih, il;
         split2(v.x, rh, rl);
         split2(v.y, ih, il);
-        __nv_bfloat16 *row = A + ((size_t)b * N + m) * 6 * NB + kc + kk;
+        __nv_bfloat16 *row = A + ((size_t)b * N + m) * 4 * NB + kc + kk;
         row[0 * NB] = rh; row[1 * NB] = ih;
-        row[2 * NB] = rh; row[3 * NB] = ih;
-        row[4 * NB] = rl; row[5 * NB] = il;
+        row[2 * NB] = rl; row[3 * NB] = il;
       }
     }
     __syncthreads();
   }
 }
 
-// B[b][n][6*NB] (real-part rows) and B[b][Ncap + n][6*NB] (imaginary-part rows)
+// B[b][n][4*NB] (real-part rows) and B[b][Ncap + n][4*NB] (imaginary-part rows)
 // for U rows J..J+jb-1 and columns n = 0..Ncols-1 (matrix columns J+jb+n)
 __global__ void __launch_bounds__(256)
 k_split_b(const z32 *M, size_t strideM, int N, int J, int jb, int Ncols, int Ncap, int NB,
@@ -768,10 +768,10 @@ k_split_b(const z32 *M, size_t strideM, int N, int J, int jb, int Ncols, int Nca
   split2(v.x, rh, rl);
   split2(v.y, ih, il);
   const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
-  __nv_bfloat16 *re = B + ((size_t)b * 2 * Ncap + n) * 6 * NB + k;
-  __nv_bfloat16 *im = B + ((size_t)b * 2 * Ncap + Ncap + n) * 6 * NB + k;
-  re[0 * NB] = rh; re[1 * NB] = nih; re[2 * NB] = rl; re[3 * NB] = nil; re[4 * NB] = rh; re[5 * NB] = nih;
-  im[0 * NB] = ih; im[1 * NB] = rh;  im[2 * NB] = il; im[3 * NB] = rl;  im[4 * NB] = ih; im[5 * NB] = rh;
+  __nv_bfloat16 *re = B + ((size_t)b * 2 * Ncap + n) * 4 * NB + k;
+  __nv_bfloat16 *im = B + ((size_t)b * 2 * Ncap + Ncap + n) * 4 * NB + k;
+  re[0 * NB] = rh; re[1 * NB] = nih; re[2 * NB] = rl; re[3 * NB] = nil;
+  im[0 * NB] = ih; im[1 * NB] = rh;  im[2 * NB] = il; im[3 * NB] = rl;
 }
 
 // ---------------------------------------------------------------------------
@@ -849,18 +849,18 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   c->M = M;
   c->lb = lb;
   c->Ncap = lb.ncols;
-  const size_t K6 = 6 * (size_t)lb.NB;
-  cudaError_t e = cudaMalloc(&c->A, sizeof(__nv_bfloat16) * K6 * lb.N * lb.batch);
-  if (e == cudaSuccess) e = cudaMalloc(&c->B, sizeof(__nv_bfloat16) * K6 * 2 * c->Ncap * lb.batch);
+  const size_t K4 = 4 * (size_t)lb.NB;       // four staging segments per step
+  cudaError_t e = cudaMalloc(&c->A, sizeof(__nv_bfloat16) * K4 * lb.N * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->B, sizeof(__nv_bfloat16) * K4 * 2 * c->Ncap * lb.batch);
   // second staging for the unpivoted path's delayed two-step updates
-  if (e == cudaSuccess) e = cudaMalloc(&c->A2, sizeof(__nv_bfloat16) * K6 * lb.N * lb.batch);
-  if (e == cudaSuccess) e = cudaMalloc(&c->B2, sizeof(__nv_bfloat16) * K6 * 2 * c->Ncap * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->A2, sizeof(__nv_bfloat16) * K4 * lb.N * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->B2, sizeof(__nv_bfloat16) * K4 * 2 * c->Ncap * lb.batch);
   if (e == cudaSuccess) e = cudaMalloc(&c->err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemsetAsync(c->err, 0, sizeof(int), st);
-  if (e == cudaSuccess && (!make_map(&c->mapA, c->A, K6, lb.N, lb.batch) ||
-                           !make_map(&c->mapB, c->B, K6, 2 * (uint64_t)c->Ncap, lb.batch) ||
-                           !make_map(&c->mapA2, c->A2, K6, lb.N, lb.batch) ||
-                           !make_map(&c->mapB2, c->B2, K6, 2 * (uint64_t)c->Ncap, lb.batch)))
+  if (e == cudaSuccess && (!make_map(&c->mapA, c->A, K4, lb.N, lb.batch) ||
+                           !make_map(&c->mapB, c->B, K4, 2 * (uint64_t)c->Ncap, lb.batch) ||
+                           !make_map(&c->mapA2, c->A2, K4, lb.N, lb.batch) ||
+                           !make_map(&c->mapB2, c->B2, K4, 2 * (uint64_t)c->Ncap, lb.batch)))
     e = cudaErrorInvalidValue;
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
@@ -905,11 +905,11 @@ cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, 
     const int nkb = 6 * NB / BK;
     k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapA, c->mapB, c->mapC, c->M,
                                                          lb.strideM, lb.N, J + jb, J + jb, 0, 0, 0, 0, nkb, Mrows,
-                                                         Ncols, c->Ncap, nkb, first, count, c->err);
+                                                         Ncols, c->Ncap, nkb, first, count, NB / BK, c->err);
   } else {
     dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), count);
     k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA, c->mapB, c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
-                                               c->Ncap, 6 * NB / BK, first, c->err);
+                                               c->Ncap, 6 * NB / BK, first, NB / BK, c->err);
   }
   e = ADGA_LAUNCH_CHECK();
   if (ev1) cudaEventRecord(ev1, st);
@@ -939,7 +939,7 @@ cudaError_t persist_region(TcCtx *c, bool two, int first, int count, int crow0, 
   k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapA2, c->mapB2, c->mapC, c->M,
                                                        lb.strideM, lb.N, crow0, ccol0, arow0, bcol0, arow2, bcol2,
                                                        nkb1, Mrows, Ncols, c->Ncap, two ? 2 * nkb1 : nkb1, first,
-                                                       count, c->err);
+                                                       count, lb.NB / BK, c->err);
   return ADGA_LAUNCH_CHECK();
 }
 
