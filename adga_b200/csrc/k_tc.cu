@@ -412,10 +412,11 @@ constexpr int TT_KBLK = TT_ROWS * 128;             // one K block: 128 rows x 64
 constexpr int TT_OPER = 4 * TT_KBLK;               // A hi, A lo, B hi, B lo of one K half: 64 KB
 constexpr int TT_SROW = 528;                       // padded stride of a staged 512 B operand row
 constexpr int TT_FROW = 528;                       // padded stride of a staged 512 B matrix column
-constexpr int TT_SMEM_BYTES = TT_OPER + 1024 + 64;
+constexpr int TT_STAGE = TT_ROWS * TT_SROW;         // epilogue staging: all 128 rows (67.6 KB)
+constexpr int TT_REGION = TT_STAGE > TT_OPER ? TT_STAGE : TT_OPER;
+constexpr int TT_SMEM_BYTES = TT_REGION + 1024 + 64;
 constexpr int TT_TMEM_COLS = 128;
-static_assert(64 * TT_SROW <= TT_OPER && 64 * TT_FROW <= TT_OPER,
-              "the epilogue stages 64 rows at a time in the operand buffers");
+static_assert(TT_SROW == TT_FROW, "operand rows and matrix columns are staged with one stride");
 // kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
 constexpr uint32_t IDESC_N128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 / 8) << 17) |
                                 ((uint32_t)(TT_ROWS / 16) << 24);
@@ -482,7 +483,8 @@ __device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat1
 // [Cr | Ci] = Xr [Wr | Wi] + Xi [-Wi | Wr] runs as two MMA phases over the
 // real and the imaginary part of X (64 KB of operands at a time, so two
 // CTAs share an SM and the load, MMA and store phases of different tiles
-// overlap); the epilogue stages 64 tile rows at a time.
+// overlap); the epilogue stages all 128 tile rows per round in the same
+// shared memory (67.6 KB).
 __global__ void __launch_bounds__(TT_THREADS, 2)
 k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
          const z32 *Uinv, __nv_bfloat16 *Astage, __nv_bfloat16 *Bstage, int Ncap, int b0, int ntA, int ntU,
@@ -491,7 +493,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gA = smraw + (sbase - smem_u32(smraw));    // A hi, A lo, B hi, B lo
   unsigned char *gB = gA + 2 * TT_KBLK;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(gA + TT_OPER);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(gA + TT_REGION);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
   const uint32_t sA = sbase, sB = sbase + 2 * TT_KBLK, sbar = smem_u32(bar);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -609,8 +611,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
 
   // ---- epilogue: warp w reads TMEM lanes 32 (w % 4).. (tile rows) and output columns
   //      32 (w / 4) .. + 31; the results reach global memory through shared memory (the
-  //      operand buffers, free once the MMAs completed), 64 tile rows per round, so that
-  //      every store is coalesced
+  //      operand buffers, free once the MMAs completed), so that every store is coalesced
   if (ok) {
     const int quad = warp & 3, half = warp >> 2;
     const int r = quad * 32 + lane;
@@ -624,90 +625,76 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
     };
     if (lower) {
+      unsigned char *row = stg + r * TT_SROW + n0 * 2;
 #pragma unroll 1
-      for (int rnd = 0; rnd < 2; ++rnd) {
-        if (rnd) __syncthreads();
-        if ((quad >> 1) == rnd) {
-          unsigned char *row = stg + (r - 64 * rnd) * TT_SROW + n0 * 2;
-#pragma unroll 1
-          for (int piece = 0; piece < 2; ++piece) {
-            float re[16], im[16];
-            tload(piece, re, im);
-            // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
-            if (r < nv) {
-              z32 *dst = Am + (size_t)(J + jb + m0 + r);
+      for (int piece = 0; piece < 2; ++piece) {
+        float re[16], im[16];
+        tload(piece, re, im);
+        // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
+        if (r < nv) {
+          z32 *dst = Am + (size_t)(J + jb + m0 + r);
 #pragma unroll
-              for (int j = 0; j < 16; ++j)
-                if (n0 + 16 * piece + j < jb)
-                  dst[(size_t)(J + n0 + 16 * piece + j) * N] = make_float2(re[j], im[j]);
-            }
-            // k_split_a's rows [Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-              const int o = 32 * piece + 16 * c;
-              *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 0, false);
-              *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 2, false);
-              *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 1, false);
-              *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 3, false);
-            }
-          }
+          for (int j = 0; j < 16; ++j)
+            if (n0 + 16 * piece + j < jb) dst[(size_t)(J + n0 + 16 * piece + j) * N] = make_float2(re[j], im[j]);
         }
-        __syncthreads();
-        copy_rows(stg, Astage + ((size_t)b * N + m0 + 64 * rnd) * 4 * NB, min(64, nv - 64 * rnd), t);
+        // k_split_a's rows [Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int o = 32 * piece + 16 * c;
+          *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 0, false);
+          *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 2, false);
+          *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 1, false);
+          *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 3, false);
+        }
       }
+      __syncthreads();
+      copy_rows(stg, Astage + ((size_t)b * N + m0) * 4 * NB, nv, t);
     } else {
       const int pc = jb / 2;                       // 16-byte pieces of a U12 column (jb is even)
-      // rounds 0, 1: U12 columns (rows 64 rnd ..); 2..5: k_split_b's real rows [Ur_hi, -Ui_hi,
-      // Ur_lo, -Ui_lo] and imaginary rows [Ui_hi, Ur_hi, Ui_lo, Ur_lo]
+      // round 0: the tile's U12 columns; 1, 2: k_split_b's real rows [Ur_hi, -Ui_hi, Ur_lo,
+      // -Ui_lo] and imaginary rows [Ui_hi, Ur_hi, Ui_lo, Ur_lo]
 #pragma unroll 1
-      for (int rnd = 0; rnd < 6; ++rnd) {
-        const int rh64 = rnd & 1;                  // tile rows 64 rh64 .. 64 rh64 + 63
+      for (int rnd = 0; rnd < 3; ++rnd) {
         if (rnd) __syncthreads();
-        if ((quad >> 1) == rh64) {
-          const int rr = r - 64 * rh64;
 #pragma unroll 1
-          for (int piece = 0; piece < 2; ++piece) {
-            float re[16], im[16];
-            tload(piece, re, im);
-            const int nn = n0 + 16 * piece;
-            if (rnd < 2) {
-              unsigned char *col = stg + rr * TT_FROW + nn * 8;
+        for (int piece = 0; piece < 2; ++piece) {
+          float re[16], im[16];
+          tload(piece, re, im);
+          const int nn = n0 + 16 * piece;
+          if (rnd == 0) {
+            unsigned char *col = stg + r * TT_FROW + nn * 8;
 #pragma unroll
-              for (int j = 0; j < 16; j += 2)
-                *reinterpret_cast<float4 *>(col + j * 8) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
-            } else {
-              unsigned char *row = stg + rr * TT_SROW + nn * 2;
-              const bool imag = rnd >= 4;
+            for (int j = 0; j < 16; j += 2)
+              *reinterpret_cast<float4 *>(col + j * 8) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
+          } else {
+            unsigned char *row = stg + r * TT_SROW + nn * 2;
 #pragma unroll
-              for (int c = 0; c < 2; ++c) {
-                const float *xr = re + 8 * c, *xi = im + 8 * c;
-                const int o = 16 * c;
-                if (!imag) {
-                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 0, false);
-                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 2, true);
-                  *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 1, false);
-                  *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 3, true);
-                } else {
-                  *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 2, false);
-                  *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 0, false);
-                  *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 3, false);
-                  *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 1, false);
-                }
+            for (int c = 0; c < 2; ++c) {
+              const float *xr = re + 8 * c, *xi = im + 8 * c;
+              const int o = 16 * c;
+              if (rnd == 1) {
+                *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 0, false);
+                *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 2, true);
+                *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 1, false);
+                *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 3, true);
+              } else {
+                *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 2, false);
+                *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 0, false);
+                *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 3, false);
+                *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 1, false);
               }
             }
           }
         }
         __syncthreads();
-        const int nrw = min(64, nv - 64 * rh64);
-        if (rnd < 2) {
-          for (int e = t; e < nrw * pc; e += TT_THREADS) {
+        if (rnd == 0) {
+          for (int e = t; e < nv * pc; e += TT_THREADS) {
             const int cc = e / pc, pp = e % pc;
-            *reinterpret_cast<float4 *>(Am + (size_t)(J + jb + m0 + 64 * rh64 + cc) * N + J + 2 * pp) =
+            *reinterpret_cast<float4 *>(Am + (size_t)(J + jb + m0 + cc) * N + J + 2 * pp) =
                 *reinterpret_cast<const float4 *>(stg + cc * TT_FROW + pp * 16);
           }
         } else {
-          copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (rnd >= 4 ? (size_t)Ncap : 0) + m0 + 64 * rh64) * 4 * NB,
-                    nrw, t);
+          copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (rnd == 2 ? (size_t)Ncap : 0) + m0) * 4 * NB, nv, t);
         }
       }
     }
