@@ -52,7 +52,7 @@ class RunStats(C.Structure):
 
 class Tune(C.Structure):
     _fields_ = [("factor", C.c_int), ("pairs", C.c_int), ("tri_tc", C.c_int), ("batch", C.c_int),
-                ("resid", C.c_int)]
+                ("resid", C.c_int), ("trsv_tc", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

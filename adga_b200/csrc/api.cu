@@ -33,6 +33,7 @@ static cudaError_t tc_trail_range_fn(void *r, int J, int jb, cudaStream_t st, cu
 void tc_trail_free(void *ctx);
 int tc_available();
 int tc_trail_error(void *ctx);
+int *tc_err_flag(void *ctx);
 int tc_pair_supported(void *ctx);
 cudaError_t tc_pair_narrow(void *ctx, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
                            cudaEvent_t ev0, cudaEvent_t ev1, bool staged);
@@ -115,7 +116,7 @@ struct adga_handle {
   bool refine_estimate = true;   // stop on the bounded next correction (ADGA_REFINE_EXACT=1: on a solved one)
   bool mixed_nopiv = true;   // FP32 factorisation without row interchanges (ADGA_MIXED_PIVOT=1: with)
   double tol = 1e-10;   // stop when max|dX| <= tol * max|X| (the error is then far below)
-  adga_tune tune{0, 1, 1, 0, 1};   // mixed-path kernel choices (adga_set_tune / adga_autotune)
+  adga_tune tune{0, 1, 1, 0, 1, 1};   // mixed-path kernel choices (adga_set_tune / adga_autotune)
   void *ri8 = nullptr;            // int8-slice residual context (k_resid_i8.cu), with the mixed work
   long long frow_gen = 0;         // bumped whenever F~ is recomputed (its residual slices go stale)
   // last-run statistics
@@ -314,6 +315,7 @@ extern "C" int adga_create(const adga_dims *d, const double *iw_data, const adga
   if (getenv("ADGA_NO_PAIRS")) h->tune.pairs = 0;
   if (getenv("ADGA_TRI_TILE")) h->tune.tri_tc = 0;
   if (getenv("ADGA_RESID_FP64")) h->tune.resid = 0;
+  if (getenv("ADGA_TRSV_STREAM")) h->tune.trsv_tc = 0;
   const char *ev = getenv("ADGA_NB");
   if (ev) h->NB = std::max(16, std::min(64, atoi(ev) / 8 * 8));   // the LU kernels assume NB <= 64
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1207,6 +1209,9 @@ static int run_batch(adga_handle *h, int iwb, int np, int off, int prec, int *st
                              strideM, h->gq, h->qidx_d, st, h->Frow32_m));
     cudaEventRecord(ev[2], st);
     CK(factor_batch<z32>(h, T, lb, true, h->tc != nullptr, &tt, h->mixed_nopiv));
+    // the solves of the FP32 factors on the tensor cores (tune.trsv_tc = 0: streaming solves)
+    lb.nopiv = h->mixed_nopiv;
+    lb.tc_err = h->tune.trsv_tc ? tc_err_flag(h->tc) : nullptr;
     CK(lu_backsolve<z32>(T, lb, T + N * N, strideM, (int)N, (int)R, st));
     CK(launch_init_x(T, strideM, (int)N, (int)R, 2 * np, h->X64, st));
     CK(lu_build_perm(lb, h->perm, st));
@@ -1477,8 +1482,8 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
 extern "C" int adga_set_tune(adga_handle *h, const adga_tune *t) {
   if (!h || !t) return ADGA_EINVAL;
   if (t->factor < 0 || t->factor > 1 || t->pairs < 0 || t->pairs > 1 || t->tri_tc < 0 || t->tri_tc > 1 ||
-      t->batch < 0 || t->resid < 0 || t->resid > 1)
-    return fail(h, ADGA_EINVAL, "adga_set_tune: factor, pairs, tri_tc, resid in {0, 1}, batch >= 0");
+      t->batch < 0 || t->resid < 0 || t->resid > 1 || t->trsv_tc < 0 || t->trsv_tc > 1)
+    return fail(h, ADGA_EINVAL, "adga_set_tune: factor, pairs, tri_tc, resid, trsv_tc in {0, 1}, batch >= 0");
   h->tune = *t;
   return 0;
 }
@@ -1531,21 +1536,22 @@ extern "C" int adga_autotune(adga_handle *h, int qwstart, int qwstop, double tol
   // candidates: the tensor-core variants (when the tensor cores serve this size), then
   // the FP64 factorisation
   std::vector<adga_tune> cand;
-  auto with = [&](int f, int p, int t, int rs) {
-    adga_tune x = start; x.factor = f; x.pairs = p; x.tri_tc = t; x.resid = rs; return x;
+  auto with = [&](int f, int p, int t, int rs, int ts) {
+    adga_tune x = start; x.factor = f; x.pairs = p; x.tri_tc = t; x.resid = rs; x.trsv_tc = ts; return x;
   };
   const bool tc = tc_available() && !getenv("ADGA_NO_TC");
   if (tc) {
     if (c.N % 2 == 0) {
-      cand.push_back(with(0, 1, 1, 1));
-      cand.push_back(with(0, 1, 1, 0));
+      cand.push_back(with(0, 1, 1, 1, 1));
+      cand.push_back(with(0, 1, 1, 1, 0));
+      cand.push_back(with(0, 1, 1, 0, 1));
     }
-    cand.push_back(with(0, 1, 0, 1));
-    cand.push_back(with(0, 0, 0, 1));
+    cand.push_back(with(0, 1, 0, 1, 0));
+    cand.push_back(with(0, 0, 0, 1, 0));
   } else {
-    cand.push_back(with(0, 0, 0, 0));
+    cand.push_back(with(0, 0, 0, 0, 0));
   }
-  cand.push_back(with(1, 0, 0, 0));
+  cand.push_back(with(1, 0, 0, 0, 0));
   std::vector<z64> ref_chi, ref_sig, chi, sig;
   double ms = 0.0;
   h->tune = start;

@@ -1156,6 +1156,11 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
 template <typename T>
 static cudaError_t trisolve(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
                             bool upper, T *work, cudaStream_t st) {
+  // FP32 factors, up to 16 right-hand sides: the tensor-core solve (k_trsv_tc.cu)
+  if constexpr (sizeof(T) == sizeof(z32))
+    if (trsv_tc_supported(lb, R, upper))
+      return launch_trsv_tc(reinterpret_cast<const z32 *>(M), lb, reinterpret_cast<z32 *>(C), strideC, ldc, R,
+                            upper, st);
   // few right-hand sides and NB = 64: the streaming solve (k_trsv.cu)
   if (trsv_stream_supported<T>(lb, strideC, R, upper, lb.perm, work))
     return launch_trsv_stream<T>(M, lb, C, strideC, ldc, R, upper, lb.perm, work, st);

@@ -287,26 +287,9 @@ k_resid_i8(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUt
   }
 }
 
-typedef CUresult (*encode_fn_t)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
-                                CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
-                                CUtensorMapFloatOOBfill);
-
-encode_fn_t get_encode_ri() {
-  static encode_fn_t fn = nullptr;
-  if (!fn) {
-    cudaDriverEntryPointQueryResult q;
-    void *p = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (encode_fn_t)p;
-  }
-  return fn;
-}
-
 // int8 slices [planes][rows][K2p], box 64 B x box_rows, 64 B swizzle
 bool make_map_i8(CUtensorMap *map, void *base, uint64_t K2p, uint64_t rows, uint64_t planes, uint32_t box_rows) {
-  encode_fn_t enc = get_encode_ri();
+  encode_fn_t enc = tmap_encoder();
   if (!enc) return false;
   cuuint64_t dims[3] = {K2p, rows, planes};
   cuuint64_t strides[2] = {K2p, K2p * rows};

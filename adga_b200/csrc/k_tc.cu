@@ -775,25 +775,8 @@ struct TcCtx {
   CUtensorMap mapA2, mapB2;
 };
 
-typedef CUresult (*encode_fn_t)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
-                                CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
-                                CUtensorMapFloatOOBfill);
-
-encode_fn_t get_encode() {
-  static encode_fn_t fn = nullptr;
-  if (!fn) {
-    cudaDriverEntryPointQueryResult q;
-    void *p = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (encode_fn_t)p;
-  }
-  return fn;
-}
-
 bool make_map(CUtensorMap *map, void *base, uint64_t inner, uint64_t rows, uint64_t batch) {
-  encode_fn_t enc = get_encode();
+  encode_fn_t enc = tmap_encoder();
   if (!enc) return false;
   cuuint64_t dims[3] = {inner, rows, batch};
   cuuint64_t strides[2] = {inner * 2, inner * rows * 2};
@@ -807,7 +790,7 @@ bool make_map(CUtensorMap *map, void *base, uint64_t inner, uint64_t rows, uint6
 
 // C as FP32: dims (2N floats per column, columns, matrices), box 128 rows x 64 columns
 bool make_map_c(CUtensorMap *map, void *base, uint64_t N, uint64_t ncols, uint64_t strideM, uint64_t batch) {
-  encode_fn_t enc = get_encode();
+  encode_fn_t enc = tmap_encoder();
   if (!enc) return false;
   cuuint64_t dims[3] = {2 * N, ncols, batch};
   cuuint64_t strides[2] = {N * 8, strideM * 8};
@@ -826,7 +809,7 @@ int tc_available() {
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
   cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
-  return (major == 10 && minor == 0 && get_encode() != nullptr) ? 1 : 0;
+  return (major == 10 && minor == 0 && tmap_encoder() != nullptr) ? 1 : 0;
 }
 
 cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream_t st) {
@@ -1006,6 +989,9 @@ int tc_trail_error(void *ctxp) {
   if (cudaMemcpy(&v, c->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
   return v;
 }
+
+// the device flag the tensor-core kernels' bounded waits report to
+int *tc_err_flag(void *ctxp) { return ctxp ? ((TcCtx *)ctxp)->err : nullptr; }
 
 void tc_trail_free(void *ctxp) {
   TcCtx *c = (TcCtx *)ctxp;

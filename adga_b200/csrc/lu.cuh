@@ -27,6 +27,9 @@ struct LUBatch {
   void *Linv, *Uinv;        // [batch][nsteps][NB*NB] of the element type
   int *rmap;                // [batch][RMAP_STRIDE]
   int *perm = nullptr;      // [batch][N] row i of P B = row perm[i] of B (lu_build_perm); optional
+  bool nopiv = false;       // factored without row interchanges (P = 1)
+  int *tc_err = nullptr;    // FP32 solves on the tensor cores (k_trsv_tc.cu) where they apply:
+                            // the device flag their bounded waits report to; null: streaming solves
   int nsteps() const { return (N + NB - 1) / NB; }
 };
 
@@ -97,6 +100,11 @@ cudaError_t lu_build_perm(const LUBatch &lb, int *perm, cudaStream_t st);
 template <typename T>
 bool trsv_stream_supported(const LUBatch &lb, size_t strideC, int R, bool upper, const int *perm,
                            const T *work);
+// tensor-core solves of FP32 factors (k_trsv_tc.cu): NB = 64, R <= 16, N <= 1088 and even,
+// the forward one only without row interchanges; needs lb.tc_err
+bool trsv_tc_supported(const LUBatch &lb, int R, bool upper);
+cudaError_t launch_trsv_tc(const z32 *M, const LUBatch &lb, z32 *C, size_t strideC, int ldc, int R, bool upper,
+                           cudaStream_t st);
 template <typename T>
 cudaError_t launch_trsv_stream(const T *M, const LUBatch &lb, T *C, size_t strideC, int ldc, int R,
                                bool upper, const int *perm, T *work, cudaStream_t st);

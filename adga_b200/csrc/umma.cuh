@@ -5,6 +5,7 @@
 // No load here uses cluster multicast.
 #pragma once
 #include <cuda.h>
+#include <cuda_runtime.h>
 #include <cstdint>
 
 namespace umma {
@@ -76,5 +77,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// the driver's cuTensorMapEncodeTiled, looked up once through the runtime
+typedef CUresult (*encode_fn_t)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                CUtensorMapFloatOOBfill);
+inline encode_fn_t tmap_encoder() {
+  static encode_fn_t fn = [] {
+    cudaDriverEntryPointQueryResult q;
+    void *p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      return (encode_fn_t)p;
+    return (encode_fn_t) nullptr;
+  }();
+  return fn;
+}
 
 }  // namespace umma

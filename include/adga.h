@@ -228,11 +228,15 @@ int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
  *   batch   points per batch (0: as many as 60% of the free memory holds)
  *   resid   1: the FP64 refinement residual's product X D F~ formed exactly
  *              from int8 slices on the tensor cores; 0: FP64 CUDA-core GEMM
- * A new handle starts at {0, 1, 1, 0, 1} (the environment switches
- * ADGA_NO_PAIRS, ADGA_TRI_TILE, ADGA_BATCH and ADGA_RESID_FP64 override it).
+ *   trsv_tc 1: the triangular solves of the FP32 factors on the tensor cores
+ *              (3-term TF32 split; N <= 1088, ndim^2 <= 16); 0: streaming
+ *              CUDA-core solves
+ * A new handle starts at {0, 1, 1, 0, 1, 1} (the environment switches
+ * ADGA_NO_PAIRS, ADGA_TRI_TILE, ADGA_BATCH, ADGA_RESID_FP64 and
+ * ADGA_TRSV_STREAM override it).
  */
 typedef struct adga_tune {
-  int factor, pairs, tri_tc, batch, resid;
+  int factor, pairs, tri_tc, batch, resid, trsv_tc;
 } adga_tune;
 typedef struct adga_tune_trial {
   adga_tune tune;

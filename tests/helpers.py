@@ -47,7 +47,8 @@ def rel_err(a, b):
 
 
 LIBRARY_ENV = ("ADGA_DFT_MIN_POINTS", "ADGA_BUBBLE", "ADGA_MIXED_PIVOT", "ADGA_MAX_REFINE",
-               "ADGA_REFINE_EXACT", "ADGA_NO_PAIRS", "ADGA_TRI_TILE", "ADGA_BATCH", "ADGA_RESID_FP64")
+               "ADGA_REFINE_EXACT", "ADGA_NO_PAIRS", "ADGA_TRI_TILE", "ADGA_BATCH", "ADGA_RESID_FP64",
+               "ADGA_TRSV_STREAM")
 
 
 @contextlib.contextmanager
