@@ -976,8 +976,12 @@ static int tan_work(adga_handle *h) {
 // dX = r A^-1 for the tangents of a mixed batch: the forward pass's FP32
 // factors and FP64 refinement against 1 - D F~ with r in place of (1+gamma^w)
 // (the residual r - dX + (dX D) F~), the same stopping rules as the forward
-// refinement.  Matrices flagged in skip (points the forward re-solves in FP64)
-// are left out of the convergence test.
+// refinement, with up to kTanIterFactor times the forward's sweeps (a tangent's
+// relative error starts where the forward's starts, but its right-hand side
+// may be small beside the solve's scale, which takes the relative test longer).
+// Matrices flagged in skip (points the forward re-solves in FP64) are left out
+// of the convergence test.
+constexpr int kTanIterFactor = 3;
 static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 *chi0q, int np, const z64 *r,
                            z64 *dX, const std::vector<char> &skip) {
   DevCtx &c = h->c;
@@ -994,7 +998,9 @@ static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 
   CK(lu_backsolve<z32>(T, lb, h->V32, per, (int)N, (int)R, st));
   CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
   CK(launch_update((int)per, nmat, h->V32, dX, h->norms, nullptr, st));
-  for (int it = 0; it < h->max_iter; ++it) {
+  int nbad = 0, wbad = -1;
+  double wrel = 0.0;
+  for (int it = 0; it < kTanIterFactor * h->max_iter; ++it) {
     CK(cudaMemsetAsync(h->norms, 0, sizeof(unsigned long long) * 2 * nmat, st));
     CK(cudaMemsetAsync(rnorm, 0, sizeof(unsigned long long) * nmat, st));
     CK(launch_residual(c, np, dX, chi0q, h->c0inv, h->Frow_d, h->Frow_m, h->opg_d, h->opg_m, h->XD, h->V32,
@@ -1019,7 +1025,9 @@ static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 
       CK(cudaMemcpyAsync(nh.data() + 2 * nmat, rnorm, sizeof(unsigned long long) * nmat, cudaMemcpyDeviceToHost,
                          st));
     CK(cudaStreamSynchronize(st));
-    bool all = true;
+    nbad = 0;
+    wbad = -1;
+    wrel = 0.0;
     for (int m = 0; m < nmat; ++m) {
       const double md = bits(nh[2 * m]), mx = bits(nh[2 * m + 1]);
       xmax[m] = mx;
@@ -1027,11 +1035,21 @@ static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 
         const double r1 = bits(nh[2 * nmat + m]);
         rho[m] = r1 > 0 ? md / r1 : 1.0;
       }
-      if (!skip[m] && !((mx > 0 ? md / mx : md) <= h->tol)) all = false;
+      const double rel = mx > 0 ? md / mx : md;
+      if (!skip[m] && !(rel <= h->tol)) {
+        ++nbad;
+        if (!(rel <= wrel)) { wrel = rel; wbad = m; }
+      }
     }
-    if (all) return 0;
+    if (!nbad) return 0;
   }
-  return fail(h, ADGA_ENOCONV, "tangent refinement did not converge");
+  char msg[256];
+  snprintf(msg, sizeof msg,
+           "tangent refinement did not converge: %d of %d matrices after %d sweeps (worst: matrix %d, "
+           "max|correction| / max|dX| = %.3g, max|dX| = %.3g, first-sweep amplification %.3g)",
+           nbad, nmat, kTanIterFactor * h->max_iter, wbad, wrel, wbad >= 0 ? xmax[wbad] : 0.0,
+           wbad >= 0 ? rho[wbad] : 0.0);
+  return fail(h, ADGA_ENOCONV, msg);
 }
 
 // the tangent of direction d for one batch, after its forward pass.  FP64: T holds
