@@ -11,6 +11,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libadga_b200.so"
 
 ADGA_FP64, ADGA_MIXED = 0, 1
+ADGA_ENOCONV = -6
 ERRORS = {-1: "ADGA_EINVAL", -2: "ADGA_ECUDA", -3: "ADGA_ENOMEM", -4: "ADGA_ETIMEOUT",
           -5: "ADGA_ESTATE", -6: "ADGA_ENOCONV"}
 

@@ -1015,7 +1015,10 @@ static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 
         const double est = kEstSafety * std::max(rho[m], 1.0) * bits(nh[2 * nmat + m]);
         if (!((xmax[m] > 0 ? est / xmax[m] : est) <= h->tol)) all = false;
       }
-      if (all) return 0;
+      if (all) {
+        h->stats.max_refine_iters = std::max(h->stats.max_refine_iters, it + 1);
+        return 0;
+      }
     }
     CK(lu_fwdsolve_ws<z32>(T, lb, h->V32, per, (int)N, (int)R, h->work32, st));
     CK(lu_backsolve<z32>(T, lb, h->V32, per, (int)N, (int)R, st));
@@ -1041,7 +1044,11 @@ static int tan_solve_mixed(adga_handle *h, z32 *T, const LUBatch &lb, const z64 
         if (!(rel <= wrel)) { wrel = rel; wbad = m; }
       }
     }
-    if (!nbad) return 0;
+    if (!nbad) {
+      // the run's refinement statistics cover the tangent solves too
+      h->stats.max_refine_iters = std::max(h->stats.max_refine_iters, it + 1);
+      return 0;
+    }
   }
   char msg[256];
   snprintf(msg, sizeof msg,

@@ -11,7 +11,9 @@ in the same pass (`adga_ladder_run_tangent`), then, on the same handle, the
 FP64 ladder with the same tangents, which gives the per-point error of the
 mixed outputs and gradients.  Throughput counts mixed device time only.  The
 mixed path's kernel choices come from the autotuner, measured once per
-(orbital count, BSE size) on the first point of that size and reused.
+(orbital count, BSE size) on the first point of that size and reused.  A
+point whose tangent refinement does not converge (the library's
+ADGA_ENOCONV) runs its pass again in FP64, recorded as 'fp64_pass'.
 
     python -m adga_b200.sweep [--points 64] [--omegas all|0] [--no-fp64] [--json FILE]
 """
@@ -26,7 +28,8 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 from . import synth
-from .ladder import Ladder
+from ._lib import ADGA_ENOCONV
+from .ladder import AdgaError, Ladder
 
 GRAD_PARAMS = ("U", "J")
 
@@ -104,10 +107,21 @@ def run_point(prepared, omegas, check_fp64=True, keep=False, tune_cache=None, pr
             if dv:
                 for iwb, (a, b) in dv.items():
                     lad.set_vertex_tangent(iwb, a, b, direction=dr)
-        ms, iters, fb, mx = _run_pass(lad, prob, ranges, "mixed", probe)
+        fell_back = None
+        try:
+            ms, iters, fb, mx = _run_pass(lad, prob, ranges, "mixed", probe)
+        except AdgaError as e:
+            # a tangent refinement that does not converge: the point's pass again in FP64
+            # (its accumulators restart from zero), timed as this point's mixed time
+            if e.code != ADGA_ENOCONV:
+                raise
+            fell_back = str(e)
+            ms, iters, fb, mx = _run_pass(lad, prob, ranges, "fp64", probe)
         rec = dict(name=s.name, ndim=s.ndim, iwf=s.iwf, beta=s.beta, U=s.U, J=s.J, N=N, points=npts,
                    ms_mixed=ms, pts_per_s=npts / (ms * 1e-3), max_refine_iters=iters, mixed_fallbacks=fb,
                    tune=lad.tune)
+        if fell_back:
+            rec["fp64_pass"] = fell_back
         if tuned:
             rec["autotune"] = tuned
         if mx["probe"] is not None:

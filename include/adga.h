@@ -185,7 +185,8 @@ typedef struct adga_run_stats {
   int points;                  /* (q, omega) points processed                  */
   int lu_info_nonzero;         /* points whose LU hit an exactly-zero pivot    */
   int mixed_fallbacks;         /* mixed points re-solved in FP64               */
-  int max_refine_iters;        /* largest count of FP64 residuals of a batch   */
+  int max_refine_iters;        /* largest count of FP64 residuals of a batch
+                                  (its tangent solves included)                */
   double max_refine_resid;     /* largest final relative correction, or its
                                   bound when the last solve was skipped        */
   double ms_total;             /* device time of the run (CUDA events)         */
