@@ -189,30 +189,26 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
 // ---------------------------------------------------------------------------
 // Persistent variant: one CTA per SM loops over the (column tile, row tile,
-// matrix) tiles of the launch.  The operand k-blocks stream through a
-// 4-stage TMA ring (192 KB), the accumulator is double-buffered in TMEM
-// (2 x 256 columns), so the epilogue of one tile overlaps the loads and MMAs
-// of the next; the C tile is prefetched into L2 when its operand loads start
-// and read from there by the epilogue, next to the TMEM accumulator.
-//   warp 0        TMA loads of the A/B k-blocks, L2 prefetch of the C tile
+// matrix) tiles of the launch.  The C tile of each output tile is brought
+// into shared memory by TMA (two 64-column halves) while the MMAs of that
+// tile run, and the accumulator is double-buffered in TMEM (2 x 256
+// columns), so the epilogue of one tile overlaps the loads and MMAs of the
+// next and the C read-modify-write no longer waits on DRAM latency.
+//   warp 0        TMA loads of the A/B k-blocks (ring of P_STAGES)
 //   warp 1        TMEM allocation (512 columns) and tcgen05.mma issue
-//   warps 4..11   epilogue: group h = 0, 1 owns C columns 64 h.., warp w reads
-//                 TMEM lanes 32*(w%4)..; C - acc is stored straight to global
+//   warp 2        TMA loads of the C halves
+//   warps 4..11   epilogue: group h = 0, 1 owns C half h, warp w reads TMEM
+//                 lanes 32*(w%4)..; C - acc is stored straight to global
 // Every wait is bounded (WAIT_NS); on a timeout a role records an error and
 // stops issuing work.
 // ---------------------------------------------------------------------------
-constexpr int P_STAGES = 4;
-constexpr int P_CH_COLS = 64;                         // columns per epilogue group
+constexpr int P_STAGES = 2;
+constexpr int P_CH_COLS = 64;                         // columns per C half
+constexpr int P_CH_BYTES = BM * 8 * P_CH_COLS;        // 64 KB of complex FP32
 constexpr int P_TMEM_COLS = 2 * TMEM_COLS;            // two accumulators
 constexpr int P_THREADS = 384;
-constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + 2 * P_CH_BYTES + 1024 + 256;
 
-__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x, int y, int z) {
-  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
-                   (unsigned long long)map),
-               "r"(x), "r"(y), "r"(z)
-               : "memory");
-}
 
 __global__ void __launch_bounds__(P_THREADS, 1)
 k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
@@ -223,11 +219,15 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
-  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + P_STAGES * STAGE_BYTES);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * P_STAGES + 4);
+  const uint32_t scbase = sbase + P_STAGES * STAGE_BYTES;           // the two C halves
+  const unsigned char *gc = gbase + P_STAGES * STAGE_BYTES;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + P_STAGES * STAGE_BYTES + 2 * P_CH_BYTES);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * P_STAGES + 8);
   const uint32_t bar_full = smem_u32(bars), bar_empty = bar_full + 8 * P_STAGES;
   const uint32_t bar_accf = bar_empty + 8 * P_STAGES;   // [2]
   const uint32_t bar_acce = bar_accf + 16;              // [2]
+  const uint32_t bar_cfull = bar_acce + 16;             // [2]
+  const uint32_t bar_cempty = bar_cfull + 16;           // [2]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntn = (Ncols + BN - 1) / BN, ntm = (Mrows + BM - 1) / BM;
   const int ntiles = ntn * ntm * count;
@@ -240,6 +240,8 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
     for (int a = 0; a < 2; ++a) {
       mbar_init(bar_accf + 8 * a, 1);
       mbar_init(bar_acce + 8 * a, 8);      // one arrival per epilogue warp
+      mbar_init(bar_cfull + 8 * a, 1);
+      mbar_init(bar_cempty + 8 * a, 4);    // one arrival per warp of the group
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -258,10 +260,6 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
       int kbt = 0;
       for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
-        // the tile's C (two 64-column boxes) into L2 for the epilogue; x counts floats: rows
-        // crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
-        tma_prefetch_l2_3d(&mapC, 2 * (crow0 + tm * BM), ccol0 + tn * BN, b);
-        tma_prefetch_l2_3d(&mapC, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
         bool ok = true;
         for (int kb = 0; kb < nkb; ++kb, ++kbt) {
           const int s = kbt % P_STAGES;
@@ -305,52 +303,69 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
         mma_commit(bar_accf + 8 * a);
       }
     }
+  } else if (warp == 2) {
+    if (lane == 0) {
+      int it = 0;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
+        bool ok = true;
+        for (int h = 0; h < 2 && ok; ++h) {
+          if (it > 0) ok = mbar_wait(bar_cempty + 8 * h, (it - 1) & 1, err, 14);
+          if (!ok) break;
+          mbar_expect_tx(bar_cfull + 8 * h, P_CH_BYTES);
+          // x counts floats: rows crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
+          tma_load_3d(scbase + h * P_CH_BYTES, &mapC, bar_cfull + 8 * h, 2 * (crow0 + tm * BM),
+                      ccol0 + tn * BN + h * P_CH_COLS, b);
+        }
+        if (!ok) break;
+      }
+    }
   } else if (warp >= 4) {
     const int e = warp - 4, h = e >> 2, quad = warp & 3;
     const int row = quad * 32 + lane;
+    const z32 *cs = reinterpret_cast<const z32 *>(gc + h * P_CH_BYTES);   // [col][128 rows]
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
       const int a = it & 1;
-      // the warp leaves together if any lane gave up, so tcgen05.ld stays warp-wide
-      const bool ok = mbar_wait(bar_accf + 8 * a, (it >> 1) & 1, err, 15);
+      // every lane waits (and so observes the TMA-written C half); the warp
+      // leaves together if any lane gave up, so tcgen05.ld stays warp-wide
+      bool ok = mbar_wait(bar_accf + 8 * a, (it >> 1) & 1, err, 15);
+      ok = ok && mbar_wait(bar_cfull + 8 * h, it & 1, err, 16);
       if (!__all_sync(0xffffffffu, ok)) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int m = tm * BM + row;
       const bool rowok = m < Mrows;
-      const int nbase = tn * BN + h * P_CH_COLS;
-      const int nv = rowok ? min(P_CH_COLS, Ncols - nbase) : 0;     // valid columns of this row
-      z32 *Cb = M + (size_t)b * strideM + (size_t)(crow0 + m) + (size_t)(ccol0 + nbase) * N;
+      z32 *Cb = M + (size_t)b * strideM + (size_t)(crow0 + m);
       const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * TMEM_COLS + h * P_CH_COLS);
-      // C of a 16-column chunk (a warp reads 32 consecutive rows of a column), the next
-      // chunk's loads in flight while one chunk is finished
-      z32 cv[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) cv[j] = j < nv ? Cb[j * N] : make_float2(0.f, 0.f);
+      const int nbase = tn * BN + h * P_CH_COLS;
 #pragma unroll 1
       for (int c = 0; c < P_CH_COLS; c += 16) {
         float re[16], im[16];
         tmem_ld16(tl + c, re);
         tmem_ld16(tl + BN + c, im);
-        z32 cn[16];
-        if (c + 16 < P_CH_COLS) {
+        z32 cv[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            cn[j] = c + 16 + j < nv ? Cb[(c + 16 + j) * N] : make_float2(0.f, 0.f);
-        }
+        for (int j = 0; j < 16; ++j) cv[j] = cs[(c + j) * BM + row];
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-          if (c + j < nv) Cb[(c + j) * N] = make_float2(cv[j].x - re[j], cv[j].y - im[j]);
-        if (c + 16 < P_CH_COLS) {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) cv[j] = cn[j];
+        for (int j = 0; j < 16; ++j) {
+          const int n = nbase + c + j;
+          if (rowok && n < Ncols) {
+            z32 v = cv[j];
+            v.x -= re[j];
+            v.y -= im[j];
+            Cb[(size_t)(ccol0 + n) * N] = v;
+          }
         }
       }
-      // this warp is done with the accumulator
+      // this warp is done with the C half and with the accumulator
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
-      if (lane == 0) mbar_arrive(bar_acce + 8 * a);
+      if (lane == 0) {
+        mbar_arrive(bar_cempty + 8 * h);
+        mbar_arrive(bar_acce + 8 * a);
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
