@@ -189,25 +189,34 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
 // ---------------------------------------------------------------------------
 // Persistent variant: one CTA per SM loops over the (column tile, row tile,
-// matrix) tiles of the launch.  The C tile of each output tile is brought
-// into shared memory by TMA (two 64-column halves) while the MMAs of that
-// tile run, and the accumulator is double-buffered in TMEM (2 x 256
-// columns), so the epilogue of one tile overlaps the loads and MMAs of the
-// next and the C read-modify-write no longer waits on DRAM latency.
+// matrix) tiles of the launch.  The operand k-blocks stream through a
+// 3-stage TMA ring (144 KB); the accumulator is double-buffered in TMEM
+// (2 x 256 columns), so the epilogue of one tile overlaps the loads and MMAs
+// of the next.  The C tile reaches shared memory by TMA one 64-column half at
+// a time through one 64 KB buffer (the second half is prefetched into L2
+// when the first is loaded).
 //   warp 0        TMA loads of the A/B k-blocks (ring of P_STAGES)
 //   warp 1        TMEM allocation (512 columns) and tcgen05.mma issue
 //   warp 2        TMA loads of the C halves
-//   warps 4..11   epilogue: group h = 0, 1 owns C half h, warp w reads TMEM
-//                 lanes 32*(w%4)..; C - acc is stored straight to global
+//   warps 4..11   epilogue: per half, group g = 0, 1 owns its columns 32 g..,
+//                 warp w reads TMEM lanes 32*(w%4)..; C - acc is stored
+//                 straight to global
 // Every wait is bounded (WAIT_NS); on a timeout a role records an error and
 // stops issuing work.
 // ---------------------------------------------------------------------------
-constexpr int P_STAGES = 2;
+constexpr int P_STAGES = 3;
 constexpr int P_CH_COLS = 64;                         // columns per C half
 constexpr int P_CH_BYTES = BM * 8 * P_CH_COLS;        // 64 KB of complex FP32
 constexpr int P_TMEM_COLS = 2 * TMEM_COLS;            // two accumulators
 constexpr int P_THREADS = 384;
-constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + 2 * P_CH_BYTES + 1024 + 256;
+constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + P_CH_BYTES + 1024 + 256;
+
+__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                   (unsigned long long)map),
+               "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
 
 
 __global__ void __launch_bounds__(P_THREADS, 1)
@@ -221,7 +230,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
   const uint32_t scbase = sbase + P_STAGES * STAGE_BYTES;           // the two C halves
   const unsigned char *gc = gbase + P_STAGES * STAGE_BYTES;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + P_STAGES * STAGE_BYTES + 2 * P_CH_BYTES);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + P_STAGES * STAGE_BYTES + P_CH_BYTES);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * P_STAGES + 8);
   const uint32_t bar_full = smem_u32(bars), bar_empty = bar_full + 8 * P_STAGES;
   const uint32_t bar_accf = bar_empty + 8 * P_STAGES;   // [2]
@@ -240,9 +249,9 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
     for (int a = 0; a < 2; ++a) {
       mbar_init(bar_accf + 8 * a, 1);
       mbar_init(bar_acce + 8 * a, 8);      // one arrival per epilogue warp
-      mbar_init(bar_cfull + 8 * a, 1);
-      mbar_init(bar_cempty + 8 * a, 4);    // one arrival per warp of the group
     }
+    mbar_init(bar_cfull, 1);
+    mbar_init(bar_cempty, 8);              // one arrival per epilogue warp
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -310,62 +319,70 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
         const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
         bool ok = true;
         for (int h = 0; h < 2 && ok; ++h) {
-          if (it > 0) ok = mbar_wait(bar_cempty + 8 * h, (it - 1) & 1, err, 14);
+          // use u = 2 it + h of the one C buffer: the epilogue has released use u - 1
+          const int u = 2 * it + h;
+          if (u > 0) ok = mbar_wait(bar_cempty, (u - 1) & 1, err, 14);
           if (!ok) break;
-          mbar_expect_tx(bar_cfull + 8 * h, P_CH_BYTES);
+          mbar_expect_tx(bar_cfull, P_CH_BYTES);
           // x counts floats: rows crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
-          tma_load_3d(scbase + h * P_CH_BYTES, &mapC, bar_cfull + 8 * h, 2 * (crow0 + tm * BM),
-                      ccol0 + tn * BN + h * P_CH_COLS, b);
+          tma_load_3d(scbase, &mapC, bar_cfull, 2 * (crow0 + tm * BM), ccol0 + tn * BN + h * P_CH_COLS, b);
+          if (h == 0)
+            tma_prefetch_l2_3d(&mapC, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
         }
         if (!ok) break;
       }
     }
   } else if (warp >= 4) {
-    const int e = warp - 4, h = e >> 2, quad = warp & 3;
+    const int e = warp - 4, grp = e >> 2, quad = warp & 3;
     const int row = quad * 32 + lane;
-    const z32 *cs = reinterpret_cast<const z32 *>(gc + h * P_CH_BYTES);   // [col][128 rows]
+    const z32 *cs = reinterpret_cast<const z32 *>(gc);   // [col][128 rows] of the current half
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
       const int a = it & 1;
-      // every lane waits (and so observes the TMA-written C half); the warp
-      // leaves together if any lane gave up, so tcgen05.ld stays warp-wide
+      // the warp leaves together if any lane gave up, so tcgen05.ld stays warp-wide
       bool ok = mbar_wait(bar_accf + 8 * a, (it >> 1) & 1, err, 15);
-      ok = ok && mbar_wait(bar_cfull + 8 * h, it & 1, err, 16);
       if (!__all_sync(0xffffffffu, ok)) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int m = tm * BM + row;
       const bool rowok = m < Mrows;
       z32 *Cb = M + (size_t)b * strideM + (size_t)(crow0 + m);
-      const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * TMEM_COLS + h * P_CH_COLS);
-      const int nbase = tn * BN + h * P_CH_COLS;
+      for (int h = 0; h < 2 && ok; ++h) {
+        // every lane waits (and so observes the TMA-written C half)
+        ok = mbar_wait(bar_cfull, (2 * it + h) & 1, err, 16);
+        if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
+        const int c0 = h * P_CH_COLS + grp * 32;            // accumulator column of this warp's part
+        const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * TMEM_COLS + c0);
+        const int nbase = tn * BN + c0;
 #pragma unroll 1
-      for (int c = 0; c < P_CH_COLS; c += 16) {
-        float re[16], im[16];
-        tmem_ld16(tl + c, re);
-        tmem_ld16(tl + BN + c, im);
-        z32 cv[16];
+        for (int c = 0; c < 32; c += 16) {
+          float re[16], im[16];
+          tmem_ld16(tl + c, re);
+          tmem_ld16(tl + BN + c, im);
+          z32 cv[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) cv[j] = cs[(c + j) * BM + row];
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          for (int j = 0; j < 16; ++j) cv[j] = cs[(grp * 32 + c + j) * BM + row];
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int n = nbase + c + j;
-          if (rowok && n < Ncols) {
-            z32 v = cv[j];
-            v.x -= re[j];
-            v.y -= im[j];
-            Cb[(size_t)(ccol0 + n) * N] = v;
+          for (int j = 0; j < 16; ++j) {
+            const int n = nbase + c + j;
+            if (rowok && n < Ncols) {
+              z32 v = cv[j];
+              v.x -= re[j];
+              v.y -= im[j];
+              Cb[(size_t)(ccol0 + n) * N] = v;
+            }
           }
         }
+        // this warp is done with the C half
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar_cempty);
       }
-      // this warp is done with the C half and with the accumulator
+      if (!ok) break;
+      // and with the accumulator
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
-      if (lane == 0) {
-        mbar_arrive(bar_cempty + 8 * h);
-        mbar_arrive(bar_acce + 8 * a);
-      }
+      if (lane == 0) mbar_arrive(bar_acce + 8 * a);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -391,9 +408,9 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
 //                                   of the step's jb rows
 // with U11^-1 / L11^-1 the 64 x 64 block inverses of k_diag_inv.  One CTA per
 // tile of 128 rows (mode 0) or 128 columns (mode 1) of one matrix, K = 64:
-//   * every thread loads its part of the FP32 tile from the matrix (coalesced),
-//     splits each value into bf16 hi + lo and writes the K-major, 128 B
-//     swizzled A operand [Xr_hi | Xi_hi | Xr_lo | Xi_lo] (four 64-wide K blocks);
+//   * every thread (512 per CTA, two CTAs per SM) loads its 16 values of the
+//     FP32 tile from the matrix (coalesced), splits each into bf16 hi + lo
+//     and writes the K-major, 128 B swizzled A operand;
 //   * the block inverse W becomes the B operand, real-part rows
 //     [Wr | -Wi] and imaginary-part rows [Wi | Wr], hi and lo K blocks;
 //   * one thread issues 24 MMAs (M = 128, N = 128, K = 16): the (hi, hi),
@@ -406,7 +423,7 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
 // The wait on the MMAs is bounded (WAIT_NS); on a timeout the CTA records an
 // error and skips its epilogue.
 // ---------------------------------------------------------------------------
-constexpr int TT_THREADS = 256;
+constexpr int TT_THREADS = 512;
 constexpr int TT_ROWS = 128;                       // tile rows (MMA M)
 constexpr int TT_KBLK = TT_ROWS * 128;             // one K block: 128 rows x 64 bf16
 constexpr int TT_OPER = 4 * TT_KBLK;               // A hi, A lo, B hi, B lo of one K half: 64 KB
@@ -521,31 +538,32 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   const uint32_t tmem = *tslot;
 
   // ---- the tile, 128 rows x 64 K (zero outside the matrix / beyond jb), loaded once with all of
-  //      a thread's loads in flight: real parts feed phase 0, imaginary parts (kept) phase 1
-  float xi[32];
-  int ar, akh;
+  //      a thread's loads in flight: real parts feed phase 0, imaginary parts (kept) phase 1;
+  //      thread (ar, akq) holds K values akq*16 .. akq*16 + 15 of tile row ar
+  float xi[16];
+  int ar, akq;
   {
-    float xr[32];
+    float xr[16];
     if (lower) {
       // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
       ar = t & 127;
-      akh = t >> 7;
+      akq = t >> 7;
       const z32 *src = Am + (size_t)(J + jb + m0 + ar);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        const int k = akh * 32 + i;
+      for (int i = 0; i < 16; ++i) {
+        const int k = akq * 16 + i;
         const z32 v = (ar < nv && k < jb) ? src[(size_t)(J + k) * N] : make_float2(0.f, 0.f);
         xr[i] = v.x;
         xi[i] = v.y;
       }
     } else {
-      // columns J+jb+m0+r, rows J+k: two threads per column, 256 contiguous bytes each
-      ar = t >> 1;
-      akh = t & 1;
+      // columns J+jb+m0+r, rows J+k: four threads per column, 128 contiguous bytes each
+      ar = t >> 2;
+      akq = t & 3;
       const z32 *src = Am + (size_t)(J + jb + m0 + ar) * N + J;
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int k = akh * 32 + 2 * i;            // jb is even: k, k+1 are both in or both out
+      for (int i = 0; i < 8; ++i) {
+        const int k = akq * 16 + 2 * i;            // jb is even: k, k+1 are both in or both out
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ar < nv && k < jb) v = *reinterpret_cast<const float4 *>(src + k);
         xr[2 * i] = v.x;
@@ -555,7 +573,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       }
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) put8(gA, ar, akh * 4 + q, xr + 8 * q, 1.f);
+    for (int q = 0; q < 2; ++q) put8(gA, ar, akq * 2 + q, xr + 8 * q, 1.f);
   }
 
   bool ok = true;
@@ -567,26 +585,23 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       if (!ok) break;
       // ---- A operand of phase 1: the imaginary part of the tile
 #pragma unroll
-      for (int q = 0; q < 4; ++q) put8(gA, ar, akh * 4 + q, xi + 8 * q, 1.f);
+      for (int q = 0; q < 2; ++q) put8(gA, ar, akq * 2 + q, xi + 8 * q, 1.f);
     }
     // ---- B operand: rows n (real part of the output) and 64 + n (imaginary part):
     //      phase 0 [Wr(:, n)], [Wi(:, n)]; phase 1 [-Wi(:, n)], [Wr(:, n)];
     //      mode 0 W(k, n) = U11^-1(k, n), mode 1 W(k, n) = L11^-1(n, k)
     {
-      const int n = t & 63, kq = t >> 6;          // K values kq*16 .. kq*16+15 of column n
-#pragma unroll 1
-      for (int j = 0; j < 2; ++j) {
-        float wr[8], wi[8];
+      const int n = t & 63, kq = t >> 6;          // K values kq*8 .. kq*8+7 of column n
+      float wr[8], wi[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int k = kq * 16 + j * 8 + i;
-          const z32 w = lower ? W[k + n * NB] : W[n + k * NB];
-          wr[i] = w.x;
-          wi[i] = w.y;
-        }
-        put8(gB, n, kq * 2 + j, h ? wi : wr, h ? -1.f : 1.f);
-        put8(gB, 64 + n, kq * 2 + j, h ? wr : wi, 1.f);
+      for (int i = 0; i < 8; ++i) {
+        const int k = kq * 8 + i;
+        const z32 w = lower ? W[k + n * NB] : W[n + k * NB];
+        wr[i] = w.x;
+        wi[i] = w.y;
       }
+      put8(gB, n, kq, h ? wi : wr, h ? -1.f : 1.f);
+      put8(gB, 64 + n, kq, h ? wr : wi, 1.f);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -610,12 +625,12 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   asm volatile("tcgen05.fence::after_thread_sync;");
 
   // ---- epilogue: warp w reads TMEM lanes 32 (w % 4).. (tile rows) and output columns
-  //      32 (w / 4) .. + 31; the results reach global memory through shared memory (the
+  //      16 (w / 4) .. + 15; the results reach global memory through shared memory (the
   //      operand buffers, free once the MMAs completed), so that every store is coalesced
   if (ok) {
-    const int quad = warp & 3, half = warp >> 2;
+    const int quad = warp & 3, grp = warp >> 2;
     const int r = quad * 32 + lane;
-    const int n0 = half * 32;
+    const int n0 = grp * 16;
     unsigned char *stg = gA;
     const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)n0;
     // the thread's 32 output values of part `piece` (16 columns each), re then im
@@ -626,21 +641,20 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
     };
     if (lower) {
       unsigned char *row = stg + r * TT_SROW + n0 * 2;
-#pragma unroll 1
-      for (int piece = 0; piece < 2; ++piece) {
+      {
         float re[16], im[16];
-        tload(piece, re, im);
+        tload(0, re, im);
         // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
         if (r < nv) {
           z32 *dst = Am + (size_t)(J + jb + m0 + r);
 #pragma unroll
           for (int j = 0; j < 16; ++j)
-            if (n0 + 16 * piece + j < jb) dst[(size_t)(J + n0 + 16 * piece + j) * N] = make_float2(re[j], im[j]);
+            if (n0 + j < jb) dst[(size_t)(J + n0 + j) * N] = make_float2(re[j], im[j]);
         }
         // k_split_a's rows [Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-          const int o = 32 * piece + 16 * c;
+          const int o = 16 * c;
           *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 0, false);
           *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 2, false);
           *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 1, false);
@@ -656,11 +670,10 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
 #pragma unroll 1
       for (int rnd = 0; rnd < 3; ++rnd) {
         if (rnd) __syncthreads();
-#pragma unroll 1
-        for (int piece = 0; piece < 2; ++piece) {
+        {
           float re[16], im[16];
-          tload(piece, re, im);
-          const int nn = n0 + 16 * piece;
+          tload(0, re, im);
+          const int nn = n0;
           if (rnd == 0) {
             unsigned char *col = stg + r * TT_FROW + nn * 8;
 #pragma unroll

@@ -267,6 +267,15 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
     }
     for (int p = 0; p < nblk; ++p) {
       const int r0 = geo.blk(p) * QB, jb = min(QB, N - r0);
+      // this lane's right-hand-side values of block p (row r, part c), loaded before the wait for
+      // the accumulator so that their latency overlaps it
+      const int r = q * 16 + (lane >> 1), c = lane & 1;
+      float bv[Q_RMAX];
+#pragma unroll
+      for (int n = 0; n < Q_RMAX; ++n) {
+        bv[n] = 0.f;
+        if (p > 0 && n < R && r < jb) bv[n] = reinterpret_cast<const float *>(Cb + (size_t)(r0 + r) + (size_t)n * ldc)[c];
+      }
       bool w = true;
       if (p > 0) w = mbar_wait(b_crit, (p - 1) & 1, err, 46);
       w = w && mbar_wait(b_dfull, p & 1, err, 47);
@@ -279,19 +288,11 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
         tmem_ld16(ta + 16, *reinterpret_cast<float(*)[16]>(v + 16));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         // lane 2r: [Tr Yr | Tr Yi], lane 2r + 1: [Ti Yr | Ti Yi] of complex row r
-        const int r = q * 16 + (lane >> 1), c = lane & 1;
 #pragma unroll
         for (int n = 0; n < Q_RMAX; ++n) {
           const float pv = __shfl_xor_sync(0xffffffffu, v[16 + n], 1);
           const float upd = c ? v[n] + pv : v[n] - pv;
-          if (n < R) {
-            float val = 0.f;
-            if (r < jb) {
-              const z32 bb = Cb[(size_t)(r0 + r) + (size_t)n * ldc];
-              val = (c ? bb.y : bb.x) - upd;
-            }
-            reinterpret_cast<float *>(vst)[(n * QB + r) * 2 + c] = val;
-          }
+          if (n < R) reinterpret_cast<float *>(vst)[(n * QB + r) * 2 + c] = r < jb ? bv[n] - upd : 0.f;
         }
       } else {
         for (int e = dt_; e < QB * R; e += 128) {
