@@ -537,6 +537,27 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tslot;
 
+  // ---- B operand: rows n (real part of the output) and 64 + n (imaginary part):
+  //      phase 0 [Wr(:, n)], [Wi(:, n)]; phase 1 [-Wi(:, n)], [Wr(:, n)];
+  //      mode 0 W(k, n) = U11^-1(k, n), mode 1 W(k, n) = L11^-1(n, k).  Phase 0's is built
+  //      before the tile is loaded (fewer live registers)
+  auto build_b = [&](int h) {
+    const int n = t & 63, kq = t >> 6;          // K values kq*8 .. kq*8+7 of column n
+    const int ks = lower ? 1 : NB;               // W(k, n) at W[k * ks + n * (NB + 1 - ks)]
+    const z32 *wp = W + kq * 8 * ks + n * (NB + 1 - ks);
+    float wr[8], wi[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const z32 w = wp[i * ks];
+      wr[i] = w.x;
+      wi[i] = w.y;
+    }
+    put8(gB, n, kq, h ? wi : wr, h ? -1.f : 1.f);
+    put8(gB, 64 + n, kq, h ? wr : wi, 1.f);
+  };
+  build_b(0);
+  asm volatile("" ::: "memory");   // the tile's loads start after it (fewer live registers)
+
   // ---- the tile, 128 rows x 64 K (zero outside the matrix / beyond jb), loaded once with all of
   //      a thread's loads in flight: real parts feed phase 0, imaginary parts (kept) phase 1;
   //      thread (ar, akq) holds K values akq*16 .. akq*16 + 15 of tile row ar
@@ -548,11 +569,11 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       // rows J+jb+m0+r, columns J+k: a warp reads 32 consecutive rows of one column
       ar = t & 127;
       akq = t >> 7;
-      const z32 *src = Am + (size_t)(J + jb + m0 + ar);
+      const z32 *src = Am + (size_t)(J + akq * 16) * N + (J + jb + m0 + ar);
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int k = akq * 16 + i;
-        const z32 v = (ar < nv && k < jb) ? src[(size_t)(J + k) * N] : make_float2(0.f, 0.f);
+        const z32 v = (ar < nv && k < jb) ? src[i * N] : make_float2(0.f, 0.f);
         xr[i] = v.x;
         xi[i] = v.y;
       }
@@ -576,39 +597,13 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
     for (int q = 0; q < 2; ++q) put8(gA, ar, akq * 2 + q, xr + 8 * q, 1.f);
   }
 
-  bool ok = true;
-#pragma unroll 1
-  for (int h = 0; h < 2; ++h) {
-    if (h == 1) {
-      // the phase-0 MMAs must have read the operands before they are overwritten
-      ok = __syncthreads_and(mbar_wait(sbar, 0, err, 21));
-      if (!ok) break;
-      // ---- A operand of phase 1: the imaginary part of the tile
-#pragma unroll
-      for (int q = 0; q < 2; ++q) put8(gA, ar, akq * 2 + q, xi + 8 * q, 1.f);
-    }
-    // ---- B operand: rows n (real part of the output) and 64 + n (imaginary part):
-    //      phase 0 [Wr(:, n)], [Wi(:, n)]; phase 1 [-Wi(:, n)], [Wr(:, n)];
-    //      mode 0 W(k, n) = U11^-1(k, n), mode 1 W(k, n) = L11^-1(n, k)
-    {
-      const int n = t & 63, kq = t >> 6;          // K values kq*8 .. kq*8+7 of column n
-      float wr[8], wi[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int k = kq * 8 + i;
-        const z32 w = lower ? W[k + n * NB] : W[n + k * NB];
-        wr[i] = w.x;
-        wi[i] = w.y;
-      }
-      put8(gB, n, kq, h ? wi : wr, h ? -1.f : 1.f);
-      put8(gB, 64 + n, kq, h ? wr : wi, 1.f);
-    }
+  // one MMA phase: (hi, hi), (hi, lo), (lo, hi) over the operands in shared memory
+  auto mma_phase = [&](int h) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (t == 32) {
-      // (hi, hi), (hi, lo), (lo, hi) over this K half
 #pragma unroll
       for (int term = 0; term < 3; ++term)
 #pragma unroll
@@ -619,6 +614,16 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
         }
       mma_commit(sbar);
     }
+  };
+  mma_phase(0);
+  // the phase-0 MMAs must have read the operands before they are overwritten
+  bool ok = __syncthreads_and(mbar_wait(sbar, 0, err, 21));
+  if (ok) {
+    // ---- A operand of phase 1: the imaginary part of the tile; B of phase 1
+#pragma unroll
+    for (int q = 0; q < 2; ++q) put8(gA, ar, akq * 2 + q, xi + 8 * q, 1.f);
+    build_b(1);
+    mma_phase(1);
   }
   // CTA-uniform: the epilogue below has block barriers
   if (ok) ok = __syncthreads_and(mbar_wait(sbar, 1, err, 22));
