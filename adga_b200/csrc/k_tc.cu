@@ -315,18 +315,20 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
   } else if (warp == 2) {
     if (lane == 0) {
       int it = 0;
+      int u = 0;     // uses of the one C buffer so far (halves with columns inside the region)
       for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
         bool ok = true;
         for (int h = 0; h < 2 && ok; ++h) {
-          // use u = 2 it + h of the one C buffer: the epilogue has released use u - 1
-          const int u = 2 * it + h;
+          if (tn * BN + h * P_CH_COLS >= Ncols) break;   // the half lies outside the region
+          // the epilogue has released use u - 1
           if (u > 0) ok = mbar_wait(bar_cempty, (u - 1) & 1, err, 14);
           if (!ok) break;
+          ++u;
           mbar_expect_tx(bar_cfull, P_CH_BYTES);
           // x counts floats: rows crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
           tma_load_3d(scbase, &mapC, bar_cfull, 2 * (crow0 + tm * BM), ccol0 + tn * BN + h * P_CH_COLS, b);
-          if (h == 0)
+          if (h == 0 && tn * BN + P_CH_COLS < Ncols)
             tma_prefetch_l2_3d(&mapC, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
         }
         if (!ok) break;
@@ -336,7 +338,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
     const int e = warp - 4, grp = e >> 2, quad = warp & 3;
     const int row = quad * 32 + lane;
     const z32 *cs = reinterpret_cast<const z32 *>(gc);   // [col][128 rows] of the current half
-    int it = 0;
+    int it = 0, u = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
       const int a = it & 1;
@@ -348,8 +350,10 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
       const bool rowok = m < Mrows;
       z32 *Cb = M + (size_t)b * strideM + (size_t)(crow0 + m);
       for (int h = 0; h < 2 && ok; ++h) {
+        if (tn * BN + h * P_CH_COLS >= Ncols) break;     // no C loaded: outside the region
         // every lane waits (and so observes the TMA-written C half)
-        ok = mbar_wait(bar_cfull, (2 * it + h) & 1, err, 16);
+        ok = mbar_wait(bar_cfull, u & 1, err, 16);
+        ++u;
         if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
         const int c0 = h * P_CH_COLS + grp * 32;            // accumulator column of this warp's part
         const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * TMEM_COLS + c0);
