@@ -497,8 +497,8 @@ constexpr int DN_LD = 65;
 
 // Diagonal block of an unpivoted step with its inverses, one CTA per matrix
 // (FP32): the jb x jb block is padded with the identity to 64 x 64 and
-// factored right-looking with one barrier per column (the column scaling by
-// 1/u_kk is deferred to the end, so no thread writes what another reads);
+// factored right-looking in 4 x 4 register blocks (16 block steps, two
+// barriers each, packed two-lane FMAs in the trailing blocks);
 // L11^-1 (strictly lower; unit diagonal implied) and U11^-1 (upper with the
 // diagonal) then share one array and follow in 16 x 16 blocks: eight warps
 // invert the diagonal blocks of both triangles (lane = column, no barriers),
@@ -532,24 +532,98 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
     D[i + j * DN_LD] = (i < jb && j < jb) ? A[(size_t)(J + i) + (size_t)(J + j) * N] : (i == j ? one : zero);
   }
   __syncthreads();
-  if (t == 0) rcps[0] = crcp(D[0]);
-  __syncthreads();
   {
-    // the thread that finishes pivot k+1 (row k+1, part 0: its first column) forms 1/u for the next column
-    const int i = t & 63, part = t >> 6;
-    for (int k = 0; k < 64; ++k) {
-      const T rcp = rcps[k];
-      if (i > k) {
-        const T l = cmul(D[i + k * DN_LD], rcp);
-        for (int j = k + 1 + part; j < 64; j += 4) D[i + j * DN_LD] = csub(D[i + j * DN_LD], cmul(l, D[k + j * DN_LD]));
-        if (i == k + 1 && part == 0) rcps[k + 1] = crcp(D[i + i * DN_LD]);
+    // Right-looking LU in 4 x 4 blocks held in registers: thread (bi, bj) owns
+    // D[4bi.., 4bj..].  Per block step kb: the diagonal thread factors its block
+    // (unit L, U, the reciprocals of U's diagonal), the column panel solves
+    // L[bi,kb] U_kk = A[bi,kb], the row panel L_kk U[kb,bj] = A[kb,bj], and the
+    // trailing blocks take A -= L[bi,kb] U[kb,bj] as four rank-1 updates; two
+    // barriers per block step.  Panels are exchanged through S (stride 17 per
+    // block, conflict-free for the 16 column owners of a warp).
+    static_assert(sizeof(T) == sizeof(z32), "the blocked LU is the FP32 path's");
+    const int bi = t >> 4, bj = t & 15;
+    T *xL = S, *xU = S + 16 * 17, *xD = S + 2 * 16 * 17;   // xD: the factored diagonal block + 1/u
+    T a[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) a[r][c] = D[(4 * bi + r) + (4 * bj + c) * DN_LD];
+#pragma unroll 1
+    for (int kb = 0; kb < 16; ++kb) {
+      if (bi == kb && bj == kb) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const T rp = crcp(a[k][k]);
+          xD[16 + k] = rp;
+          rcps[4 * kb + k] = rp;
+#pragma unroll
+          for (int i = k + 1; i < 4; ++i) a[i][k] = cmul(a[i][k], rp);
+#pragma unroll
+          for (int i = k + 1; i < 4; ++i)
+#pragma unroll
+            for (int j = k + 1; j < 4; ++j) a[i][j] = csub(a[i][j], cmul(a[i][k], a[k][j]));
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) xD[r + 4 * c] = a[r][c];
       }
       __syncthreads();
+      if (bj == kb && bi > kb) {
+        // L[bi,kb] = A[bi,kb] U_kk^-1, column by column
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            T v = a[r][c];
+#pragma unroll
+            for (int c2 = 0; c2 < c; ++c2) v = csub(v, cmul(a[r][c2], xD[c2 + 4 * c]));
+            a[r][c] = cmul(v, xD[16 + c]);
+          }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) xL[bi * 17 + r + 4 * c] = a[r][c];
+      } else if (bi == kb && bj > kb) {
+        // U[kb,bj] = L_kk^-1 A[kb,bj] (unit diagonal), row by row
+#pragma unroll
+        for (int r = 1; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int r2 = 0; r2 < r; ++r2) a[r][c] = csub(a[r][c], cmul(xD[r + 4 * r2], a[r2][c]));
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) xU[bj * 17 + r + 4 * c] = a[r][c];
+      }
+      __syncthreads();
+      if (bi > kb && bj > kb) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          T l[4], u[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) l[r] = xL[bi * 17 + r + 4 * k];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) u[c] = xU[bj * 17 + k + 4 * c];
+          // a[r][c] -= l[r] u[c] as two packed FMAs per complex entry
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const float2 us = make_float2(u[c].y, u[c].x);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              a[r][c] = __ffma2_rn(make_float2(-l[r].x, -l[r].x), u[c], a[r][c]);
+              a[r][c] = __ffma2_rn(make_float2(l[r].y, -l[r].y), us, a[r][c]);
+            }
+          }
+        }
+      }
     }
-  }
-  for (int e = t; e < 64 * 64; e += 256) {
-    const int i = e & 63, k = e >> 6;
-    if (i > k) D[i + k * DN_LD] = cmul(D[i + k * DN_LD], rcps[k]);
+    // the packed factors (multipliers below the diagonal, U on and above it) back into D
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) D[(4 * bi + r) + (4 * bj + c) * DN_LD] = a[r][c];
   }
   __syncthreads();
   {
