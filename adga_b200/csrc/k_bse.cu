@@ -308,28 +308,47 @@ k_post(DevCtx c, const z64 *__restrict__ X, size_t sp, size_t sc, int ldX, const
   __syncthreads();
   const z64 *c0 = chi0q + (size_t)p * nd2 * nd2 * 2 * iwf;
   const double b2 = c.beta * c.beta;
-  // 2. chi sums, one thread per (i1, i2, channel)
-  for (int t = threadIdx.x; t < 2 * nd2 * nd2; t += blockDim.x) {
-    int ch = t / (nd2 * nd2), e = t % (nd2 * nd2);
-    int i1 = e % nd2, i2 = e / nd2;
-    const z64 *g = ch ? gam_m : gam_d;
-    const z64 *et = ch ? em : ed;
-    z64 s1 = make_double2(0.0, 0.0), s2 = make_double2(0.0, 0.0);
-    for (int dum = 0; dum < 2 * iwf; ++dum) {
-      const z64 *cq = c0 + (size_t)dum * nd2 * nd2 + (size_t)i2 * nd2;
-      for (int i3 = 0; i3 < nd2; ++i3) {
-        size_t col = (size_t)(i3 + dum * nd2) * nd2;
-        z64 q = cq[i3];
-        z64 nl = q;
-        if (i3 == i2) nl = csub(q, c0w[dum * nd2 + i2]);
-        cfma(s1, g[i1 + col], nl);
-        cfma(s2, et[i1 + col], q);
+  // 2. chi sums: eight lanes per (i1, i2, channel), lane l of the group summing the
+  //    frequencies dum = l mod 8, then a shuffle reduction (every lane of a warp
+  //    runs the same rounds)
+  {
+    const int l8 = threadIdx.x & 7, grp = threadIdx.x >> 3, ngrp = blockDim.x >> 3;
+    const int total = 2 * nd2 * nd2;
+    for (int base = 0; base < total; base += ngrp) {
+      const int t = base + grp;
+      z64 s1 = make_double2(0.0, 0.0), s2 = make_double2(0.0, 0.0);
+      int ch = 0, e = 0;
+      if (t < total) {
+        ch = t / (nd2 * nd2);
+        e = t % (nd2 * nd2);
+        const int i1 = e % nd2, i2 = e / nd2;
+        const z64 *g = ch ? gam_m : gam_d;
+        const z64 *et = ch ? em : ed;
+        for (int dum = l8; dum < 2 * iwf; dum += 8) {
+          const z64 *cq = c0 + (size_t)dum * nd2 * nd2 + (size_t)i2 * nd2;
+          for (int i3 = 0; i3 < nd2; ++i3) {
+            const size_t col = (size_t)(i3 + dum * nd2) * nd2;
+            const z64 q = cq[i3];
+            z64 nl = q;
+            if (i3 == i2) nl = csub(q, c0w[dum * nd2 + i2]);
+            cfma(s1, g[i1 + col], nl);
+            cfma(s2, et[i1 + col], q);
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) {
+        s1.x += __shfl_xor_sync(0xffffffffu, s1.x, o);
+        s1.y += __shfl_xor_sync(0xffffffffu, s1.y, o);
+        s2.x += __shfl_xor_sync(0xffffffffu, s2.x, o);
+        s2.y += __shfl_xor_sync(0xffffffffu, s2.y, o);
+      }
+      if (t < total && l8 == 0) {
+        z64 *out = (ch ? chi_qw_m : chi_qw_d) + (size_t)p * nd2 * nd2 + e;
+        z64 v = make_double2(s1.x / b2, s1.y / b2);
+        *out = cadd(v, make_double2(s2.x / b2, s2.y / b2));
       }
     }
-    z64 *out = (ch ? chi_qw_m : chi_qw_d) + (size_t)p * nd2 * nd2 + e;
-    z64 v = make_double2(s1.x / b2, s1.y / b2);
-    v = cadd(v, make_double2(s2.x / b2, s2.y / b2));
-    *out = v;
   }
   // 3. m_tot for the nu >= 0 half of the columns
   if (mtot) {
