@@ -5,17 +5,19 @@
 //     L U ~= L_hi U_hi + L_hi U_lo + L_lo U_hi .
 // Complex arithmetic is embedded as
 //     [Re C | Im C] = [Lr | Li] . [[Ur, Ui], [-Ui, Ur]]
-// so one MMA with N = 2*BN produces the real (columns 0..BN) and imaginary
+// so two MMAs of N = BN produce the real (columns 0..BN) and imaginary
 // (BN..2BN) parts of BN complex columns.  Operands are staged per step in
 // K-major BF16, four segments of NB each (K4 = 4*NB per step):
 //     A[m]     = [Lr_hi, Li_hi, Lr_lo, Li_lo]
 //     Bre[n]   = [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo]
-//     Bim[n]   = [Ui_hi,  Ur_hi, Ui_lo,  Ur_lo]
 // and the GEMMs run six segment pairs per step (A, B) = (0,0), (1,1), (0,2),
 // (1,3), (2,0), (3,1): the hi*hi, hi*lo and lo*hi products of the real and
-// imaginary parts (K = 6*NB of MMAs from 4*NB of staging).
-// 128B swizzle into a ring of shared-memory stages, tcgen05.mma M=128,
-// N=256, K=16 issued by one thread, FP32 accumulators in TMEM):
+// imaginary parts (K = 6*NB of MMAs from 4*NB of staging).  The rows of
+// [Ui, Ur], Bim[n] = [Ui_hi, Ur_hi, Ui_lo, Ur_lo], are segment s ^ 1 of
+// Bre[n], negated for even s: the imaginary-part MMA reads them from the
+// real-part staging with the instruction's B negation, so only Bre is staged.
+// (TMA loads, 128B swizzle, into a ring of shared-memory stages; tcgen05.mma
+// M=128, N=128, K=16 issued by one thread, FP32 accumulators in TMEM):
 //   k_tc_persist  (used when the C strides are 16-byte multiples) one CTA per
 //                 SM loops over the tiles; C tiles arrive in shared memory by
 //                 TMA during the MMAs and the accumulator is double-buffered,
@@ -49,6 +51,11 @@ __device__ __forceinline__ int seg_b(int j) { return j < 4 ? j : j - 4; }
 // x coordinate (bf16) in the four-segment staging of k-block kb of a step (nbk = NB / BK)
 __device__ __forceinline__ int kx_a(int kb, int nbk) { return (seg_a(kb / nbk) * nbk + kb % nbk) * BK; }
 __device__ __forceinline__ int kx_b(int kb, int nbk) { return (seg_b(kb / nbk) * nbk + kb % nbk) * BK; }
+// B's imaginary-part rows [Ui_hi, Ur_hi, Ui_lo, Ur_lo] are not staged: segment s of such a row is
+// segment s ^ 1 of the real-part row [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo], negated for even s; the
+// k-block's x coordinate in the real-part staging, and whether its MMA negates B
+__device__ __forceinline__ int kx_bi(int kb, int nbk) { return ((seg_b(kb / nbk) ^ 1) * nbk + kb % nbk) * BK; }
+__device__ __forceinline__ uint32_t neg_bi(int kb, int nbk) { return (seg_b(kb / nbk) & 1) ? 0u : 1u; }
 // K-major, 128 B swizzle: LBO = 16 B (unused), SBO = 1024 B between 8-row groups
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   uint64_t d = 0;
@@ -59,16 +66,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
   return d;
 }
-// kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 256
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(2 * BN / 8) << 17) |
-                           ((uint32_t)(BM / 16) << 24);
+// kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128 (bit 14: negate B)
+constexpr uint32_t IDESC_H = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN / 8) << 17) |
+                             ((uint32_t)(BM / 16) << 24);
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma_bf16_h(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-      "l"(a), "l"(b), "r"(IDESC), "r"(acc));
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+// one K = 16 slice of a k-block into [Re C | Im C]: the real-part columns from B's first 128
+// rows, the imaginary-part columns from the second 128 (B negated when neg)
+__device__ __forceinline__ void mma_cplx(uint32_t tmem, uint32_t sa, uint32_t sb, uint32_t neg, uint32_t acc) {
+  mma_bf16_h(tmem, smem_desc(sa), smem_desc(sb), IDESC_H, acc);
+  mma_bf16_h(tmem + BN, smem_desc(sa), smem_desc(sb + B_BYTES / 2), IDESC_H | (neg << 14), acc);
 }
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(192, 2)
@@ -114,7 +127,7 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         mbar_expect_tx(bar_full + 8 * s, STAGE_BYTES);
         tma_load_3d(sa, &mapA, bar_full + 8 * s, kx_a(kb, nbk), m0, b);
         tma_load_3d(sb, &mapB, bar_full + 8 * s, kx_b(kb, nbk), n0, b);
-        tma_load_3d(sb + B_BYTES / 2, &mapB, bar_full + 8 * s, kx_b(kb, nbk), Ncap + n0, b);
+        tma_load_3d(sb + B_BYTES / 2, &mapB, bar_full + 8 * s, kx_bi(kb, nbk), n0, b);
       }
     }
   } else if (warp == 1) {
@@ -125,9 +138,9 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
+        const uint32_t neg = neg_bi(kb, nbk);
 #pragma unroll
-        for (int k = 0; k < BK / 16; ++k)
-          mma_bf16(tmem, smem_desc(sa + 32 * k), smem_desc(sb + 32 * k), (kb > 0 || k > 0) ? 1u : 0u);
+        for (int k = 0; k < BK / 16; ++k) mma_cplx(tmem, sa + 32 * k, sb + 32 * k, neg, (kb > 0 || k > 0) ? 1u : 0u);
         mma_commit(bar_empty + 8 * s);
       }
       mma_commit(bar_acc);
@@ -283,7 +296,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           const int xa = kx_a(kl, nbk), xb = kx_b(kl, nbk);
           tma_load_3d(sa, ma, bar_full + 8 * s, xa, ar + tm * BM, b);
           tma_load_3d(sb, mb, bar_full + 8 * s, xb, bc + tn * BN, b);
-          tma_load_3d(sb + B_BYTES / 2, mb, bar_full + 8 * s, xb, Ncap + bc + tn * BN, b);
+          tma_load_3d(sb + B_BYTES / 2, mb, bar_full + 8 * s, kx_bi(kl, nbk), bc + tn * BN, b);
         }
         if (!ok) break;
       }
@@ -303,9 +316,10 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           if (!(ok = mbar_wait(bar_full + 8 * s, (kbt / P_STAGES) & 1, err, 13))) break;
           asm volatile("tcgen05.fence::after_thread_sync;");
           const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
+          const uint32_t neg = neg_bi(kb >= nkb1 ? kb - nkb1 : kb, nbk);
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k)
-            mma_bf16(dacc, smem_desc(sa + 32 * k), smem_desc(sb + 32 * k), (kb > 0 || k > 0) ? 1u : 0u);
+            mma_cplx(dacc, sa + 32 * k, sb + 32 * k, neg, (kb > 0 || k > 0) ? 1u : 0u);
           mma_commit(bar_empty + 8 * s);
         }
         if (!ok) break;
@@ -674,10 +688,9 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
       copy_rows(stg, Astage + ((size_t)b * N + m0) * 4 * NB, nv, t);
     } else {
       const int pc = jb / 2;                       // 16-byte pieces of a U12 column (jb is even)
-      // round 0: the tile's U12 columns; 1, 2: k_split_b's real rows [Ur_hi, -Ui_hi, Ur_lo,
-      // -Ui_lo] and imaginary rows [Ui_hi, Ur_hi, Ui_lo, Ur_lo]
+      // round 0: the tile's U12 columns; 1: k_split_b's real-part rows [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo]
 #pragma unroll 1
-      for (int rnd = 0; rnd < 3; ++rnd) {
+      for (int rnd = 0; rnd < 2; ++rnd) {
         if (rnd) __syncthreads();
         {
           float re[16], im[16];
@@ -694,17 +707,10 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
             for (int c = 0; c < 2; ++c) {
               const float *xr = re + 8 * c, *xi = im + 8 * c;
               const int o = 16 * c;
-              if (rnd == 1) {
-                *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 0, false);
-                *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 2, true);
-                *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 1, false);
-                *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 3, true);
-              } else {
-                *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 2, false);
-                *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 0, false);
-                *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 3, false);
-                *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 1, false);
-              }
+              *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 0, false);
+              *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 2, true);
+              *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 1, false);
+              *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 3, true);
             }
           }
         }
@@ -716,7 +722,7 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
                 *reinterpret_cast<const float4 *>(stg + cc * TT_FROW + pp * 16);
           }
         } else {
-          copy_rows(stg, Bstage + ((size_t)b * 2 * Ncap + (rnd == 2 ? (size_t)Ncap : 0) + m0) * 4 * NB, nv, t);
+          copy_rows(stg, Bstage + ((size_t)b * Ncap + m0) * 4 * NB, nv, t);
         }
       }
     }
@@ -762,8 +768,9 @@ k_split_a(const z32 *M, size_t strideM, int N, int J, int jb, int Mrows, int NB,
   }
 }
 
-// B[b][n][4*NB] (real-part rows) and B[b][Ncap + n][4*NB] (imaginary-part rows)
-// for U rows J..J+jb-1 and columns n = 0..Ncols-1 (matrix columns J+jb+n)
+// B[b][n][4*NB]: the real-part rows [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo] for U rows J..J+jb-1
+// and columns n = 0..Ncols-1 (matrix columns J+jb+n); the GEMMs read the imaginary-part
+// rows from them (kx_bi, neg_bi)
 __global__ void __launch_bounds__(256)
 k_split_b(const z32 *M, size_t strideM, int N, int J, int jb, int Ncols, int Ncap, int NB,
           __nv_bfloat16 *B, int b0) {
@@ -776,11 +783,8 @@ k_split_b(const z32 *M, size_t strideM, int N, int J, int jb, int Ncols, int Nca
   __nv_bfloat16 rh, rl, ih, il;
   split2(v.x, rh, rl);
   split2(v.y, ih, il);
-  const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
-  __nv_bfloat16 *re = B + ((size_t)b * 2 * Ncap + n) * 4 * NB + k;
-  __nv_bfloat16 *im = B + ((size_t)b * 2 * Ncap + Ncap + n) * 4 * NB + k;
-  re[0 * NB] = rh; re[1 * NB] = nih; re[2 * NB] = rl; re[3 * NB] = nil;
-  im[0 * NB] = ih; im[1 * NB] = rh;  im[2 * NB] = il; im[3 * NB] = rl;
+  __nv_bfloat16 *re = B + ((size_t)b * Ncap + n) * 4 * NB + k;
+  re[0 * NB] = rh; re[1 * NB] = __hneg(ih); re[2 * NB] = rl; re[3 * NB] = __hneg(il);
 }
 
 // ---------------------------------------------------------------------------
@@ -843,16 +847,16 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   c->Ncap = lb.ncols;
   const size_t K4 = 4 * (size_t)lb.NB;       // four staging segments per step
   cudaError_t e = cudaMalloc(&c->A, sizeof(__nv_bfloat16) * K4 * lb.N * lb.batch);
-  if (e == cudaSuccess) e = cudaMalloc(&c->B, sizeof(__nv_bfloat16) * K4 * 2 * c->Ncap * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->B, sizeof(__nv_bfloat16) * K4 * c->Ncap * lb.batch);
   // second staging for the unpivoted path's delayed two-step updates
   if (e == cudaSuccess) e = cudaMalloc(&c->A2, sizeof(__nv_bfloat16) * K4 * lb.N * lb.batch);
-  if (e == cudaSuccess) e = cudaMalloc(&c->B2, sizeof(__nv_bfloat16) * K4 * 2 * c->Ncap * lb.batch);
+  if (e == cudaSuccess) e = cudaMalloc(&c->B2, sizeof(__nv_bfloat16) * K4 * c->Ncap * lb.batch);
   if (e == cudaSuccess) e = cudaMalloc(&c->err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemsetAsync(c->err, 0, sizeof(int), st);
   if (e == cudaSuccess && (!make_map(&c->mapA, c->A, K4, lb.N, lb.batch) ||
-                           !make_map(&c->mapB, c->B, K4, 2 * (uint64_t)c->Ncap, lb.batch) ||
+                           !make_map(&c->mapB, c->B, K4, (uint64_t)c->Ncap, lb.batch) ||
                            !make_map(&c->mapA2, c->A2, K4, lb.N, lb.batch) ||
-                           !make_map(&c->mapB2, c->B2, K4, 2 * (uint64_t)c->Ncap, lb.batch)))
+                           !make_map(&c->mapB2, c->B2, K4, (uint64_t)c->Ncap, lb.batch)))
     e = cudaErrorInvalidValue;
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
