@@ -79,10 +79,13 @@ __device__ __forceinline__ void mma_bf16_h(uint32_t tmem, uint64_t a, uint64_t b
 }
 // one K = 16 slice of a k-block into [Re C | Im C]: the real-part columns from B's first 128
 // rows, the imaginary-part columns from the second 128 (B negated when neg)
-__device__ __forceinline__ void mma_cplx(uint32_t tmem, uint32_t sa, uint32_t sb, uint32_t neg, uint32_t acc) {
-  mma_bf16_h(tmem, smem_desc(sa), smem_desc(sb), IDESC_H, acc);
-  mma_bf16_h(tmem + BN, smem_desc(sa), smem_desc(sb + B_BYTES / 2), IDESC_H | (neg << 14), acc);
+__device__ __forceinline__ void mma_cplx(uint32_t tmem, uint32_t sa, uint32_t sb, uint32_t neg, uint32_t acc,
+                                         uint32_t idesc = IDESC_H) {
+  mma_bf16_h(tmem, smem_desc(sa), smem_desc(sb), idesc, acc);
+  mma_bf16_h(tmem + BN, smem_desc(sa), smem_desc(sb + B_BYTES / 2), idesc | (neg << 14), acc);
 }
+// the same with N = 64: a tile with at most 64 columns inside the region (the narrow strips)
+constexpr uint32_t IDESC_Q = (IDESC_H & ~(0x3Fu << 17)) | ((uint32_t)(64 / 8) << 17);
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(192, 2)
 k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
@@ -317,9 +320,10 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           asm volatile("tcgen05.fence::after_thread_sync;");
           const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
           const uint32_t neg = neg_bi(kb >= nkb1 ? kb - nkb1 : kb, nbk);
+          const uint32_t idesc = Ncols - (tile % ntn) * BN <= 64 ? IDESC_Q : IDESC_H;
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k)
-            mma_cplx(dacc, sa + 32 * k, sb + 32 * k, neg, (kb > 0 || k > 0) ? 1u : 0u);
+            mma_cplx(dacc, sa + 32 * k, sb + 32 * k, neg, (kb > 0 || k > 0) ? 1u : 0u, idesc);
           mma_commit(bar_empty + 8 * s);
         }
         if (!ok) break;
