@@ -500,11 +500,10 @@ constexpr int DN_LD = 65;
 // factored right-looking in 4 x 4 register blocks (16 block steps, two
 // barriers each, packed two-lane FMAs in the trailing blocks);
 // L11^-1 (strictly lower; unit diagonal implied) and U11^-1 (upper with the
-// diagonal) then share one array: the 4 x 4 diagonal blocks' inverses from
-// their owners' registers, then four doubling levels (4 -> 8 -> 16 -> 32 -> 64)
-// whose off-diagonal quadrants are 4 x 4 block products with the triangles'
-// zero blocks skipped, three barriers per level.  73 KB of shared memory:
-// three CTAs per SM.
+// diagonal) then share one array and follow in 16 x 16 blocks: eight warps
+// invert the diagonal blocks of both triangles (lane = column, no barriers),
+// and three block rounds fill L^-1 downwards and U^-1 upwards, each a pair of
+// small block products per triangle.  73 KB of shared memory: three CTAs per SM.
 constexpr int DI_SCR = 3 * 256;
 
 __device__ __forceinline__ void cfma2(z32 &acc, z32 a, z32 u) {
@@ -625,115 +624,80 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int c = 0; c < 4; ++c) D[(4 * bi + r) + (4 * bj + c) * DN_LD] = a[r][c];
-    // ---- inverses, in X: L^-1 strictly below the diagonal (unit diagonal implied), U^-1 on
-    //      and above it.  The sixteen 4 x 4 diagonal blocks first (their owners, from
-    //      registers), then four doubling levels: the 2s x 2s diagonal blocks' off-diagonal
-    //      quadrants from the s x s inverses, Q = -A^-1 (C B^-1) for U and -B^-1 (C A^-1)
-    //      for L, as 4 x 4 block products with the triangular factors' zero blocks skipped
-    if (bi == bj) {
-      T xl[4][4], xu[4][4];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) xl[r][c] = r == c ? one : zero;
-#pragma unroll
-        for (int r = c + 1; r < 4; ++r) {
-          T v = zero;
-#pragma unroll
-          for (int k = c; k < r; ++k) cfma(v, a[r][k], xl[k][c]);
-          xl[r][c] = cneg(v);
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) xu[r][c] = zero;
-        xu[c][c] = rcps[4 * bi + c];
-#pragma unroll
-        for (int r = c - 1; r >= 0; --r) {
-          T v = zero;
-#pragma unroll
-          for (int k = r + 1; k <= c; ++k) cfma(v, a[r][k], xu[k][c]);
-          xu[r][c] = cneg(cmul(v, rcps[4 * bi + r]));
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) X[(4 * bi + r) + (4 * bi + c) * DN_LD] = r > c ? xl[r][c] : xu[r][c];
-    }
   }
   __syncthreads();
   {
-    const int bi = t >> 4, bj = t & 15;
-    // 4 x 4 block of X; a diagonal block masked to L^-1 (lower: unit diagonal) or U^-1 (upper)
-    auto xblk = [&](int r0, int c0, int r, int c, int mask) -> T {
-      if (mask == 1) { if (r < c) return zero; if (r == c) return one; }
-      if (mask == 2 && r > c) return zero;
-      return X[(4 * r0 + r) + (4 * c0 + c) * DN_LD];
-    };
-    // acc += P Q for 4 x 4 blocks given element getters, streamed over k
-    auto bmm = [&](T (&acc)[4][4], auto pget, auto qget) {
+    const int w = t >> 5, lane = t & 31;
+    if (lane < 16) {
+      const int o = 16 * (w & 3), l = lane;
+      T x[16];
+      const T xd = w < 4 ? one : rcps[o + l];    // diagonal entry of the inverse's column l
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        T pl[4], qr[4];
+      for (int r = 0; r < 16; ++r) x[r] = r == l ? xd : zero;
+      if (w < 4) {                                // unit lower: column l of the block inverse, below l
 #pragma unroll
-        for (int r = 0; r < 4; ++r) pl[r] = pget(r, k);
+        for (int r = 1; r < 16; ++r) {
+          if (r > l) {
+            T s = zero;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) qr[c] = qget(k, c);
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-          for (int r = 0; r < 4; ++r) cfma2(acc[r][c], pl[r], qr[c]);
-      }
-    };
-#pragma unroll 1
-    for (int m = 0; m < 4; ++m) {
-      const int hs = 1 << m, gs = 2 * hs, g0 = (bi / gs) * gs;
-      const bool same = bi / gs == bj / gs;
-      const bool upq = same && bi % gs < hs && bj % gs >= hs;     // U^-1's upper-right quadrant
-      const bool loq = same && bi % gs >= hs && bj % gs < hs;     // L^-1's lower-left quadrant
-      T acc[4][4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = zero;
-      // step 1: T = C B^-1 (U: C = U(bi, k), k in B's rows up to bj) or C A^-1 (L: C = L(bi, k), k >= bj)
-      if (upq || loq) {
-        const int k0 = upq ? g0 + hs : bj, k1 = upq ? bj : g0 + hs - 1;
-        for (int k = k0; k <= k1; ++k) {
-          const int mk = k == bj ? (upq ? 2 : 1) : 0;
-          bmm(acc, [&](int r, int c) { return D[(4 * bi + r) + (4 * k + c) * DN_LD]; },
-              [&](int r, int c) { return xblk(k, bj, r, c, mk); });
+            for (int kk = 0; kk < r; ++kk)
+              if (kk >= l) cfma(s, D[(o + r) + (o + kk) * DN_LD], x[kk]);
+            x[r] = cneg(s);
+          }
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < 16; ++r)
+          if (r > l) X[(o + r) + (o + l) * DN_LD] = x[r];
+      } else {                                    // upper: column l, on and above the diagonal
 #pragma unroll
-          for (int c = 0; c < 4; ++c) X[(4 * bi + r) + (4 * bj + c) * DN_LD] = acc[r][c];
-      }
-      __syncthreads();
-      // step 2: Q = -A^-1 T (U: k from bi through A's rows) or -B^-1 T (L: k from B's first row to bi)
-      if (upq || loq) {
+        for (int r = 14; r >= 0; --r) {
+          if (r < l) {
+            T s = zero;
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) acc[r][c] = zero;
-        const int k0 = upq ? bi : g0 + hs, k1 = upq ? g0 + hs - 1 : bi;
-        for (int k = k0; k <= k1; ++k) {
-          const int mk = k == bi ? (upq ? 2 : 1) : 0;
-          bmm(acc, [&](int r, int c) { return xblk(bi, k, r, c, mk); },
-              [&](int r, int c) { return X[(4 * k + r) + (4 * bj + c) * DN_LD]; });
+            for (int kk = r + 1; kk < 16; ++kk)
+              if (kk <= l) cfma(s, D[(o + r) + (o + kk) * DN_LD], x[kk]);
+            x[r] = cneg(cmul(rcps[o + r], s));
+          }
         }
-      }
-      __syncthreads();
-      if (upq || loq) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) X[(4 * bi + r) + (4 * bj + c) * DN_LD] = cneg(acc[r][c]);
+        for (int r = 0; r < 16; ++r)
+          if (r <= l) X[(o + r) + (o + l) * DN_LD] = x[r];
       }
-      __syncthreads();
     }
+  }
+  __syncthreads();
+  for (int st = 1; st < 4; ++st) {
+    const int bl = st, bu = 3 - st;               // block row of L^-1 / U^-1 filled in this round
+    // L: S_bj = sum_{bk=bj}^{bl-1} L(bl,bk) L^-1(bk,bj), then L^-1(bl,bj) = -L^-1(bl,bl) S_bj
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = e >> 8, r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      for (int m = 16 * bj; m < 16 * bl; ++m) cfma(s, D[(16 * bl + r) + m * DN_LD], lval(m, 16 * bj + c));
+      S[bj * 256 + r + 16 * c] = s;
+    }
+    __syncthreads();
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = e >> 8, r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      for (int m = 0; m < 16; ++m) cfma(s, lval(16 * bl + r, 16 * bl + m), S[bj * 256 + m + 16 * c]);
+      X[(16 * bl + r) + (16 * bj + c) * DN_LD] = cneg(s);
+    }
+    __syncthreads();
+    // U: S_bj = sum_{bk=bu+1}^{bj} U(bu,bk) U^-1(bk,bj), then U^-1(bu,bj) = -U^-1(bu,bu) S_bj
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = bu + 1 + (e >> 8), r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      for (int m = 16 * (bu + 1); m < 16 * (bj + 1); ++m) cfma(s, D[(16 * bu + r) + m * DN_LD], uval(m, 16 * bj + c));
+      S[(e >> 8) * 256 + r + 16 * c] = s;
+    }
+    __syncthreads();
+    for (int e = t; e < 256 * st; e += 256) {
+      const int bj = bu + 1 + (e >> 8), r = e & 15, c = (e >> 4) & 15;
+      T s = zero;
+      for (int m = 0; m < 16; ++m) cfma(s, uval(16 * bu + r, 16 * bu + m), S[(e >> 8) * 256 + m + 16 * c]);
+      X[(16 * bu + r) + (16 * bj + c) * DN_LD] = cneg(s);
+    }
+    __syncthreads();
   }
   const size_t off = ((size_t)b * nsteps + J / NB) * NB * NB;
   for (int e = t; e < NB * NB; e += 256) {
