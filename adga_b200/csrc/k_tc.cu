@@ -227,6 +227,12 @@ constexpr int P_TMEM_COLS = 2 * TMEM_COLS;            // two accumulators
 constexpr int P_THREADS = 384;
 constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + P_CH_BYTES + 1024 + 256;
 
+__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                   (unsigned long long)map),
+               "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
 
 
 __global__ void __launch_bounds__(P_THREADS, 1)
@@ -277,21 +283,8 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
   if (warp == 0) {
     if (lane == 0) {
       int kbt = 0;
-      // a tile's staged operand rows (A: 128 rows, B: 128 real-part rows; four 64-wide segments
-      // of each staging it reads) into L2
-      auto prefetch_tile = [&](int tile) {
-        const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
-        for (int st = 0; st < (nkb > nkb1 ? 2 : 1); ++st)
-          for (int sg = 0; sg < 4 * nbk; ++sg) {
-            tma_prefetch_l2_3d(st ? &mapA2 : &mapA, sg * BK, (st ? arow2 : arow0) + tm * BM, b);
-            tma_prefetch_l2_3d(st ? &mapB2 : &mapB, sg * BK, (st ? bcol2 : bcol0) + tn * BN, b);
-          }
-      };
-      if (blockIdx.x < ntiles) prefetch_tile(blockIdx.x);
       for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
-        // the next tile's operands into L2 while this one's k-blocks stream
-        if (tile + (int)gridDim.x < ntiles) prefetch_tile(tile + gridDim.x);
         bool ok = true;
         for (int kb = 0; kb < nkb; ++kb, ++kbt) {
           const int s = kbt % P_STAGES;
@@ -343,13 +336,6 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
       int u = 0;     // uses of the one C buffer so far (halves with columns inside the region)
       for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
-        // this CTA's next tile's C into L2 now, a whole tile ahead of its loads
-        const int nx = tile + gridDim.x;
-        if (nx < ntiles) {
-          const int tn2 = nx % ntn, tm2 = (nx / ntn) % ntm, b2 = b0 + nx / (ntn * ntm);
-          for (int h = 0; h < 2 && tn2 * BN + h * P_CH_COLS < Ncols; ++h)
-            tma_prefetch_l2_3d(&mapC, 2 * (crow0 + tm2 * BM), ccol0 + tn2 * BN + h * P_CH_COLS, b2);
-        }
         bool ok = true;
         for (int h = 0; h < 2 && ok; ++h) {
           if (tn * BN + h * P_CH_COLS >= Ncols) break;   // the half lies outside the region
@@ -360,7 +346,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           mbar_expect_tx(bar_cfull, P_CH_BYTES);
           // x counts floats: rows crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
           tma_load_3d(scbase, &mapC, bar_cfull, 2 * (crow0 + tm * BM), ccol0 + tn * BN + h * P_CH_COLS, b);
-          if (it == 0 && h == 0 && tn * BN + P_CH_COLS < Ncols)   // later tiles were prefetched a tile ahead
+          if (h == 0 && tn * BN + P_CH_COLS < Ncols)
             tma_prefetch_l2_3d(&mapC, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
         }
         if (!ok) break;
@@ -541,31 +527,7 @@ __device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat1
 __global__ void __launch_bounds__(TT_THREADS, 2)
 k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
          const z32 *Uinv, __nv_bfloat16 *Astage, __nv_bfloat16 *Bstage, int Ncap, int b0, int ntA, int ntU,
-         int ahead, int nblocks, int *err) {
-  // the tile of the CTA `ahead` blocks later (the next wave) into L2: one 16-byte-aligned
-  // contiguous piece per column (mode 0: 128 rows of one of the 64 columns, mode 1: the 64
-  // rows of one of the 128 columns), clipped to the matrix
-  if (threadIdx.x < 128 && blockIdx.x + ahead < nblocks) {
-    const int nb = blockIdx.x + ahead, per2 = ntA + ntU;
-    const int b2 = b0 + nb / per2, tile2 = nb % per2;
-    const bool lo2 = tile2 < ntA;
-    const int mm = (lo2 ? tile2 : tile2 - ntA) * TT_ROWS;
-    const int nr2 = min(TT_ROWS, (lo2 ? N : ncols) - J - jb - mm);
-    const z32 *base = M + (size_t)b2 * strideM;
-    const int c = threadIdx.x;
-    const z32 *src = nullptr;
-    int bytes = 0;
-    if (lo2 && c < jb) {
-      src = base + (size_t)(J + c) * N + (J + jb + mm);
-      bytes = nr2 * 8;
-    } else if (!lo2 && c < nr2) {
-      src = base + (size_t)(J + jb + mm + c) * N + J;
-      bytes = jb * 8;
-    }
-    bytes &= ~15;
-    if (bytes > 0)
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-  }
+         int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gA = smraw + (sbase - smem_u32(smraw));    // A hi, A lo, B hi, B lo
@@ -1015,7 +977,7 @@ cudaError_t tc_tri_step(void *ctxp, int first, int count, int J, int jb, int set
   if (e != cudaSuccess) return e;
   k_tc_tri<<<(unsigned)((ntA + ntU) * count), TT_THREADS, TT_SMEM_BYTES, st>>>(
       c->M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, lb.nsteps(), (const z32 *)lb.Linv, (const z32 *)lb.Uinv,
-      set ? c->A2 : c->A, set ? c->B2 : c->B, c->Ncap, first, ntA, ntU, 2 * c->nsm, (ntA + ntU) * count, c->err);
+      set ? c->A2 : c->A, set ? c->B2 : c->B, c->Ncap, first, ntA, ntU, c->err);
   return ADGA_LAUNCH_CHECK();
 }
 

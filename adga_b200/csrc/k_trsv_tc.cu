@@ -47,7 +47,6 @@ using namespace umma;
 constexpr int QB = 64;                        // block width (the factorisation's NB)
 constexpr int Q_THREADS = 384;
 constexpr int Q_NS = 6;                       // ring stages
-constexpr int Q_PF = 16;                      // stages prefetched into L2 ahead of the ring
 constexpr int Q_KC = 32;                      // panel columns per stage
 constexpr int Q_STAGE = 128 * Q_KC * 4;       // 128 reals (64 complex rows) x 32 columns FP32 (16 KB)
 constexpr int Q_NP = 32;                      // MMA N: 16 real-part + 16 imaginary-part rows of B
@@ -183,18 +182,6 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
   if (warp == 0) {
     // ---- TMA producer: the stages of every panel in solve order
     if (lane == 0) {
-      // a second cursor over the same stage sequence runs Q_PF stages ahead and prefetches those
-      // tiles into L2, so that the ring's loads meet L2 latency rather than DRAM latency
-      int pp = 0, pt = 0, ph = 0;
-      auto prefetch_next = [&]() {
-        if (pp >= nblk - 1) return;
-        tma_prefetch_l2_3d(&tmap, 128 * geo.tile_blk(pp, pt), geo.blk(pp) * QB + Q_KC * ph, b);
-        if (++ph == 2) {
-          ph = 0;
-          if (++pt == geo.ntiles(pp)) { pt = 0; ++pp; }
-        }
-      };
-      for (int i = 0; i < Q_PF; ++i) prefetch_next();
       bool ok = true;
       int g = 0;
       for (int p = 0; p < nblk - 1 && ok; ++p) {
@@ -206,7 +193,6 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
             if (g >= Q_NS && !(ok = mbar_wait(b_empty + 8 * s, ((g / Q_NS) - 1) & 1, err, 41))) break;
             mbar_expect_tx(b_full + 8 * s, Q_STAGE);
             tma_load_3d(s0 + OFF_RING + s * Q_STAGE, &tmap, b_full + 8 * s, 128 * j, col0 + Q_KC * h, b);
-            prefetch_next();
           }
         }
       }

@@ -58,13 +58,6 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
       "l"((unsigned long long)map), "r"(bar), "r"(x), "r"(y), "r"(z)
       : "memory");
 }
-// a tile of a tensor map into L2 only (no shared memory, no completion to wait for)
-__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x, int y, int z) {
-  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
-                   (unsigned long long)map),
-               "r"(x), "r"(y), "r"(z)
-               : "memory");
-}
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
