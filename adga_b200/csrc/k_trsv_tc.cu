@@ -8,9 +8,8 @@
 // on the tensor cores, and every row block keeps its accumulated update in
 // TMEM for the whole solve:
 //   * the triangle's tiles (64 complex rows x 32 columns of one panel, 16 KB
-//     FP32) stream through a 6-stage TMA ring as they lie in memory, real
-//     and imaginary parts interleaved (a tile's load takes ~3 us under the
-//     full load, so the ring's depth sets the rate);
+//     FP32) stream through a 5-stage TMA ring as they lie in memory, real
+//     and imaginary parts interleaved;
 //   * warps 4-7 split every landed tile into hi = tf32(x) (round to nearest)
 //     and lo = x - hi (exact in FP32) and write both as the K-major A
 //     operand of an M = 128 MMA whose rows are the real and imaginary parts
@@ -27,8 +26,7 @@
 //     8-11 solve the diagonal blocks, Y_p = D_p^-1 (B_p - acc_p) with the
 //     64 x 64 block inverses of k_diag_inv, as soon as the first tile of the
 //     previous panel (the one that updates block p) has completed, so that
-//     the rest of that panel streams meanwhile; Y_p enters the (single) B
-//     operand once panel p - 1's MMAs have completed.
+//     the rest of that panel streams meanwhile.
 // TMEM holds one 32-column accumulator per row block after the first solved
 // one: N <= 17 * 64 = 1088.  Every wait is bounded (WAIT_NS); on a timeout the
 // kernel records an error code in *err and returns.
@@ -46,7 +44,7 @@ using namespace umma;
 
 constexpr int QB = 64;                        // block width (the factorisation's NB)
 constexpr int Q_THREADS = 384;
-constexpr int Q_NS = 6;                       // ring stages
+constexpr int Q_NS = 5;                       // ring stages
 constexpr int Q_KC = 32;                      // panel columns per stage
 constexpr int Q_STAGE = 128 * Q_KC * 4;       // 128 reals (64 complex rows) x 32 columns FP32 (16 KB)
 constexpr int Q_NP = 32;                      // MMA N: 16 real-part + 16 imaginary-part rows of B
@@ -57,12 +55,12 @@ constexpr int Q_VST = QB * Q_RMAX * 8;        // B_p - acc_p, [rhs][row] complex
 constexpr int Q_MAXBLK = 17;                  // TMEM: (blocks - 1) x 32 columns <= 512
 constexpr int OFF_RING = 0;
 constexpr int OFF_AOP = OFF_RING + Q_NS * Q_STAGE;   // two A operand pairs (hi, lo), K-major
-constexpr int OFF_BOP = OFF_AOP + 4 * Q_STAGE;       // the B operand pair (hi, lo)
-constexpr int OFF_DINV = OFF_BOP + 2 * Q_BOP;
+constexpr int OFF_BOP = OFF_AOP + 4 * Q_STAGE;       // two B operand pairs (hi, lo)
+constexpr int OFF_DINV = OFF_BOP + 4 * Q_BOP;
 constexpr int OFF_VST = OFF_DINV + Q_DINV;
 constexpr int OFF_BAR = OFF_VST + Q_VST;
-// full[NS] empty[NS] conv[2] opfree[2] crit yready dfull done pdone
-constexpr int Q_NBAR = 2 * Q_NS + 9;
+// full[NS] empty[NS] conv[2] opfree[2] crit yready dfull done
+constexpr int Q_NBAR = 2 * Q_NS + 8;
 constexpr int Q_SMEM = OFF_BAR + 8 * Q_NBAR + 16 + 1024;
 static_assert(Q_SMEM <= 227 * 1024, "shared memory of the tensor-core solve");
 
@@ -144,7 +142,6 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
   const uint32_t bar0 = s0 + OFF_BAR;
   const uint32_t b_full = bar0, b_empty = bar0 + 8 * Q_NS, b_conv = bar0 + 16 * Q_NS, b_opfree = b_conv + 16;
   const uint32_t b_crit = b_opfree + 16, b_yready = b_crit + 8, b_dfull = b_crit + 16, b_done = b_crit + 24;
-  const uint32_t b_pdone = b_crit + 32;     // every MMA of a panel has completed (the B operand is free)
   uint32_t *tslot = reinterpret_cast<uint32_t *>(g0 + OFF_BAR + 8 * Q_NBAR);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int b = blockIdx.x;
@@ -162,11 +159,11 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
       mbar_init(b_conv + 8 * i, 128);
       mbar_init(b_opfree + 8 * i, 1);
     }
-    for (int i = 0; i < 5; ++i) mbar_init(b_crit + 8 * i, 1);
+    for (int i = 0; i < 4; ++i) mbar_init(b_crit + 8 * i, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // the B operand starts at zero: rows n >= R (and 16 + n) are never written
-  for (int e = t; e < 2 * Q_BOP / 16; e += Q_THREADS)
+  // both B operand sets start at zero: rows n >= R (and 16 + n) are never written
+  for (int e = t; e < 4 * Q_BOP / 16; e += Q_THREADS)
     reinterpret_cast<uint4 *>(g0 + OFF_BOP)[e] = make_uint4(0u, 0u, 0u, 0u);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == 0) {
@@ -205,7 +202,7 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
       for (int p = 0; p < nblk - 1 && ok; ++p) {
         if (!(ok = mbar_wait(b_yready, p & 1, err, 42))) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t bop = s0 + OFF_BOP;
+        const uint32_t bop = s0 + OFF_BOP + (p & 1) * 2 * Q_BOP;
         for (int tt = 0; tt < geo.ntiles(p) && ok; ++tt) {
           const uint32_t dt = tmem + geo.tcol(geo.tile_blk(p, tt));
           for (int h = 0; h < 2; ++h, ++g) {
@@ -223,7 +220,6 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
               }
             mma_commit(b_opfree + 8 * o);
             if (tt == 0 && h == 1) mma_commit(b_crit);
-            if (tt == geo.ntiles(p) - 1 && h == 1) mma_commit(b_pdone);
           }
         }
       }
@@ -305,14 +301,11 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
         }
       }
       named_sync(1, 128);
-      // Y_p = D_p^-1 V into registers (item u: row r = e % 64, right-hand side n = e / 64)
-      constexpr int QI = QB * Q_RMAX / 128;
-      z32 yv[QI];
-#pragma unroll
-      for (int u = 0; u < QI; ++u) {
-        const int e = dt_ + 128 * u, r = e % QB, n = e / QB;
-        yv[u] = make_float2(0.f, 0.f);
-        if (n < R && r < jb) {
+      unsigned char *bh = g0 + OFF_BOP + (p & 1) * 2 * Q_BOP, *bl = bh + Q_BOP;
+      for (int e = dt_; e < QB * R; e += 128) {
+        const int r = e % QB, n = e / QB;
+        z32 y = make_float2(0.f, 0.f);
+        if (r < jb) {
           // D^-1 of U is upper triangular, of the unit-lower L lower triangular
           const int kb = geo.upper ? r : 0, ke = geo.upper ? jb : r + 1;
           const float2 *vn = vst + n * QB;
@@ -323,24 +316,14 @@ k_trsv_tc(const __grid_constant__ CUtensorMap tmap, int N, int nsteps, const z32
             cfma(a1, D[r + (k + 1) * QB], vn[k + 1]);
           }
           if (k < ke) cfma(a0, D[r + k * QB], vn[k]);
-          yv[u] = cadd(a0, a1);
-          Cb[(size_t)(r0 + r) + (size_t)n * ldc] = yv[u];
+          y = cadd(a0, a1);
+          Cb[(size_t)(r0 + r) + (size_t)n * ldc] = y;
         }
-      }
-      // the B operand is free once panel p - 1's MMAs completed
-      w = p == 0 || mbar_wait(b_pdone, (p - 1) & 1, err, 49);
-      if (!named_and(1, 128, w)) break;
-      unsigned char *bh = g0 + OFF_BOP, *bl = bh + Q_BOP;
-#pragma unroll
-      for (int u = 0; u < QI; ++u) {
-        const int e = dt_ + 128 * u, r = e % QB, n = e / QB;
-        if (n < R) {
-          const float hr = tf32_rna(yv[u].x), hi = tf32_rna(yv[u].y);
-          *reinterpret_cast<float *>(bh + bop_off(n, r)) = hr;
-          *reinterpret_cast<float *>(bl + bop_off(n, r)) = yv[u].x - hr;
-          *reinterpret_cast<float *>(bh + bop_off(16 + n, r)) = hi;
-          *reinterpret_cast<float *>(bl + bop_off(16 + n, r)) = yv[u].y - hi;
-        }
+        const float hr = tf32_rna(y.x), hi = tf32_rna(y.y);
+        *reinterpret_cast<float *>(bh + bop_off(n, r)) = hr;
+        *reinterpret_cast<float *>(bl + bop_off(n, r)) = y.x - hr;
+        *reinterpret_cast<float *>(bh + bop_off(16 + n, r)) = hi;
+        *reinterpret_cast<float *>(bl + bop_off(16 + n, r)) = y.y - hi;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       named_sync(1, 128);
