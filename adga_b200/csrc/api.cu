@@ -35,20 +35,13 @@ int tc_available();
 int tc_trail_error(void *ctx);
 int *tc_err_flag(void *ctx);
 int tc_pair_supported(void *ctx);
-cudaError_t tc_pair_narrow(void *ctx, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                           cudaEvent_t ev0, cudaEvent_t ev1, bool staged);
-cudaError_t tc_pair_wide(void *ctx, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                         cudaEvent_t ev0, cudaEvent_t ev1, bool staged);
+cudaError_t tc_group_update(void *ctx, int first, int count, int nst, const int *Js, const int *jbs, bool wide,
+                            cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, bool staged);
 cudaError_t tc_tri_step(void *ctx, int first, int count, int J, int jb, int set, cudaStream_t st);
-static cudaError_t tc_pair_narrow_fn(void *r, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0,
-                                     cudaEvent_t ev1) {
+static cudaError_t tc_group_fn(void *r, int nst, const int *Js, const int *jbs, bool wide, cudaStream_t st,
+                               cudaEvent_t ev0, cudaEvent_t ev1) {
   TcRange *x = (TcRange *)r;
-  return tc_pair_narrow(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1, x->staged);
-}
-static cudaError_t tc_pair_wide_fn(void *r, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0,
-                                   cudaEvent_t ev1) {
-  TcRange *x = (TcRange *)r;
-  return tc_pair_wide(x->ctx, x->first, x->count, J0, jb, jb2, st, ev0, ev1, x->staged);
+  return tc_group_update(x->ctx, x->first, x->count, nst, Js, jbs, wide, st, ev0, ev1, x->staged);
 }
 static cudaError_t tc_tri_fn(void *r, int J, int jb, int set, cudaStream_t st) {
   TcRange *x = (TcRange *)r;
@@ -679,6 +672,7 @@ static size_t bytes_per_point(const adga_handle *h, int prec, int NB) {
     b += 2 * N * (N + R) * 8 + 2 * 2 * nsteps * NB * NB * 8;
     b += 2 * 2 * R * N * 16 + 2 * R * N * 8 + 2 * ((R + 15) / 16) * 16 * N * 8 + 2 * N * 4 + 64;
     b += 2 * 7 * R * ((2 * N + 63) / 64 * 64) + 2 * R * 4;   // int8 residual slices and scales
+    b += 2 * 3 * (N + N + R) * 4 * NB * 2;                     // three tensor-core operand stagings
   }
   return b;
 }
@@ -765,14 +759,15 @@ static cudaError_t factor_batch(adga_handle *h, T *M, const LUBatch &lb, bool ap
   // overlap on the t2g workload; kept as an option (ADGA_TWO_STREAMS=1)
   const bool split = h->st2 && lb.batch >= 8 && getenv("ADGA_TWO_STREAMS");
   if constexpr (sizeof(T) == sizeof(z32)) {
-    // unpivoted FP32 with the tensor cores: delayed two-step updates (tune.pairs = 0: step by step)
+    // unpivoted FP32 with the tensor cores: delayed updates in groups of tune.pairs + 1 steps
+    // (tune.pairs = 0: step by step)
     if (!split && nopiv && tc && tc_pair_supported(h->tc) && h->tune.pairs) {
       // L21 / U12 on the tensor cores with the staging written by the same kernel
       // (tune.tri_tc = 0: the FP32 CUDA-core tile products and the split kernels)
       const bool tri_tc = (lb.N % 2) == 0 && h->tune.tri_tc;
       TcRange r{h->tc, 0, lb.batch, tri_tc};
-      PairOps ops{tc_pair_narrow_fn, tc_pair_wide_fn, &r, tri_tc ? tc_tri_fn : nullptr};
-      return lu_factor_pairs(M, lb, ops, st, tt);
+      GroupOps ops{tc_group_fn, &r, tri_tc ? tc_tri_fn : nullptr, h->tune.pairs + 1};
+      return lu_factor_groups(M, lb, ops, st, tt);
     }
   }
   if (!split) {
@@ -1506,9 +1501,10 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
 // ---------------------------------------------------------------------------
 extern "C" int adga_set_tune(adga_handle *h, const adga_tune *t) {
   if (!h || !t) return ADGA_EINVAL;
-  if (t->factor < 0 || t->factor > 1 || t->pairs < 0 || t->pairs > 1 || t->tri_tc < 0 || t->tri_tc > 1 ||
+  if (t->factor < 0 || t->factor > 1 || t->pairs < 0 || t->pairs > 2 || t->tri_tc < 0 || t->tri_tc > 1 ||
       t->batch < 0 || t->resid < 0 || t->resid > 1 || t->trsv_tc < 0 || t->trsv_tc > 1)
-    return fail(h, ADGA_EINVAL, "adga_set_tune: factor, pairs, tri_tc, resid, trsv_tc in {0, 1}, batch >= 0");
+    return fail(h, ADGA_EINVAL,
+                "adga_set_tune: factor, tri_tc, resid, trsv_tc in {0, 1}, pairs in {0, 1, 2}, batch >= 0");
   h->tune = *t;
   return 0;
 }
@@ -1568,6 +1564,7 @@ extern "C" int adga_autotune(adga_handle *h, int qwstart, int qwstop, double tol
   if (tc) {
     if (c.N % 2 == 0) {
       cand.push_back(with(0, 1, 1, 1, 1));
+      cand.push_back(with(0, 2, 1, 1, 1));
       cand.push_back(with(0, 1, 1, 1, 0));
       cand.push_back(with(0, 1, 1, 0, 1));
     }

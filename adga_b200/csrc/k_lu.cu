@@ -1155,25 +1155,31 @@ static void trail_account(TrailTiming *tt, double m, double n, double k, int bat
 // Unpivoted FP32 factorisation with delayed updates: steps in pairs (J0, J1 = J0 + NB);
 // after J0 only the parts of its update that step J1 reads (ops.narrow), after J1
 // both steps' updates of the rest at once (ops.wide)
-cudaError_t lu_factor_pairs(z32 *M, const LUBatch &lb, const PairOps &ops, cudaStream_t st, TrailTiming *tt) {
+cudaError_t lu_factor_groups(z32 *M, const LUBatch &lb, const GroupOps &ops, cudaStream_t st, TrailTiming *tt) {
+  if (ops.G < 2 || ops.G > 3) return cudaErrorInvalidValue;
   const int nsteps = lb.nsteps();
+  int Js[3], jbs[3];
   for (int s = 0; s < nsteps; ++s) {
-    const int J = s * lb.NB, jb = min(lb.NB, lb.N - J);
+    const int J = s * lb.NB, jb = min(lb.NB, lb.N - J), g = s % ops.G;
+    Js[g] = J;
+    jbs[g] = jb;
     cudaError_t e = nopiv_step_kernels(M, lb, J, jb, st, ops.tri == nullptr);
-    if (e == cudaSuccess && ops.tri) e = ops.tri(ops.ctx, J, jb, s % 2, st);
+    if (e == cudaSuccess && ops.tri) e = ops.tri(ops.ctx, J, jb, g, st);
     if (e != cudaSuccess) return e;
     if (J + jb >= lb.N) break;
     cudaEvent_t ev0 = (tt && tt->ev) ? tt->ev[2 * tt->n] : nullptr;
     cudaEvent_t ev1 = (tt && tt->ev) ? tt->ev[2 * tt->n + 1] : nullptr;
-    if (s % 2 == 0) {
-      const int J1 = J + jb, jb2 = min(lb.NB, lb.N - J1);
-      e = ops.narrow(ops.ctx, J, jb, jb2, st, ev0, ev1);
-      trail_account(tt, lb.N - J1, jb2, jb, lb.batch);
-      trail_account(tt, jb2, lb.ncols - J1 - jb2, jb, lb.batch);
+    const bool wide = g == ops.G - 1;
+    e = ops.update(ops.ctx, g + 1, Js, jbs, wide, st, ev0, ev1);
+    int K = 0;
+    for (int i = 0; i <= g; ++i) K += jbs[i];
+    const int R = J + jb;
+    if (wide) {
+      trail_account(tt, lb.N - R, lb.ncols - R, K, lb.batch);
     } else {
-      const int J0 = J - lb.NB, R0 = J + jb;
-      e = ops.wide(ops.ctx, J0, lb.NB, jb, st, ev0, ev1);
-      trail_account(tt, lb.N - R0, lb.ncols - R0, lb.NB + jb, lb.batch);
+      const int jt = min(lb.NB, lb.N - R);
+      trail_account(tt, lb.N - R, jt, K, lb.batch);
+      trail_account(tt, jt, lb.ncols - R - jt, K, lb.batch);
     }
     if (e != cudaSuccess) return e;
     if (tt && tt->ev) tt->n++;

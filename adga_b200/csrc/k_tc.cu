@@ -235,12 +235,19 @@ __device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x
 }
 
 
+// the tensor maps of up to three operand stagings (the steps of a delayed group) and of C,
+// and each staging's row / column offset for the region's first C row / column
+constexpr int P_MAXST = 3;
+struct alignas(64) PMaps {
+  CUtensorMap a[P_MAXST], b[P_MAXST], c;
+};
+struct POff {
+  int ar[P_MAXST], bc[P_MAXST];
+};
+
 __global__ void __launch_bounds__(P_THREADS, 1)
-k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-             const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB2,
-             const __grid_constant__ CUtensorMap mapC, z32 *M, size_t strideM, int N, int crow0, int ccol0,
-             int arow0, int bcol0, int arow2, int bcol2, int nkb1, int Mrows, int Ncols, int Ncap, int nkb, int b0,
-             int count, int nbk, int *err) {
+k_tc_persist(const __grid_constant__ PMaps maps, z32 *M, size_t strideM, int N, int crow0, int ccol0, POff off,
+             int nkb1, int Mrows, int Ncols, int Ncap, int nkb, int b0, int count, int nbk, int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
@@ -292,10 +299,11 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
             break;
           const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
           mbar_expect_tx(bar_full + 8 * s, STAGE_BYTES);
-          // k-blocks [0, nkb1) from the first staging, the rest from the second
-          const bool second = kb >= nkb1;
-          const CUtensorMap *ma = second ? &mapA2 : &mapA, *mb = second ? &mapB2 : &mapB;
-          const int kl = second ? kb - nkb1 : kb, ar = second ? arow2 : arow0, bc = second ? bcol2 : bcol0;
+          // k-blocks [i nkb1, (i + 1) nkb1) from staging i
+          const int sti = kb / nkb1, kl = kb - sti * nkb1;
+          const CUtensorMap *ma = &maps.a[sti], *mb = &maps.b[sti];
+          const int ar = sti == 0 ? off.ar[0] : sti == 1 ? off.ar[1] : off.ar[2];
+          const int bc = sti == 0 ? off.bc[0] : sti == 1 ? off.bc[1] : off.bc[2];
           const int xa = kx_a(kl, nbk), xb = kx_b(kl, nbk);
           tma_load_3d(sa, ma, bar_full + 8 * s, xa, ar + tm * BM, b);
           tma_load_3d(sb, mb, bar_full + 8 * s, xb, bc + tn * BN, b);
@@ -319,7 +327,7 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           if (!(ok = mbar_wait(bar_full + 8 * s, (kbt / P_STAGES) & 1, err, 13))) break;
           asm volatile("tcgen05.fence::after_thread_sync;");
           const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
-          const uint32_t neg = neg_bi(kb >= nkb1 ? kb - nkb1 : kb, nbk);
+          const uint32_t neg = neg_bi(kb % nkb1, nbk);
           const uint32_t idesc = Ncols - (tile % ntn) * BN <= 64 ? IDESC_Q : IDESC_H;
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k)
@@ -345,9 +353,9 @@ k_tc_persist(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ C
           ++u;
           mbar_expect_tx(bar_cfull, P_CH_BYTES);
           // x counts floats: rows crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
-          tma_load_3d(scbase, &mapC, bar_cfull, 2 * (crow0 + tm * BM), ccol0 + tn * BN + h * P_CH_COLS, b);
+          tma_load_3d(scbase, &maps.c, bar_cfull, 2 * (crow0 + tm * BM), ccol0 + tn * BN + h * P_CH_COLS, b);
           if (h == 0 && tn * BN + P_CH_COLS < Ncols)
-            tma_prefetch_l2_3d(&mapC, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
+            tma_prefetch_l2_3d(&maps.c, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
         }
         if (!ok) break;
       }
@@ -795,14 +803,13 @@ k_split_b(const z32 *M, size_t strideM, int N, int J, int jb, int Ncols, int Nca
 struct TcCtx {
   z32 *M;
   LUBatch lb;
-  __nv_bfloat16 *A = nullptr, *B = nullptr;
+  // operand stagings: set 0 for step-by-step updates, sets 0..G-1 for the steps of a delayed group
+  __nv_bfloat16 *A[P_MAXST] = {nullptr, nullptr, nullptr}, *B[P_MAXST] = {nullptr, nullptr, nullptr};
   int *err = nullptr;
   int Ncap = 0;
   int nsm = 0;
   bool persist = false;        // C tiles by TMA: needs 16-byte column and matrix strides
-  CUtensorMap mapA, mapB, mapC;
-  __nv_bfloat16 *A2 = nullptr, *B2 = nullptr;   // second staging (the later step of a delayed pair)
-  CUtensorMap mapA2, mapB2;
+  CUtensorMap mapA[P_MAXST], mapB[P_MAXST], mapC;
 };
 
 bool make_map(CUtensorMap *map, void *base, uint64_t inner, uint64_t rows, uint64_t batch) {
@@ -850,18 +857,16 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   c->lb = lb;
   c->Ncap = lb.ncols;
   const size_t K4 = 4 * (size_t)lb.NB;       // four staging segments per step
-  cudaError_t e = cudaMalloc(&c->A, sizeof(__nv_bfloat16) * K4 * lb.N * lb.batch);
-  if (e == cudaSuccess) e = cudaMalloc(&c->B, sizeof(__nv_bfloat16) * K4 * c->Ncap * lb.batch);
-  // second staging for the unpivoted path's delayed two-step updates
-  if (e == cudaSuccess) e = cudaMalloc(&c->A2, sizeof(__nv_bfloat16) * K4 * lb.N * lb.batch);
-  if (e == cudaSuccess) e = cudaMalloc(&c->B2, sizeof(__nv_bfloat16) * K4 * c->Ncap * lb.batch);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < P_MAXST && e == cudaSuccess; ++i) {
+    e = cudaMalloc(&c->A[i], sizeof(__nv_bfloat16) * K4 * lb.N * lb.batch);
+    if (e == cudaSuccess) e = cudaMalloc(&c->B[i], sizeof(__nv_bfloat16) * K4 * c->Ncap * lb.batch);
+    if (e == cudaSuccess && (!make_map(&c->mapA[i], c->A[i], K4, lb.N, lb.batch) ||
+                             !make_map(&c->mapB[i], c->B[i], K4, (uint64_t)c->Ncap, lb.batch)))
+      e = cudaErrorInvalidValue;
+  }
   if (e == cudaSuccess) e = cudaMalloc(&c->err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemsetAsync(c->err, 0, sizeof(int), st);
-  if (e == cudaSuccess && (!make_map(&c->mapA, c->A, K4, lb.N, lb.batch) ||
-                           !make_map(&c->mapB, c->B, K4, (uint64_t)c->Ncap, lb.batch) ||
-                           !make_map(&c->mapA2, c->A2, K4, lb.N, lb.batch) ||
-                           !make_map(&c->mapB2, c->B2, K4, (uint64_t)c->Ncap, lb.batch)))
-    e = cudaErrorInvalidValue;
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   // the persistent kernel: C column stride (N * 8 B) and matrix stride on 16 bytes
@@ -875,7 +880,8 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
     c->persist = c->nsm > 0;
   }
   if (e != cudaSuccess) {
-    cudaFree(c->A); cudaFree(c->B); cudaFree(c->A2); cudaFree(c->B2); cudaFree(c->err);
+    for (int i = 0; i < P_MAXST; ++i) { cudaFree(c->A[i]); cudaFree(c->B[i]); }
+    cudaFree(c->err);
     delete c;
     return e;
   }
@@ -883,63 +889,27 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   return cudaSuccess;
 }
 
-cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, cudaStream_t st,
-                               cudaEvent_t ev0, cudaEvent_t ev1) {
-  TcCtx *c = (TcCtx *)ctxp;
-  const LUBatch &lb = c->lb;
-  const int Mrows = lb.N - J - jb, Ncols = lb.ncols - J - jb;
-  if (Mrows <= 0 || Ncols <= 0 || count <= 0) return cudaSuccess;
-  const int NB = lb.NB;
-  k_split_a<<<dim3(cdiv_u(Mrows, 64), count), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Mrows, NB, c->A,
-                                                            first);
-  cudaError_t e = ADGA_LAUNCH_CHECK();
-  if (e != cudaSuccess) return e;
-  const int per = 256 / NB;
-  k_split_b<<<dim3(cdiv_u(Ncols, per), count), 256, 0, st>>>(c->M, lb.strideM, lb.N, J, jb, Ncols,
-                                                             c->Ncap, NB, c->B, first);
-  if ((e = ADGA_LAUNCH_CHECK()) != cudaSuccess) return e;
-  if (ev0) cudaEventRecord(ev0, st);
-  if (c->persist) {
-    const long long ntiles = (long long)cdiv_u(Ncols, BN) * cdiv_u(Mrows, BM) * count;
-    const int grid = (int)std::min<long long>(ntiles, c->nsm);
-    const int nkb = 6 * NB / BK;
-    k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapA, c->mapB, c->mapC, c->M,
-                                                         lb.strideM, lb.N, J + jb, J + jb, 0, 0, 0, 0, nkb, Mrows,
-                                                         Ncols, c->Ncap, nkb, first, count, NB / BK, c->err);
-  } else {
-    dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), count);
-    k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA, c->mapB, c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
-                                               c->Ncap, 6 * NB / BK, first, NB / BK, c->err);
-  }
-  e = ADGA_LAUNCH_CHECK();
-  if (ev1) cudaEventRecord(ev1, st);
-  return e;
-}
-
-// ---------------------------------------------------------------------------
-// Delayed updates of the unpivoted path, two steps J0 (width jb) and J1 = J0 + jb
-// (width jb2) at a time:
-//   tc_pair_narrow  after step J0: its update restricted to the columns of step
-//                   J1 (all rows below J0 + jb) and to the rows of step J1
-//                   (columns right of J1 + jb2) -- what step J1's factorisation reads;
-//   tc_pair_wide    after step J1: the rest, rows and columns from J1 + jb2, with
-//                   both steps' L21 / U12 as one K = 12 NB product.
-// The C read-modify-write of the largest region happens once per two steps.
-// ---------------------------------------------------------------------------
 namespace {
-// C[crow0 + m, ccol0 + n] -= A.B over rows m < Mrows, columns n < Ncols, from the first
-// staging at (arow0, bcol0) and, when two, the second at (arow2, bcol2)
-cudaError_t persist_region(TcCtx *c, bool two, int first, int count, int crow0, int ccol0, int arow0, int bcol0,
-                           int arow2, int bcol2, int Mrows, int Ncols, cudaStream_t st) {
+// C[crow0 + m, ccol0 + n] -= sum_i A_i.B_i over rows m < Mrows, columns n < Ncols, from the
+// stagings i < nst, staging i at row offset ar[i] (A) and column offset bc[i] (B)
+cudaError_t persist_region(TcCtx *c, int nst, const int *ar, const int *bc, int first, int count, int crow0,
+                           int ccol0, int Mrows, int Ncols, cudaStream_t st) {
   if (Mrows <= 0 || Ncols <= 0 || count <= 0) return cudaSuccess;
   const LUBatch &lb = c->lb;
   const long long ntiles = (long long)cdiv_u(Ncols, BN) * cdiv_u(Mrows, BM) * count;
   const int grid = (int)std::min<long long>(ntiles, c->nsm);
   const int nkb1 = 6 * lb.NB / BK;
-  k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(c->mapA, c->mapB, c->mapA2, c->mapB2, c->mapC, c->M,
-                                                       lb.strideM, lb.N, crow0, ccol0, arow0, bcol0, arow2, bcol2,
-                                                       nkb1, Mrows, Ncols, c->Ncap, two ? 2 * nkb1 : nkb1, first,
-                                                       count, lb.NB / BK, c->err);
+  PMaps maps;
+  POff off{};
+  for (int i = 0; i < P_MAXST; ++i) {
+    maps.a[i] = c->mapA[i];
+    maps.b[i] = c->mapB[i];
+    off.ar[i] = i < nst ? ar[i] : 0;
+    off.bc[i] = i < nst ? bc[i] : 0;
+  }
+  maps.c = c->mapC;
+  k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(maps, c->M, lb.strideM, lb.N, crow0, ccol0, off, nkb1, Mrows,
+                                                       Ncols, c->Ncap, nst * nkb1, first, count, lb.NB / BK, c->err);
   return ADGA_LAUNCH_CHECK();
 }
 
@@ -962,14 +932,81 @@ cudaError_t stage_step(TcCtx *c, __nv_bfloat16 *A, __nv_bfloat16 *B, int first, 
 }
 }  // namespace
 
+cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, cudaStream_t st,
+                               cudaEvent_t ev0, cudaEvent_t ev1) {
+  TcCtx *c = (TcCtx *)ctxp;
+  const LUBatch &lb = c->lb;
+  const int Mrows = lb.N - J - jb, Ncols = lb.ncols - J - jb;
+  if (Mrows <= 0 || Ncols <= 0 || count <= 0) return cudaSuccess;
+  const int NB = lb.NB;
+  cudaError_t e = stage_step(c, c->A[0], c->B[0], first, count, J, jb, st);
+  if (e != cudaSuccess) return e;
+  if (ev0) cudaEventRecord(ev0, st);
+  if (c->persist) {
+    const int zero[1] = {0};
+    e = persist_region(c, 1, zero, zero, first, count, J + jb, J + jb, Mrows, Ncols, st);
+  } else {
+    dim3 grid(cdiv_u(Ncols, BN), cdiv_u(Mrows, BM), count);
+    k_tc_update<<<grid, 192, SMEM_BYTES, st>>>(c->mapA[0], c->mapB[0], c->M, lb.strideM, lb.N, J, jb, Mrows, Ncols,
+                                               c->Ncap, 6 * NB / BK, first, NB / BK, c->err);
+    e = ADGA_LAUNCH_CHECK();
+  }
+  if (ev1) cudaEventRecord(ev1, st);
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// Delayed updates of the unpivoted path in groups of G steps (G = 2 or 3): after step
+// g of a group (steps J_i, widths jb_i, i <= g, staged in sets i):
+//   g < G - 1   the group's updates so far restricted to what step g + 1 reads: its
+//               columns below it and its rows right of it (K = (g + 1) * 6 NB);
+//   g = G - 1   the rest, rows and columns from J_g + jb_g, with all G steps' L21 / U12
+//               as one K = G * 6 NB product.
+// The C read-modify-write of the largest region happens once per G steps.
+// ---------------------------------------------------------------------------
 int tc_pair_supported(void *ctxp) { return ctxp && ((TcCtx *)ctxp)->persist && ((TcCtx *)ctxp)->lb.NB == 64; }
 
+cudaError_t tc_group_update(void *ctxp, int first, int count, int nst, const int *Js, const int *jbs, bool wide,
+                            cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, bool staged) {
+  TcCtx *c = (TcCtx *)ctxp;
+  const LUBatch &lb = c->lb;
+  if (nst < 1 || nst > P_MAXST) return cudaErrorInvalidValue;
+  const int g = nst - 1;
+  cudaError_t e = staged ? cudaSuccess : stage_step(c, c->A[g], c->B[g], first, count, Js[g], jbs[g], st);
+  if (e != cudaSuccess) return e;
+  const int R = Js[g] + jbs[g];             // first row / column after the newest step
+  int ar[P_MAXST], bc[P_MAXST];
+  auto offsets = [&](int crow0, int ccol0) {
+    for (int i = 0; i < nst; ++i) {
+      ar[i] = crow0 - (Js[i] + jbs[i]);
+      bc[i] = ccol0 - (Js[i] + jbs[i]);
+    }
+  };
+  if (ev0) cudaEventRecord(ev0, st);
+  if (wide) {
+    offsets(R, R);
+    e = persist_region(c, nst, ar, bc, first, count, R, R, lb.N - R, lb.ncols - R, st);
+  } else {
+    const int jt = std::min(lb.NB, lb.N - R);   // the next step's width
+    // its columns, every row below R
+    offsets(R, R);
+    e = persist_region(c, nst, ar, bc, first, count, R, R, lb.N - R, jt, st);
+    // its rows, the columns right of it
+    if (e == cudaSuccess) {
+      offsets(R, R + jt);
+      e = persist_region(c, nst, ar, bc, first, count, R, R + jt, jt, lb.ncols - R - jt, st);
+    }
+  }
+  if (ev1) cudaEventRecord(ev1, st);
+  return e;
+}
+
 // L21 and U12 of unpivoted step (J, jb) on the tensor cores (k_tc_tri), which also
-// writes the step's operand staging: set 0 (the first step of a pair) or 1 (the second)
+// writes the step's operand staging set (its index in its delayed group)
 cudaError_t tc_tri_step(void *ctxp, int first, int count, int J, int jb, int set, cudaStream_t st) {
   TcCtx *c = (TcCtx *)ctxp;
   const LUBatch &lb = c->lb;
-  if (!c->persist || lb.NB != 64 || (jb & 1)) return cudaErrorInvalidValue;
+  if (!c->persist || lb.NB != 64 || (jb & 1) || set < 0 || set >= P_MAXST) return cudaErrorInvalidValue;
   const int ntA = (int)cdiv_u(std::max(lb.N - J - jb, 0), TT_ROWS);
   const int ntU = (int)cdiv_u(std::max(lb.ncols - J - jb, 0), TT_ROWS);
   if (ntA + ntU == 0 || count <= 0) return cudaSuccess;
@@ -977,40 +1014,8 @@ cudaError_t tc_tri_step(void *ctxp, int first, int count, int J, int jb, int set
   if (e != cudaSuccess) return e;
   k_tc_tri<<<(unsigned)((ntA + ntU) * count), TT_THREADS, TT_SMEM_BYTES, st>>>(
       c->M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, lb.nsteps(), (const z32 *)lb.Linv, (const z32 *)lb.Uinv,
-      set ? c->A2 : c->A, set ? c->B2 : c->B, c->Ncap, first, ntA, ntU, c->err);
+      c->A[set], c->B[set], c->Ncap, first, ntA, ntU, c->err);
   return ADGA_LAUNCH_CHECK();
-}
-
-cudaError_t tc_pair_narrow(void *ctxp, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                           cudaEvent_t ev0, cudaEvent_t ev1, bool staged) {
-  TcCtx *c = (TcCtx *)ctxp;
-  const LUBatch &lb = c->lb;
-  cudaError_t e = staged ? cudaSuccess : stage_step(c, c->A, c->B, first, count, J0, jb, st);
-  if (e != cudaSuccess) return e;
-  const int J1 = J0 + jb;
-  if (ev0) cudaEventRecord(ev0, st);
-  // columns of step J1, every row below J1
-  e = persist_region(c, false, first, count, J1, J1, 0, 0, 0, 0, lb.N - J1, jb2, st);
-  // rows of step J1, the columns right of it
-  if (e == cudaSuccess)
-    e = persist_region(c, false, first, count, J1, J1 + jb2, 0, jb2, 0, 0, jb2, lb.ncols - J1 - jb2, st);
-  if (ev1) cudaEventRecord(ev1, st);
-  return e;
-}
-
-cudaError_t tc_pair_wide(void *ctxp, int first, int count, int J0, int jb, int jb2, cudaStream_t st,
-                         cudaEvent_t ev0, cudaEvent_t ev1, bool staged) {
-  TcCtx *c = (TcCtx *)ctxp;
-  const LUBatch &lb = c->lb;
-  const int J1 = J0 + jb, R0 = J1 + jb2;
-  if (lb.N - R0 <= 0) return cudaSuccess;
-  // step J0's staging (rows / columns from J1) is still valid
-  cudaError_t e = staged ? cudaSuccess : stage_step(c, c->A2, c->B2, first, count, J1, jb2, st);
-  if (e != cudaSuccess) return e;
-  if (ev0) cudaEventRecord(ev0, st);
-  e = persist_region(c, true, first, count, R0, R0, jb2, jb2, 0, 0, lb.N - R0, lb.ncols - R0, st);
-  if (ev1) cudaEventRecord(ev1, st);
-  return e;
 }
 
 int tc_trail_error(void *ctxp) {
@@ -1026,10 +1031,10 @@ int *tc_err_flag(void *ctxp) { return ctxp ? ((TcCtx *)ctxp)->err : nullptr; }
 void tc_trail_free(void *ctxp) {
   TcCtx *c = (TcCtx *)ctxp;
   if (!c) return;
-  cudaFree(c->A);
-  cudaFree(c->B);
-  cudaFree(c->A2);
-  cudaFree(c->B2);
+  for (int i = 0; i < P_MAXST; ++i) {
+    cudaFree(c->A[i]);
+    cudaFree(c->B[i]);
+  }
   cudaFree(c->err);
   delete c;
 }

@@ -55,19 +55,21 @@ cudaError_t lu_factor(T *M, const LUBatch &lb, bool apply_left, trail_fn trail, 
 template <typename T>
 cudaError_t lu_step(T *M, const LUBatch &lb, int s, bool apply_left, trail_fn trail, void *trail_ctx,
                     cudaStream_t st, TrailTiming *tt = nullptr, bool nopiv = false);
-// Delayed updates of the unpivoted FP32 factorisation (tensor cores): after step
-// J0 (width jb) `narrow` applies its update to what step J1 = J0 + jb (width jb2)
-// reads; after step J1 `wide` applies both steps' updates to the rest.
+// Delayed updates of the unpivoted FP32 factorisation (tensor cores) in groups of G
+// steps (G = 2 or 3): after step g of a group (steps Js[i], widths jbs[i], i <= g),
+// `update` applies the group's updates so far to what step g + 1 reads (wide = false)
+// or, after the group's last step, to the rest (wide = true).
 // tri (optional): L21 and U12 of step (J, jb) in place of the CUDA-core tile
-// products, also writing the operand staging set (0: first step of a pair, 1: second)
-struct PairOps {
-  cudaError_t (*narrow)(void *ctx, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
-  cudaError_t (*wide)(void *ctx, int J0, int jb, int jb2, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
+// products, also writing operand staging set `set` (the step's index in its group)
+struct GroupOps {
+  cudaError_t (*update)(void *ctx, int nst, const int *Js, const int *jbs, bool wide, cudaStream_t st,
+                        cudaEvent_t ev0, cudaEvent_t ev1);
   void *ctx;
   cudaError_t (*tri)(void *ctx, int J, int jb, int set, cudaStream_t st) = nullptr;
+  int G = 2;
 };
-cudaError_t lu_factor_pairs(z32 *M, const LUBatch &lb, const PairOps &ops, cudaStream_t st,
-                            TrailTiming *tt = nullptr);
+cudaError_t lu_factor_groups(z32 *M, const LUBatch &lb, const GroupOps &ops, cudaStream_t st,
+                             TrailTiming *tt = nullptr);
 // the matrices [first, first + count) of a batch as a batch of their own
 template <typename T>
 inline LUBatch lu_sub(const LUBatch &lb, int first, int count) {

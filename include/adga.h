@@ -222,7 +222,8 @@ int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
  *              refinement; 1: the FP64 LU (no refinement), for sizes where
  *              it is the faster way to the same accuracy
  *   pairs   1: delayed two-step tensor-core updates (K = 128 per C pass);
- *           0: one update per step (K = 64)
+ *           2: three-step groups (K = 192 per C pass); 0: one update per
+ *           step (K = 64)
  *   tri_tc  1: the L21 / U12 panel products on the tensor cores, writing the
  *              update operands directly; 0: FP32 CUDA-core tile products and
  *              separate operand-split kernels

@@ -89,6 +89,32 @@ def test_refinement_residual_matches_oracle(name, resid):
         assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
 
 
+@pytest.mark.parametrize("name", ["t3b", "t3m", "c3s"])
+def test_groups_of_three_match_oracle(name):
+    """tune pairs = 2: the tensor-core updates delayed in groups of three steps
+    (the next step's strips after each step, the rest with a K = 3 * 6 NB product
+    from three operand stagings); N = 144 (one group ending at the last step),
+    216 (a group and a lone step), 320 (a group and a pair)."""
+    p = problem(name)
+    s = p.spec
+    with library_env({}):
+        lad = Ladder.from_problem(p)
+    try:
+        for iwb in range(-s.iwb, s.iwb + 1):
+            lad.set_vertex(iwb, *p.vertex(iwb))
+        lad.tune = {"pairs": 2}
+        status, stats = lad.ladder_run(1, None, "mixed")
+        got = lad.get_outputs()
+        got.update(lad.assemble(got, p.siw))
+    finally:
+        lad.close()
+    want = oracle_run(p)
+    assert stats["mixed_fallbacks"] == 0 and not status.any()
+    assert stats["max_refine_iters"] <= 3
+    for k in ("chi_dens", "chi_magn", "sigma", "chi_qw_dens", "chi_qw_magn"):
+        assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
+
+
 @pytest.mark.parametrize("name", ["t3b", "t3m"])
 def test_step_by_step_updates_match_oracle(name):
     """ADGA_NO_PAIRS=1: the unpivoted FP32 factorisation with one tensor-core
