@@ -109,7 +109,7 @@ struct adga_handle {
   bool refine_estimate = true;   // stop on the bounded next correction (ADGA_REFINE_EXACT=1: on a solved one)
   bool mixed_nopiv = true;   // FP32 factorisation without row interchanges (ADGA_MIXED_PIVOT=1: with)
   double tol = 1e-10;   // stop when max|dX| <= tol * max|X| (the error is then far below)
-  adga_tune tune{0, 1, 1, 0, 1, 1};   // mixed-path kernel choices (adga_set_tune / adga_autotune)
+  adga_tune tune{0, 2, 1, 0, 1, 1};   // mixed-path kernel choices (adga_set_tune / adga_autotune)
   void *ri8 = nullptr;            // int8-slice residual context (k_resid_i8.cu), with the mixed work
   long long frow_gen = 0;         // bumped whenever F~ is recomputed (its residual slices go stale)
   // last-run statistics
@@ -1563,10 +1563,10 @@ extern "C" int adga_autotune(adga_handle *h, int qwstart, int qwstop, double tol
   const bool tc = tc_available() && !getenv("ADGA_NO_TC");
   if (tc) {
     if (c.N % 2 == 0) {
-      cand.push_back(with(0, 1, 1, 1, 1));
       cand.push_back(with(0, 2, 1, 1, 1));
-      cand.push_back(with(0, 1, 1, 1, 0));
-      cand.push_back(with(0, 1, 1, 0, 1));
+      cand.push_back(with(0, 1, 1, 1, 1));
+      cand.push_back(with(0, 2, 1, 1, 0));
+      cand.push_back(with(0, 2, 1, 0, 1));
     }
     cand.push_back(with(0, 1, 0, 1, 0));
     cand.push_back(with(0, 0, 0, 1, 0));

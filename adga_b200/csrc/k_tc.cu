@@ -205,13 +205,21 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
 // ---------------------------------------------------------------------------
 // Persistent variant: one CTA per SM loops over the (column tile, row tile,
-// matrix) tiles of the launch.  The operand k-blocks stream through a
-// 3-stage TMA ring (144 KB); the accumulator is double-buffered in TMEM
+// matrix) tiles of the launch; the accumulator is double-buffered in TMEM
 // (2 x 256 columns), so the epilogue of one tile overlaps the loads and MMAs
-// of the next.  The C tile reaches shared memory by TMA one 64-column half at
-// a time through one 64 KB buffer (the second half is prefetched into L2
-// when the first is loaded).
-//   warp 0        TMA loads of the A/B k-blocks (ring of P_STAGES)
+// of the next.  Operands: the six k-segment products of a step's K = 64 use
+// only four A and four B segments (A = [Lr_hi, Li_hi, Lr_lo, Li_lo], B =
+// [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo]; product j multiplies A segment seg_a(j)
+// by B segments seg_b(j) (real part) and seg_b(j) ^ 1 (imaginary part)), so
+// each 16 KB operand tile is loaded once per step and tile and serves two or
+// four products.  The tiles travel in pairs through a ring of five 32 KB
+// slots, in the order [B2 B3] [A0 A1] [B0 B1] [A2 A3]; the products run in
+// the order j = 2, 3 (first two slots), 0, 1 (third), 4, 5 (fourth), which
+// frees the slots in the order they were filled.  128 KB of operands per
+// tile and step feed 48 MMAs (M = 128, N = 128, K = 16).  The C tile reaches
+// shared memory by TMA one 64-column half at a time through one 64 KB buffer
+// (the second half is prefetched into L2 when the first is loaded).
+//   warp 0        TMA loads of the operand pairs (ring of P_SLOTS)
 //   warp 1        TMEM allocation (512 columns) and tcgen05.mma issue
 //   warp 2        TMA loads of the C halves
 //   warps 4..11   epilogue: per half, group g = 0, 1 owns its columns 32 g..,
@@ -220,12 +228,16 @@ k_tc_update(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 // Every wait is bounded (WAIT_NS); on a timeout a role records an error and
 // stops issuing work.
 // ---------------------------------------------------------------------------
-constexpr int P_STAGES = 3;
+constexpr int P_SLOTS = 5;                            // operand ring: slots of two tiles
+constexpr int P_TILE = BM * BK * 2;                   // one 128-row x 64-bf16 operand tile: 16 KB
+constexpr int P_PAIR = 2 * P_TILE;                    // a slot: two segments of A or of B
 constexpr int P_CH_COLS = 64;                         // columns per C half
 constexpr int P_CH_BYTES = BM * 8 * P_CH_COLS;        // 64 KB of complex FP32
 constexpr int P_TMEM_COLS = 2 * TMEM_COLS;            // two accumulators
 constexpr int P_THREADS = 384;
-constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + P_CH_BYTES + 1024 + 256;
+constexpr int P_SMEM_BYTES = P_SLOTS * P_PAIR + P_CH_BYTES + 1024 + 256;
+static_assert(BN == BM, "A and B operand tiles share one box");
+static_assert(P_SMEM_BYTES <= 232448, "shared memory of one CTA");
 
 __device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x, int y, int z) {
   asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
@@ -234,6 +246,17 @@ __device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x
                : "memory");
 }
 
+// the four K = 16 slices of one product: A tile sa into [Re C | Im C], the real-part
+// columns from B tile sre, the imaginary-part columns from B tile sim (negated when neg)
+__device__ __forceinline__ void mma_prod(uint32_t dacc, uint32_t sa, uint32_t sre, uint32_t sim, uint32_t neg,
+                                         bool first, uint32_t idesc) {
+#pragma unroll
+  for (int k = 0; k < BK / 16; ++k) {
+    const uint32_t acc = (first && k == 0) ? 0u : 1u;
+    mma_bf16_h(dacc, smem_desc(sa + 32 * k), smem_desc(sre + 32 * k), idesc, acc);
+    mma_bf16_h(dacc + BN, smem_desc(sa + 32 * k), smem_desc(sim + 32 * k), idesc | (neg << 14), acc);
+  }
+}
 
 // the tensor maps of up to three operand stagings (the steps of a delayed group) and of C,
 // and each staging's row / column offset for the region's first C row / column
@@ -247,25 +270,26 @@ struct POff {
 
 __global__ void __launch_bounds__(P_THREADS, 1)
 k_tc_persist(const __grid_constant__ PMaps maps, z32 *M, size_t strideM, int N, int crow0, int ccol0, POff off,
-             int nkb1, int Mrows, int Ncols, int Ncap, int nkb, int b0, int count, int nbk, int *err) {
+             int nst, int nbk, int Mrows, int Ncols, int b0, int count, int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gbase = smraw + (sbase - smem_u32(smraw));
-  const uint32_t scbase = sbase + P_STAGES * STAGE_BYTES;           // the two C halves
-  const unsigned char *gc = gbase + P_STAGES * STAGE_BYTES;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + P_STAGES * STAGE_BYTES + P_CH_BYTES);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * P_STAGES + 8);
-  const uint32_t bar_full = smem_u32(bars), bar_empty = bar_full + 8 * P_STAGES;
-  const uint32_t bar_accf = bar_empty + 8 * P_STAGES;   // [2]
+  const uint32_t scbase = sbase + P_SLOTS * P_PAIR;                 // the C half buffer
+  const unsigned char *gc = gbase + P_SLOTS * P_PAIR;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + P_SLOTS * P_PAIR + P_CH_BYTES);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * P_SLOTS + 8);
+  const uint32_t bar_full = smem_u32(bars), bar_empty = bar_full + 8 * P_SLOTS;
+  const uint32_t bar_accf = bar_empty + 8 * P_SLOTS;    // [2]
   const uint32_t bar_acce = bar_accf + 16;              // [2]
   const uint32_t bar_cfull = bar_acce + 16;             // [2]
   const uint32_t bar_cempty = bar_cfull + 16;           // [2]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntn = (Ncols + BN - 1) / BN, ntm = (Mrows + BM - 1) / BM;
   const int ntiles = ntn * ntm * count;
+  const int nunit = nst * nbk;                          // (staging, k-block) units per tile
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < P_STAGES; ++s) {
+    for (int s = 0; s < P_SLOTS; ++s) {
       mbar_init(bar_full + 8 * s, 1);
       mbar_init(bar_empty + 8 * s, 1);
     }
@@ -289,50 +313,64 @@ k_tc_persist(const __grid_constant__ PMaps maps, z32 *M, size_t strideM, int N, 
 
   if (warp == 0) {
     if (lane == 0) {
-      int kbt = 0;
-      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      int pt = 0;     // slot fills so far
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const int tn = tile % ntn, tm = (tile / ntn) % ntm, b = b0 + tile / (ntn * ntm);
-        bool ok = true;
-        for (int kb = 0; kb < nkb; ++kb, ++kbt) {
-          const int s = kbt % P_STAGES;
-          if (kbt >= P_STAGES && !(ok = mbar_wait(bar_empty + 8 * s, ((kbt / P_STAGES) - 1) & 1, err, 11)))
-            break;
-          const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
-          mbar_expect_tx(bar_full + 8 * s, STAGE_BYTES);
-          // k-blocks [i nkb1, (i + 1) nkb1) from staging i
-          const int sti = kb / nkb1, kl = kb - sti * nkb1;
+        for (int u = 0; u < nunit && ok; ++u) {
+          const int sti = u / nbk, kk = u - sti * nbk;
           const CUtensorMap *ma = &maps.a[sti], *mb = &maps.b[sti];
-          const int ar = sti == 0 ? off.ar[0] : sti == 1 ? off.ar[1] : off.ar[2];
-          const int bc = sti == 0 ? off.bc[0] : sti == 1 ? off.bc[1] : off.bc[2];
-          const int xa = kx_a(kl, nbk), xb = kx_b(kl, nbk);
-          tma_load_3d(sa, ma, bar_full + 8 * s, xa, ar + tm * BM, b);
-          tma_load_3d(sb, mb, bar_full + 8 * s, xb, bc + tn * BN, b);
-          tma_load_3d(sb + B_BYTES / 2, mb, bar_full + 8 * s, kx_bi(kl, nbk), bc + tn * BN, b);
+          const int ya = (sti == 0 ? off.ar[0] : sti == 1 ? off.ar[1] : off.ar[2]) + tm * BM;
+          const int yb = (sti == 0 ? off.bc[0] : sti == 1 ? off.bc[1] : off.bc[2]) + tn * BN;
+          // slot q: [B2 B3], [A0 A1], [B0 B1], [A2 A3]; segment s of k-block kk at x = (s nbk + kk) BK
+#pragma unroll 1
+          for (int q = 0; q < 4; ++q, ++pt) {
+            const int s = pt % P_SLOTS;
+            if (pt >= P_SLOTS && !(ok = mbar_wait(bar_empty + 8 * s, ((pt / P_SLOTS) - 1) & 1, err, 11))) break;
+            const uint32_t d = sbase + s * P_PAIR;
+            const bool isa = q & 1;
+            const int seg = (q == 0 || q == 3) ? 2 : 0;
+            const CUtensorMap *m = isa ? ma : mb;
+            const int y = isa ? ya : yb;
+            mbar_expect_tx(bar_full + 8 * s, P_PAIR);
+            tma_load_3d(d, m, bar_full + 8 * s, (seg * nbk + kk) * BK, y, b);
+            tma_load_3d(d + P_TILE, m, bar_full + 8 * s, ((seg + 1) * nbk + kk) * BK, y, b);
+          }
         }
-        if (!ok) break;
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      int kbt = 0, it = 0;
-      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+      int pt = 0, it = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
         const int a = it & 1, use = it >> 1;
-        bool ok = true;
-        if (use > 0) ok = mbar_wait(bar_acce + 8 * a, (use - 1) & 1, err, 12);
-        if (!ok) break;
+        if (use > 0 && !(ok = mbar_wait(bar_acce + 8 * a, (use - 1) & 1, err, 12))) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint32_t dacc = tmem + (uint32_t)(a * TMEM_COLS);
-        for (int kb = 0; kb < nkb; ++kb, ++kbt) {
-          const int s = kbt % P_STAGES;
-          if (!(ok = mbar_wait(bar_full + 8 * s, (kbt / P_STAGES) & 1, err, 13))) break;
+        const uint32_t idesc = Ncols - (tile % ntn) * BN <= 64 ? IDESC_Q : IDESC_H;
+        for (int u = 0; u < nunit; ++u, pt += 4) {
+          const int s0 = pt % P_SLOTS, s1 = (pt + 1) % P_SLOTS, s2 = (pt + 2) % P_SLOTS, s3 = (pt + 3) % P_SLOTS;
+          const uint32_t b23 = sbase + s0 * P_PAIR, a01 = sbase + s1 * P_PAIR;
+          const uint32_t b01 = sbase + s2 * P_PAIR, a23 = sbase + s3 * P_PAIR;
+          if (!(ok = mbar_wait(bar_full + 8 * s0, (pt / P_SLOTS) & 1, err, 13) &&
+                     mbar_wait(bar_full + 8 * s1, ((pt + 1) / P_SLOTS) & 1, err, 13)))
+            break;
           asm volatile("tcgen05.fence::after_thread_sync;");
-          const uint32_t sa = sbase + s * STAGE_BYTES, sb = sa + A_BYTES;
-          const uint32_t neg = neg_bi(kb % nkb1, nbk);
-          const uint32_t idesc = Ncols - (tile % ntn) * BN <= 64 ? IDESC_Q : IDESC_H;
-#pragma unroll
-          for (int k = 0; k < BK / 16; ++k)
-            mma_cplx(dacc, sa + 32 * k, sb + 32 * k, neg, (kb > 0 || k > 0) ? 1u : 0u, idesc);
-          mma_commit(bar_empty + 8 * s);
+          mma_prod(dacc, a01, b23, b23 + P_TILE, 1u, u == 0, idesc);            // j = 2: A0 x (B2, -B3)
+          mma_prod(dacc, a01 + P_TILE, b23 + P_TILE, b23, 0u, false, idesc);    // j = 3: A1 x (B3, B2)
+          mma_commit(bar_empty + 8 * s0);
+          if (!(ok = mbar_wait(bar_full + 8 * s2, ((pt + 2) / P_SLOTS) & 1, err, 13))) break;
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          mma_prod(dacc, a01, b01, b01 + P_TILE, 1u, false, idesc);             // j = 0: A0 x (B0, -B1)
+          mma_prod(dacc, a01 + P_TILE, b01 + P_TILE, b01, 0u, false, idesc);    // j = 1: A1 x (B1, B0)
+          mma_commit(bar_empty + 8 * s1);
+          if (!(ok = mbar_wait(bar_full + 8 * s3, ((pt + 3) / P_SLOTS) & 1, err, 13))) break;
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          mma_prod(dacc, a23, b01, b01 + P_TILE, 1u, false, idesc);             // j = 4: A2 x (B0, -B1)
+          mma_prod(dacc, a23 + P_TILE, b01 + P_TILE, b01, 0u, false, idesc);    // j = 5: A3 x (B1, B0)
+          mma_commit(bar_empty + 8 * s2);
+          mma_commit(bar_empty + 8 * s3);
         }
         if (!ok) break;
         mma_commit(bar_accf + 8 * a);
@@ -898,7 +936,6 @@ cudaError_t persist_region(TcCtx *c, int nst, const int *ar, const int *bc, int 
   const LUBatch &lb = c->lb;
   const long long ntiles = (long long)cdiv_u(Ncols, BN) * cdiv_u(Mrows, BM) * count;
   const int grid = (int)std::min<long long>(ntiles, c->nsm);
-  const int nkb1 = 6 * lb.NB / BK;
   PMaps maps;
   POff off{};
   for (int i = 0; i < P_MAXST; ++i) {
@@ -908,8 +945,8 @@ cudaError_t persist_region(TcCtx *c, int nst, const int *ar, const int *bc, int 
     off.bc[i] = i < nst ? bc[i] : 0;
   }
   maps.c = c->mapC;
-  k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(maps, c->M, lb.strideM, lb.N, crow0, ccol0, off, nkb1, Mrows,
-                                                       Ncols, c->Ncap, nst * nkb1, first, count, lb.NB / BK, c->err);
+  k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(maps, c->M, lb.strideM, lb.N, crow0, ccol0, off, nst,
+                                                       lb.NB / BK, Mrows, Ncols, first, count, c->err);
   return ADGA_LAUNCH_CHECK();
 }
 

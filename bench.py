@@ -34,10 +34,10 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "BSE q·ω pts/s at 1e-8 rel err vs FP64 oracle: mixed-prec vs plain FP64 on B200"
-# DRAM bytes / algorithmic bytes of the k_tc_persist launches of one step pair
-# (two narrow K = 64 regions and one wide K = 128 region) measured with ncu on the
-# 160-point t2g case, 320 matrices
-TRAFFIC_OVER_ALG = 1.27
+# DRAM bytes / algorithmic bytes of the k_tc_persist launches of one group of three
+# steps (two narrow K = 64 regions, two narrow K = 128 regions, one wide K = 192
+# region) measured with ncu on the 160-point t2g case, 320 matrices
+TRAFFIC_OVER_ALG = 1.06
 UNIT = "qw_points/s"
 WORKLOAD = "c1"
 
@@ -628,7 +628,7 @@ def main():
     # Its C read-modify-write makes it HBM-bound, so it is reported against
     # the measured copy bandwidth with algorithmic bytes (C read + write, L21
     # and U12 read once per launch region); `traffic` scales them by the DRAM /
-    # algorithmic ratio ncu measured on the launches of one step pair:
+    # algorithmic ratio ncu measured on the launches of one group of three steps:
     # TRAFFIC_OVER_ALG.
     pk, pk_kind = peaks()
     gflop = sum(s["trail_gflop"] for s in st_mixed)
@@ -638,8 +638,9 @@ def main():
     achieved = gbytes / mst * 1e3 if mst else 0.0          # GB/s
     peak = pk.get("hbm_gbs")
     bf16_tf = 3 * gflop / mst if mst else 0.0
-    roof = {"kernel": "k_tc_persist: tensor-core LU trailing updates of the mixed path (per step pair: the "
-                      "narrow K=64 update, two launches, and the wide K=128 update, one launch; GEMMs only)",
+    roof = {"kernel": "k_tc_persist: tensor-core LU trailing updates of the mixed path (per group of "
+                      "three steps: the narrow K=64 and K=128 updates of the next step's strips, two "
+                      "launches each, and the wide K=192 update, one launch; GEMMs only)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if peak else None,
             "traffic": TRAFFIC_OVER_ALG * gbytes * 1e9 / nlaunch,

@@ -221,9 +221,9 @@ int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
  *   factor  0: complex FP32 LU with BF16x3 tensor-core updates and FP64
  *              refinement; 1: the FP64 LU (no refinement), for sizes where
  *              it is the faster way to the same accuracy
- *   pairs   1: delayed two-step tensor-core updates (K = 128 per C pass);
- *           2: three-step groups (K = 192 per C pass); 0: one update per
- *           step (K = 64)
+ *   pairs   2: tensor-core updates delayed in three-step groups (K = 192
+ *              per C pass); 1: two-step groups (K = 128); 0: one update per
+ *              step (K = 64)
  *   tri_tc  1: the L21 / U12 panel products on the tensor cores, writing the
  *              update operands directly; 0: FP32 CUDA-core tile products and
  *              separate operand-split kernels
@@ -233,7 +233,7 @@ int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
  *   trsv_tc 1: the triangular solves of the FP32 factors on the tensor cores
  *              (3-term TF32 split; N <= 1088, ndim^2 <= 16); 0: streaming
  *              CUDA-core solves
- * A new handle starts at {0, 1, 1, 0, 1, 1} (the environment switches
+ * A new handle starts at {0, 2, 1, 0, 1, 1} (the environment switches
  * ADGA_NO_PAIRS, ADGA_TRI_TILE, ADGA_BATCH, ADGA_RESID_FP64 and
  * ADGA_TRSV_STREAM override it).
  */

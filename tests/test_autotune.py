@@ -24,7 +24,7 @@ def make_ladder(p):
 def test_tune_round_trip_and_validation():
     lad = make_ladder(problem("t3"))
     try:
-        assert lad.tune == {"factor": 0, "pairs": 1, "tri_tc": 1, "batch": 0, "resid": 1, "trsv_tc": 1}
+        assert lad.tune == {"factor": 0, "pairs": 2, "tri_tc": 1, "batch": 0, "resid": 1, "trsv_tc": 1}
         lad.tune = {"pairs": 0, "batch": 3}
         assert lad.tune == {"factor": 0, "pairs": 0, "tri_tc": 1, "batch": 3, "resid": 1, "trsv_tc": 1}
         for bad in ({"factor": 2}, {"pairs": -1}, {"pairs": 3}, {"batch": -5}, {"resid": 2}, {"trsv_tc": 3}):
