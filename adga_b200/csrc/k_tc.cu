@@ -479,11 +479,14 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
 //   * every thread (512 per CTA, two CTAs per SM) loads its 16 values of the
 //     FP32 tile from the matrix (coalesced), splits each into bf16 hi + lo
 //     and writes the K-major, 128 B swizzled A operand;
-//   * the block inverse W becomes the B operand, real-part rows
-//     [Wr | -Wi] and imaginary-part rows [Wi | Wr], hi and lo K blocks;
-//   * one thread issues 24 MMAs (M = 128, N = 128, K = 16): the (hi, hi),
-//     (hi, lo) and (lo, hi) products of the 3-term split into one TMEM
-//     accumulator (columns 0..63 real, 64..127 imaginary parts);
+//   * the block inverse W becomes the B operand once, rows [Wr(:, n)] and
+//     [Wi(:, n)], hi and lo K blocks (mode 0 stages W through shared memory
+//     so that its column-major reads are coalesced);
+//   * one thread issues the (hi, hi), (hi, lo) and (lo, hi) products of the
+//     3-term split into one TMEM accumulator (columns 0..63 real, 64..127
+//     imaginary parts): the real part of the tile times [Wr | Wi] (M = 128,
+//     N = 128, K = 16), then its imaginary part times [-Wi | Wr] as two N = 64
+//     MMAs over B's swapped halves (B negation for the real part);
 //   * the epilogue (thread = row of the tile) writes the FP32 result into the
 //     matrix and the step's operand staging of the trailing update
 //     (k_split_a's layout for L21, k_split_b's for U12), so no split kernel
@@ -506,12 +509,15 @@ static_assert(TT_SROW == TT_FROW, "operand rows and matrix columns are staged wi
 constexpr uint32_t IDESC_N128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 / 8) << 17) |
                                 ((uint32_t)(TT_ROWS / 16) << 24);
 
-__device__ __forceinline__ void mma_bf16_n128(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+// the same with N = 64 (bit 14: negate B)
+constexpr uint32_t IDESC_N64 = (IDESC_N128 & ~(0x3Fu << 17)) | ((uint32_t)(64 / 8) << 17);
+
+__device__ __forceinline__ void mma_bf16_tt(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-      "l"(a), "l"(b), "r"(IDESC_N128), "r"(acc));
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 // byte offset of 16-byte chunk c (0..7) of row r in a 128 B swizzled K block
 __device__ __forceinline__ uint32_t sw128(int r, int c) {
@@ -566,10 +572,10 @@ __device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat1
 
 // Panel products (see the block comment above).  The complex product
 // [Cr | Ci] = Xr [Wr | Wi] + Xi [-Wi | Wr] runs as two MMA phases over the
-// real and the imaginary part of X (64 KB of operands at a time, so two
-// CTAs share an SM and the load, MMA and store phases of different tiles
-// overlap); the epilogue stages all 128 tile rows per round in the same
-// shared memory (67.6 KB).
+// real and the imaginary part of X with one B operand (64 KB of operands at
+// a time, so two CTAs share an SM and the load, MMA and store phases of
+// different tiles overlap); the epilogue stages all 128 tile rows per round
+// in the same shared memory (67.6 KB).
 __global__ void __launch_bounds__(TT_THREADS, 2)
 k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
          const z32 *Uinv, __nv_bfloat16 *Astage, __nv_bfloat16 *Bstage, int Ncap, int b0, int ntA, int ntU,
@@ -605,25 +611,47 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tslot;
 
-  // ---- B operand: rows n (real part of the output) and 64 + n (imaginary part):
-  //      phase 0 [Wr(:, n)], [Wi(:, n)]; phase 1 [-Wi(:, n)], [Wr(:, n)];
-  //      mode 0 W(k, n) = U11^-1(k, n), mode 1 W(k, n) = L11^-1(n, k).  Phase 0's is built
-  //      before the tile is loaded (fewer live registers)
-  auto build_b = [&](int h) {
+  // ---- B operand: rows n = [Wr(:, n)] (real part of the output), rows 64 + n = [Wi(:, n)]
+  //      (imaginary part), hi and lo K blocks; mode 0 W(k, n) = U11^-1(k, n), mode 1
+  //      W(k, n) = L11^-1(n, k).  Phase 1 multiplies by [-Wi | Wr]: the same rows with the
+  //      halves swapped, the real part's negated (two N = 64 MMAs per slice), so B is built once.
+  {
     const int n = t & 63, kq = t >> 6;          // K values kq*8 .. kq*8+7 of column n
-    const int ks = lower ? 1 : NB;               // W(k, n) at W[k * ks + n * (NB + 1 - ks)]
-    const z32 *wp = W + kq * 8 * ks + n * (NB + 1 - ks);
     float wr[8], wi[8];
+    if (lower) {
+      // W(k, n) at W[k + n NB] (NB = 64): staged through the A region (free until the tile's
+      // operand is written) so that the global reads are coalesced; 16-byte chunk c of column n
+      // (W(2c, n), W(2c + 1, n)) at n * 512 + (c ^ (n & 7)) * 16
+      const float4 *w4 = reinterpret_cast<const float4 *>(W);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const z32 w = wp[i * ks];
-      wr[i] = w.x;
-      wi[i] = w.y;
+      for (int i = 0; i < 4; ++i) {
+        const int e = t + TT_THREADS * i, wn = e >> 5, c = e & 31;
+        *reinterpret_cast<float4 *>(gA + wn * 512 + ((c ^ (wn & 7)) << 4)) = w4[e];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float4 v = *reinterpret_cast<const float4 *>(gA + n * 512 + (((4 * kq + j) ^ (n & 7)) << 4));
+        wr[2 * j] = v.x;
+        wi[2 * j] = v.y;
+        wr[2 * j + 1] = v.z;
+        wi[2 * j + 1] = v.w;
+      }
+    } else {
+      // W(k, n) at W[k NB + n]: a warp reads 32 consecutive columns
+      const z32 *wp = W + kq * 8 * NB + n;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const z32 w = wp[i * NB];
+        wr[i] = w.x;
+        wi[i] = w.y;
+      }
     }
-    put8(gB, n, kq, h ? wi : wr, h ? -1.f : 1.f);
-    put8(gB, 64 + n, kq, h ? wr : wi, 1.f);
-  };
-  build_b(0);
+    put8(gB, n, kq, wr, 1.f);
+    put8(gB, 64 + n, kq, wi, 1.f);
+    // the staged W is read before the tile's operand overwrites it
+    if (lower) __syncthreads();
+  }
   asm volatile("" ::: "memory");   // the tile's loads start after it (fewer live registers)
 
   // ---- the tile, 128 rows x 64 K (zero outside the matrix / beyond jb), loaded once with all of
@@ -665,7 +693,9 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
     for (int q = 0; q < 2; ++q) put8(gA, ar, akq * 2 + q, xr + 8 * q, 1.f);
   }
 
-  // one MMA phase: (hi, hi), (hi, lo), (lo, hi) over the operands in shared memory
+  // one MMA phase: (hi, hi), (hi, lo), (lo, hi) over the operands in shared memory; phase 0
+  // [Cr | Ci] = Xr [Wr | Wi] (N = 128), phase 1 [Cr | Ci] += Xi [-Wi | Wr] (two N = 64 MMAs over
+  // B's halves: rows 64.. negated into the real part, rows 0.. into the imaginary part)
   auto mma_phase = [&](int h) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -678,7 +708,12 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
         for (int k = 0; k < 4; ++k) {
           const uint32_t a = sA + (term == 2 ? TT_KBLK : 0) + 32 * k;
           const uint32_t bb = sB + (term == 1 ? TT_KBLK : 0) + 32 * k;
-          mma_bf16_n128(tmem, smem_desc(a), smem_desc(bb), (h > 0 || term > 0 || k > 0) ? 1u : 0u);
+          if (h == 0) {
+            mma_bf16_tt(tmem, smem_desc(a), smem_desc(bb), IDESC_N128, (term > 0 || k > 0) ? 1u : 0u);
+          } else {
+            mma_bf16_tt(tmem, smem_desc(a), smem_desc(bb + 64 * 128), IDESC_N64 | (1u << 14), 1u);
+            mma_bf16_tt(tmem + 64, smem_desc(a), smem_desc(bb), IDESC_N64, 1u);
+          }
         }
       mma_commit(sbar);
     }
@@ -687,10 +722,9 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   // the phase-0 MMAs must have read the operands before they are overwritten
   bool ok = __syncthreads_and(mbar_wait(sbar, 0, err, 21));
   if (ok) {
-    // ---- A operand of phase 1: the imaginary part of the tile; B of phase 1
+    // ---- A operand of phase 1: the imaginary part of the tile (B stays)
 #pragma unroll
     for (int q = 0; q < 2; ++q) put8(gA, ar, akq * 2 + q, xi + 8 * q, 1.f);
-    build_b(1);
     mma_phase(1);
   }
   // CTA-uniform: the epilogue below has block barriers
