@@ -611,6 +611,30 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tslot;
 
+  // ---- the tile's lines into L2 while B is built (one 128 B line per thread, plus the line
+  //      holding the last byte of each column piece, whose start is not line-aligned)
+  {
+    const z32 *piece = nullptr;
+    int l = 0, nl = 0;
+    if (lower) {                                   // column J + (t >> 3): rows J + jb + m0.., 1 KB
+      const int k = t >> 3;
+      l = t & 7;
+      nl = 8;
+      if (k < jb) piece = Am + (size_t)(J + k) * N + (J + jb + m0);
+    } else {                                       // column J + jb + m0 + (t >> 2): rows J.., 512 B
+      const int cc = t >> 2;
+      l = t & 3;
+      nl = 4;
+      if (cc < nv) piece = Am + (size_t)(J + jb + m0 + cc) * N + J;
+    }
+    const int bytes = (lower ? nv : jb) * 8;       // valid bytes of the piece
+    if (piece && l * 128 < bytes) {
+      const char *pc = reinterpret_cast<const char *>(piece);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(pc + l * 128));
+      if (l == nl - 1) asm volatile("prefetch.global.L2 [%0];" ::"l"(pc + bytes - 1));
+    }
+  }
+
   // ---- B operand: rows n = [Wr(:, n)] (real part of the output), rows 64 + n = [Wi(:, n)]
   //      (imaginary part), hi and lo K blocks; mode 0 W(k, n) = U11^-1(k, n), mode 1
   //      W(k, n) = L11^-1(n, k).  Phase 1 multiplies by [-Wi | Wr]: the same rows with the
