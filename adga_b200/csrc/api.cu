@@ -672,7 +672,7 @@ static size_t bytes_per_point(const adga_handle *h, int prec, int NB) {
     b += 2 * N * (N + R) * 8 + 2 * 2 * nsteps * NB * NB * 8;
     b += 2 * 2 * R * N * 16 + 2 * R * N * 8 + 2 * ((R + 15) / 16) * 16 * N * 8 + 2 * N * 4 + 64;
     b += 2 * 7 * R * ((2 * N + 63) / 64 * 64) + 2 * R * 4;   // int8 residual slices and scales
-    b += 2 * 3 * (N + N + R) * 4 * NB * 2;                     // three tensor-core operand stagings
+    b += 2 * 4 * (N + N + R) * 4 * NB * 2;                     // four tensor-core operand stagings
   }
   return b;
 }
@@ -1501,10 +1501,10 @@ extern "C" int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int prec
 // ---------------------------------------------------------------------------
 extern "C" int adga_set_tune(adga_handle *h, const adga_tune *t) {
   if (!h || !t) return ADGA_EINVAL;
-  if (t->factor < 0 || t->factor > 1 || t->pairs < 0 || t->pairs > 2 || t->tri_tc < 0 || t->tri_tc > 1 ||
+  if (t->factor < 0 || t->factor > 1 || t->pairs < 0 || t->pairs > 3 || t->tri_tc < 0 || t->tri_tc > 1 ||
       t->batch < 0 || t->resid < 0 || t->resid > 1 || t->trsv_tc < 0 || t->trsv_tc > 1)
     return fail(h, ADGA_EINVAL,
-                "adga_set_tune: factor, tri_tc, resid, trsv_tc in {0, 1}, pairs in {0, 1, 2}, batch >= 0");
+                "adga_set_tune: factor, tri_tc, resid, trsv_tc in {0, 1}, pairs in {0, 1, 2, 3}, batch >= 0");
   h->tune = *t;
   return 0;
 }
@@ -1564,6 +1564,7 @@ extern "C" int adga_autotune(adga_handle *h, int qwstart, int qwstop, double tol
   if (tc) {
     if (c.N % 2 == 0) {
       cand.push_back(with(0, 2, 1, 1, 1));
+      cand.push_back(with(0, 3, 1, 1, 1));
       cand.push_back(with(0, 1, 1, 1, 1));
       cand.push_back(with(0, 2, 1, 1, 0));
       cand.push_back(with(0, 2, 1, 0, 1));

@@ -1152,13 +1152,13 @@ static void trail_account(TrailTiming *tt, double m, double n, double k, int bat
   tt->gbytes += (2.0 * sizeof(z32) * m * n + sizeof(z32) * k * (m + n)) * batch * 1e-9;
 }
 
-// Unpivoted FP32 factorisation with delayed updates in groups of G = 2 or 3 steps: after
+// Unpivoted FP32 factorisation with delayed updates in groups of G = 2..4 steps: after
 // step g < G - 1 of a group only the parts of the group's updates that step g + 1 reads
 // (narrow), after its last step all G steps' updates of the rest at once (wide)
 cudaError_t lu_factor_groups(z32 *M, const LUBatch &lb, const GroupOps &ops, cudaStream_t st, TrailTiming *tt) {
-  if (ops.G < 2 || ops.G > 3) return cudaErrorInvalidValue;
+  if (ops.G < 2 || ops.G > 4) return cudaErrorInvalidValue;
   const int nsteps = lb.nsteps();
-  int Js[3], jbs[3];
+  int Js[4], jbs[4];
   for (int s = 0; s < nsteps; ++s) {
     const int J = s * lb.NB, jb = min(lb.NB, lb.N - J), g = s % ops.G;
     Js[g] = J;

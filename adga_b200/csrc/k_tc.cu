@@ -258,9 +258,9 @@ __device__ __forceinline__ void mma_prod(uint32_t dacc, uint32_t sa, uint32_t sr
   }
 }
 
-// the tensor maps of up to three operand stagings (the steps of a delayed group) and of C,
+// the tensor maps of up to four operand stagings (the steps of a delayed group) and of C,
 // and each staging's row / column offset for the region's first C row / column
-constexpr int P_MAXST = 3;
+constexpr int P_MAXST = 4;
 struct alignas(64) PMaps {
   CUtensorMap a[P_MAXST], b[P_MAXST], c;
 };
@@ -320,8 +320,8 @@ k_tc_persist(const __grid_constant__ PMaps maps, z32 *M, size_t strideM, int N, 
         for (int u = 0; u < nunit && ok; ++u) {
           const int sti = u / nbk, kk = u - sti * nbk;
           const CUtensorMap *ma = &maps.a[sti], *mb = &maps.b[sti];
-          const int ya = (sti == 0 ? off.ar[0] : sti == 1 ? off.ar[1] : off.ar[2]) + tm * BM;
-          const int yb = (sti == 0 ? off.bc[0] : sti == 1 ? off.bc[1] : off.bc[2]) + tn * BN;
+          const int ya = (sti == 0 ? off.ar[0] : sti == 1 ? off.ar[1] : sti == 2 ? off.ar[2] : off.ar[3]) + tm * BM;
+          const int yb = (sti == 0 ? off.bc[0] : sti == 1 ? off.bc[1] : sti == 2 ? off.bc[2] : off.bc[3]) + tn * BN;
           // slot q: [B2 B3], [A0 A1], [B0 B1], [A2 A3]; segment s of k-block kk at x = (s nbk + kk) BK
 #pragma unroll 1
           for (int q = 0; q < 4; ++q, ++pt) {
@@ -900,7 +900,7 @@ struct TcCtx {
   z32 *M;
   LUBatch lb;
   // operand stagings: set 0 for step-by-step updates, sets 0..G-1 for the steps of a delayed group
-  __nv_bfloat16 *A[P_MAXST] = {nullptr, nullptr, nullptr}, *B[P_MAXST] = {nullptr, nullptr, nullptr};
+  __nv_bfloat16 *A[P_MAXST] = {}, *B[P_MAXST] = {};
   int *err = nullptr;
   int Ncap = 0;
   int nsm = 0;
@@ -1051,7 +1051,7 @@ cudaError_t tc_trail_run_range(void *ctxp, int first, int count, int J, int jb, 
 }
 
 // ---------------------------------------------------------------------------
-// Delayed updates of the unpivoted path in groups of G steps (G = 2 or 3): after step
+// Delayed updates of the unpivoted path in groups of G steps (G = 2..4): after step
 // g of a group (steps J_i, widths jb_i, i <= g, staged in sets i):
 //   g < G - 1   the group's updates so far restricted to what step g + 1 reads: its
 //               columns below it and its rows right of it (K = (g + 1) * 6 NB);

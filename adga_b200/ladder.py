@@ -219,8 +219,8 @@ class Ladder:
     def tune(self) -> Dict[str, int]:
         """The mixed path's kernel choices (adga_get_tune): factor (0: FP32 LU
         + FP64 refinement, 1: FP64 LU), pairs (0: one tensor-core update per
-        step, 1: delayed pairs, 2: groups of three), tri_tc, batch, resid,
-        trsv_tc."""
+        step, 1: delayed pairs, 2: groups of three, 3: groups of four), tri_tc,
+        batch, resid, trsv_tc."""
         t = Tune()
         self._check(self._lib.adga_get_tune(self._h, C.byref(t)), "get_tune")
         return t.as_dict()

@@ -222,8 +222,8 @@ int adga_ladder_run(adga_handle *h, int qwstart, int qwstop, int precision,
  *              refinement; 1: the FP64 LU (no refinement), for sizes where
  *              it is the faster way to the same accuracy
  *   pairs   2: tensor-core updates delayed in three-step groups (K = 192
- *              per C pass); 1: two-step groups (K = 128); 0: one update per
- *              step (K = 64)
+ *              per C pass); 3: four-step groups (K = 256); 1: two-step
+ *              groups (K = 128); 0: one update per step (K = 64)
  *   tri_tc  1: the L21 / U12 panel products on the tensor cores, writing the
  *              update operands directly; 0: FP32 CUDA-core tile products and
  *              separate operand-split kernels

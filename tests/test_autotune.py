@@ -27,7 +27,7 @@ def test_tune_round_trip_and_validation():
         assert lad.tune == {"factor": 0, "pairs": 2, "tri_tc": 1, "batch": 0, "resid": 1, "trsv_tc": 1}
         lad.tune = {"pairs": 0, "batch": 3}
         assert lad.tune == {"factor": 0, "pairs": 0, "tri_tc": 1, "batch": 3, "resid": 1, "trsv_tc": 1}
-        for bad in ({"factor": 2}, {"pairs": -1}, {"pairs": 3}, {"batch": -5}, {"resid": 2}, {"trsv_tc": 3}):
+        for bad in ({"factor": 2}, {"pairs": -1}, {"pairs": 4}, {"batch": -5}, {"resid": 2}, {"trsv_tc": 3}):
             with pytest.raises(AdgaError):
                 lad.tune = bad
         assert lad.tune["batch"] == 3
@@ -43,9 +43,9 @@ def test_autotune_picks_the_fastest_accurate_configuration(name):
     try:
         q0 = s.iwb * s.nqp + 1                      # the omega = 0 slice as the sample
         best, trials = lad.autotune(q0, q0 + s.nqp - 1)
-        # the tensor-core variants (panel products, pairs or groups of three, int8 or FP64
+        # the tensor-core variants (panel products, groups of two, three or four, int8 or FP64
         # residual, tensor-core or streaming solves) + the FP64 factorisation
-        assert len(trials) == 7
+        assert len(trials) == 8
         assert all(t["accepted"] and t["err"] <= 1e-8 for t in trials), trials
         fastest = min(trials, key=lambda t: t["ms"])
         assert best == {k: fastest[k] for k in ("factor", "pairs", "tri_tc", "batch", "resid", "trsv_tc")}

@@ -89,12 +89,15 @@ def test_refinement_residual_matches_oracle(name, resid):
         assert rel_err(got[k], want[k]) < 1e-8, (k, rel_err(got[k], want[k]))
 
 
+@pytest.mark.parametrize("pairs", [2, 3])
 @pytest.mark.parametrize("name", ["t3b", "t3m", "c3s"])
-def test_groups_of_three_match_oracle(name):
-    """tune pairs = 2: the tensor-core updates delayed in groups of three steps
-    (the next step's strips after each step, the rest with a K = 3 * 6 NB product
-    from three operand stagings); N = 144 (one group ending at the last step),
-    216 (a group and a lone step), 320 (a group and a pair)."""
+def test_delayed_groups_match_oracle(name, pairs):
+    """tune pairs = 2 / 3: the tensor-core updates delayed in groups of three /
+    four steps (the next step's strips after each step, the rest with a K = G * 6
+    NB product from G operand stagings).  Groups of three: N = 144 (one group
+    ending at the last step), 216 (a group and a lone step), 320 (a group and a
+    pair); groups of four: 144 (a partial group), 216 (one group ending at the
+    last step), 320 (a group and a lone step)."""
     p = problem(name)
     s = p.spec
     with library_env({}):
@@ -102,7 +105,7 @@ def test_groups_of_three_match_oracle(name):
     try:
         for iwb in range(-s.iwb, s.iwb + 1):
             lad.set_vertex(iwb, *p.vertex(iwb))
-        lad.tune = {"pairs": 2}
+        lad.tune = {"pairs": pairs}
         status, stats = lad.ladder_run(1, None, "mixed")
         got = lad.get_outputs()
         got.update(lad.assemble(got, p.siw))
