@@ -497,13 +497,18 @@ constexpr int DN_LD = 65;
 
 // Diagonal block of an unpivoted step with its inverses, one CTA per matrix
 // (FP32): the jb x jb block is padded with the identity to 64 x 64 and
-// factored right-looking in 4 x 4 register blocks (16 block steps, two
-// barriers each, packed two-lane FMAs in the trailing blocks);
-// L11^-1 (strictly lower; unit diagonal implied) and U11^-1 (upper with the
-// diagonal) then share one array and follow in 16 x 16 blocks: eight warps
-// invert the diagonal blocks of both triangles (lane = column, no barriers),
-// and three block rounds fill L^-1 downwards and U^-1 upwards, each a pair of
-// small block products per triangle.  73 KB of shared memory: three CTAs per SM.
+// factored right-looking in 4 x 4 register blocks, loaded straight from the
+// matrix (16 block steps, two barriers each, packed two-lane FMAs in the
+// trailing blocks; the next step's diagonal block is factored by its owner
+// right after its own trailing update, so that factorisation overlaps the
+// other blocks' updates).  L11^-1 (strictly lower; unit diagonal implied) and
+// U11^-1 (upper with the diagonal) then share one array: eight warps invert
+// the 16 x 16 diagonal blocks of both triangles (lane = column, no barriers),
+// and two levels of recursive doubling join them,
+//   [X00 0; X10 X11] with X10 = -X11 (L10 X00)   (and the transposed form for U),
+// 16 x 16 blocks, then 32 x 32 blocks, the products L10 X00 formed in place of
+// L10 (the factored block goes to the matrix before the inversion).  73 KB of
+// shared memory: three CTAs per SM.
 constexpr int DI_SCR = 3 * 256;
 
 __device__ __forceinline__ void cfma2(z32 &acc, z32 a, z32 u) {
@@ -511,64 +516,71 @@ __device__ __forceinline__ void cfma2(z32 &acc, z32 a, z32 u) {
   acc = __ffma2_rn(make_float2(-a.y, a.y), make_float2(u.y, u.x), acc);
 }
 __device__ __forceinline__ void cfma2(z64 &acc, z64 a, z64 u) { cfma(acc, a, u); }
+// 1 / z for the FP32 block LU: z = s (a + i b) with s = max(|Re z|, |Im z|), so that
+// a^2 + b^2 lies in [1, 2]; two correctly rounded reciprocals (a zero pivot gives
+// non-finite factors, which the refinement reports)
+__device__ __forceinline__ z32 crcp_lu(z32 z) {
+  const float is = __frcp_rn(fmaxf(fabsf(z.x), fabsf(z.y)));
+  const float a = z.x * is, b = z.y * is;
+  const float f = __frcp_rn(fmaf(a, a, b * b)) * is;
+  return make_float2(a * f, -b * f);
+}
 
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Linv, T *Uinv, int *ipiv_all,
            int *rmap_all) {
+  static_assert(sizeof(T) == sizeof(z32), "the blocked LU is the FP32 path's");
   extern __shared__ __align__(16) unsigned char smraw[];
   T *D = reinterpret_cast<T *>(smraw);          // [64][DN_LD] factored block
   T *X = D + 64 * DN_LD;                        // L11^-1 below the diagonal, U11^-1 on and above it
-  T *S = X + 64 * DN_LD;                        // block-product scratch (3 blocks)
+  T *S = X + 64 * DN_LD;                        // the LU's panel exchange
   __shared__ T rcps[64];
   const int b = blockIdx.x, t = threadIdx.x;
   T *A = M + (size_t)b * strideM;
   const T one = cx<T>::make(1, 0), zero = czero<T>();
-  // entries of the two inverses: L^-1 with its unit diagonal and zeros above, U^-1 with zeros below
-  auto lval = [&](int r, int c) { return r > c ? X[r + c * DN_LD] : (r == c ? one : zero); };
-  auto uval = [&](int r, int c) { return r <= c ? X[r + c * DN_LD] : zero; };
-  for (int e = t; e < 64 * 64; e += 256) {
-    const int i = e & 63, j = e >> 6;
-    D[i + j * DN_LD] = (i < jb && j < jb) ? A[(size_t)(J + i) + (size_t)(J + j) * N] : (i == j ? one : zero);
-  }
-  __syncthreads();
+  const int bi = t >> 4, bj = t & 15;
+  T a[4][4];
   {
-    // Right-looking LU in 4 x 4 blocks held in registers: thread (bi, bj) owns
-    // D[4bi.., 4bj..].  Per block step kb: the diagonal thread factors its block
-    // (unit L, U, the reciprocals of U's diagonal), the column panel solves
-    // L[bi,kb] U_kk = A[bi,kb], the row panel L_kk U[kb,bj] = A[kb,bj], and the
-    // trailing blocks take A -= L[bi,kb] U[kb,bj] as four rank-1 updates; two
-    // barriers per block step.  Panels are exchanged through S (stride 17 per
+    // thread (bi, bj) owns D[4bi.., 4bj..]: four 32-byte column pieces, all loads in flight
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = 4 * bi + r, j = 4 * bj + c;
+        a[r][c] = (i < jb && j < jb) ? A[(size_t)(J + i) + (size_t)(J + j) * N] : (i == j ? one : zero);
+      }
+  }
+  {
+    // Right-looking LU in 4 x 4 blocks.  Per block step kb: the owner of the diagonal block
+    // has factored it (unit L, U, the reciprocals of U's diagonal) into xD; the column panel
+    // solves L[bi,kb] U_kk = A[bi,kb], the row panel L_kk U[kb,bj] = A[kb,bj]; the trailing
+    // blocks take A -= L[bi,kb] U[kb,bj] as four rank-1 updates, and the owner of block
+    // (kb + 1, kb + 1) then factors it.  Panels are exchanged through S (stride 17 per
     // block, conflict-free for the 16 column owners of a warp).
-    static_assert(sizeof(T) == sizeof(z32), "the blocked LU is the FP32 path's");
-    const int bi = t >> 4, bj = t & 15;
     T *xL = S, *xU = S + 16 * 17, *xD = S + 2 * 16 * 17;   // xD: the factored diagonal block + 1/u
-    T a[4][4];
+    auto factor_diag = [&](int kb) {
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+      for (int k = 0; k < 4; ++k) {
+        const T rp = crcp_lu(a[k][k]);
+        xD[16 + k] = rp;
+        rcps[4 * kb + k] = rp;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) a[r][c] = D[(4 * bi + r) + (4 * bj + c) * DN_LD];
+        for (int i = k + 1; i < 4; ++i) a[i][k] = cmul(a[i][k], rp);
+#pragma unroll
+        for (int i = k + 1; i < 4; ++i)
+#pragma unroll
+          for (int j = k + 1; j < 4; ++j) a[i][j] = csub(a[i][j], cmul(a[i][k], a[k][j]));
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) xD[r + 4 * c] = a[r][c];
+    };
+    if (t == 0) factor_diag(0);
+    __syncthreads();
 #pragma unroll 1
     for (int kb = 0; kb < 16; ++kb) {
-      if (bi == kb && bj == kb) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const T rp = crcp(a[k][k]);
-          xD[16 + k] = rp;
-          rcps[4 * kb + k] = rp;
-#pragma unroll
-          for (int i = k + 1; i < 4; ++i) a[i][k] = cmul(a[i][k], rp);
-#pragma unroll
-          for (int i = k + 1; i < 4; ++i)
-#pragma unroll
-            for (int j = k + 1; j < 4; ++j) a[i][j] = csub(a[i][j], cmul(a[i][k], a[k][j]));
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) xD[r + 4 * c] = a[r][c];
-      }
-      __syncthreads();
       if (bj == kb && bi > kb) {
         // L[bi,kb] = A[bi,kb] U_kk^-1, column by column
 #pragma unroll
@@ -617,16 +629,28 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
             }
           }
         }
+        // xD is free once the panels are solved: the next diagonal block is factored now
+        if (bi == kb + 1 && bj == kb + 1) factor_diag(kb + 1);
       }
+      __syncthreads();
     }
-    // the packed factors (multipliers below the diagonal, U on and above it) back into D
+    // the packed factors (multipliers below the diagonal, U on and above it) into D and the matrix
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) D[(4 * bi + r) + (4 * bj + c) * DN_LD] = a[r][c];
+      for (int r = 0; r < 4; ++r) {
+        const int i = 4 * bi + r, j = 4 * bj + c;
+        D[i + j * DN_LD] = a[r][c];
+        if (i < jb && j < jb) A[(size_t)(J + i) + (size_t)(J + j) * N] = a[r][c];
+      }
   }
   __syncthreads();
+  // entries of the two inverses: L^-1 with its unit diagonal and zeros above, U^-1 with zeros below
+  auto xl = [&](int r, int c) { return r > c ? X[r + c * DN_LD] : (r == c ? one : zero); };
+  auto xu = [&](int r, int c) { return r <= c ? X[r + c * DN_LD] : zero; };
   {
+    // the 16 x 16 diagonal blocks of both inverses: warp w < 4 column l of L block w, warp w >= 4
+    // column l of U block w - 4, by substitution
     const int w = t >> 5, lane = t & 31;
     if (lane < 16) {
       const int o = 16 * (w & 3), l = lane;
@@ -666,53 +690,117 @@ k_diag_inv(T *M, size_t strideM, int N, int J, int jb, int NB, int nsteps, T *Li
     }
   }
   __syncthreads();
-  for (int st = 1; st < 4; ++st) {
-    const int bl = st, bu = 3 - st;               // block row of L^-1 / U^-1 filled in this round
-    // L: S_bj = sum_{bk=bj}^{bl-1} L(bl,bk) L^-1(bk,bj), then L^-1(bl,bj) = -L^-1(bl,bl) S_bj
-    for (int e = t; e < 256 * st; e += 256) {
-      const int bj = e >> 8, r = e & 15, c = (e >> 4) & 15;
-      T s = zero;
-      for (int m = 16 * bj; m < 16 * bl; ++m) cfma(s, D[(16 * bl + r) + m * DN_LD], lval(m, 16 * bj + c));
-      S[bj * 256 + r + 16 * c] = s;
+  {
+    // 16 -> 32: for the 32-blocks at o = 0, 32 of both triangles
+    //   L: X10 = -X11 (L10 X00),   U: Y01 = -Y00 (U01 Y11),
+    // warp w: product (w >> 1): L at o = 0, 32, then U at o = 0, 32; columns 8 (w & 1).. + 7;
+    // lane: row i = lane & 15, columns 4 (lane >> 4) + q
+    const int w = t >> 5, lane = t & 31;
+    const bool up = w >= 4;
+    const int o = 32 * ((w >> 1) & 1), i = lane & 15, j0 = 8 * (w & 1) + 4 * (lane >> 4);
+    T v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = zero;
+    if (!up) {
+#pragma unroll 4
+      for (int k = 0; k < 16; ++k) {
+        const T d = D[(o + 16 + i) + (o + k) * DN_LD];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cfma2(v[q], d, xl(o + k, o + j0 + q));
+      }
+    } else {
+#pragma unroll 4
+      for (int k = 0; k < 16; ++k) {
+        const T d = D[(o + i) + (o + 16 + k) * DN_LD];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cfma2(v[q], d, xu(o + 16 + k, o + 16 + j0 + q));
+      }
+    }
+    __syncthreads();     // every product has read its block of D: the products replace them
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (!up) D[(o + 16 + i) + (o + j0 + q) * DN_LD] = v[q];
+      else D[(o + i) + (o + 16 + j0 + q) * DN_LD] = v[q];
+      v[q] = zero;
     }
     __syncthreads();
-    for (int e = t; e < 256 * st; e += 256) {
-      const int bj = e >> 8, r = e & 15, c = (e >> 4) & 15;
-      T s = zero;
-      for (int m = 0; m < 16; ++m) cfma(s, lval(16 * bl + r, 16 * bl + m), S[bj * 256 + m + 16 * c]);
-      X[(16 * bl + r) + (16 * bj + c) * DN_LD] = cneg(s);
+    if (!up) {
+#pragma unroll 4
+      for (int k = 0; k < 16; ++k) {
+        const T x = xl(o + 16 + i, o + 16 + k);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cfma2(v[q], x, D[(o + 16 + k) + (o + j0 + q) * DN_LD]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) X[(o + 16 + i) + (o + j0 + q) * DN_LD] = cneg(v[q]);
+    } else {
+#pragma unroll 4
+      for (int k = 0; k < 16; ++k) {
+        const T x = xu(o + i, o + k);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cfma2(v[q], x, D[(o + k) + (o + 16 + j0 + q) * DN_LD]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) X[(o + i) + (o + 16 + j0 + q) * DN_LD] = cneg(v[q]);
     }
-    __syncthreads();
-    // U: S_bj = sum_{bk=bu+1}^{bj} U(bu,bk) U^-1(bk,bj), then U^-1(bu,bj) = -U^-1(bu,bu) S_bj
-    for (int e = t; e < 256 * st; e += 256) {
-      const int bj = bu + 1 + (e >> 8), r = e & 15, c = (e >> 4) & 15;
-      T s = zero;
-      for (int m = 16 * (bu + 1); m < 16 * (bj + 1); ++m) cfma(s, D[(16 * bu + r) + m * DN_LD], uval(m, 16 * bj + c));
-      S[(e >> 8) * 256 + r + 16 * c] = s;
-    }
-    __syncthreads();
-    for (int e = t; e < 256 * st; e += 256) {
-      const int bj = bu + 1 + (e >> 8), r = e & 15, c = (e >> 4) & 15;
-      T s = zero;
-      for (int m = 0; m < 16; ++m) cfma(s, uval(16 * bu + r, 16 * bu + m), S[(e >> 8) * 256 + m + 16 * c]);
-      X[(16 * bu + r) + (16 * bj + c) * DN_LD] = cneg(s);
-    }
-    __syncthreads();
   }
+  __syncthreads();
+  {
+    // 32 -> 64: L: X10 = -X11 (L10 X00), U: Y01 = -Y00 (U01 Y11) with 32 x 32 blocks;
+    // warp w: columns 4w + q of both products, lane: row i
+    const int w = t >> 5, i = t & 31, j0 = 4 * w;
+    T vl[4], vu[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) vl[q] = vu[q] = zero;
+    // L10 X00: X00(k, j) = 0 for k < j
+#pragma unroll 4
+    for (int k = j0; k < 32; ++k) {
+      const T d = D[(32 + i) + k * DN_LD];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) cfma2(vl[q], d, xl(k, j0 + q));
+    }
+    // U01 Y11: Y11(k, j) = 0 for k > j
+#pragma unroll 4
+    for (int k = 0; k < j0 + 4; ++k) {
+      const T d = D[i + (32 + k) * DN_LD];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) cfma2(vu[q], d, xu(32 + k, 32 + j0 + q));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      D[(32 + i) + (j0 + q) * DN_LD] = vl[q];
+      D[i + (32 + j0 + q) * DN_LD] = vu[q];
+      vl[q] = vu[q] = zero;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      const T xa = xl(32 + i, 32 + k), xb = xu(i, k);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        cfma2(vl[q], xa, D[(32 + k) + (j0 + q) * DN_LD]);
+        cfma2(vu[q], xb, D[k + (32 + j0 + q) * DN_LD]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      X[(32 + i) + (j0 + q) * DN_LD] = cneg(vl[q]);
+      X[i + (32 + j0 + q) * DN_LD] = cneg(vu[q]);
+    }
+  }
+  __syncthreads();
   const size_t off = ((size_t)b * nsteps + J / NB) * NB * NB;
+#pragma unroll 4
   for (int e = t; e < NB * NB; e += 256) {
     const int i = e % NB, k = e / NB;
     T lv = zero, uv = zero;
     if (i < jb && k < jb) {
-      lv = lval(i, k);
-      uv = uval(i, k);
+      lv = xl(i, k);
+      uv = xu(i, k);
     }
     Linv[off + e] = lv;
     Uinv[off + e] = uv;
-  }
-  for (int e = t; e < jb * jb; e += 256) {
-    const int i = e % jb, j = e / jb;
-    A[(size_t)(J + i) + (size_t)(J + j) * N] = D[i + j * DN_LD];
   }
   int *ip = ipiv_all + (size_t)b * N + J;
   for (int i = t; i < jb; i += 256) ip[i] = J + i;
