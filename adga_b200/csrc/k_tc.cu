@@ -498,13 +498,11 @@ constexpr int TT_THREADS = 512;
 constexpr int TT_ROWS = 128;                       // tile rows (MMA M)
 constexpr int TT_KBLK = TT_ROWS * 128;             // one K block: 128 rows x 64 bf16
 constexpr int TT_OPER = 4 * TT_KBLK;               // A hi, A lo, B hi, B lo of one K half: 64 KB
-constexpr int TT_SROW = 528;                       // padded stride of a staged 512 B operand row
-constexpr int TT_FROW = 528;                       // padded stride of a staged 512 B matrix column
-constexpr int TT_STAGE = TT_ROWS * TT_SROW;         // epilogue staging: all 128 rows (67.6 KB)
-constexpr int TT_REGION = TT_STAGE > TT_OPER ? TT_STAGE : TT_OPER;
+constexpr int TT_BOX = TT_ROWS * 128;              // one 128 B swizzled store box: 128 rows x 128 B
+constexpr int TT_REGION = TT_OPER;                 // operands, then the epilogue's four store boxes
 constexpr int TT_SMEM_BYTES = TT_REGION + 1024 + 64;
+static_assert(4 * TT_BOX == TT_OPER, "the epilogue's boxes reuse the operand region");
 constexpr int TT_TMEM_COLS = 128;
-static_assert(TT_SROW == TT_FROW, "operand rows and matrix columns are staged with one stride");
 // kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
 constexpr uint32_t IDESC_N128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 / 8) << 17) |
                                 ((uint32_t)(TT_ROWS / 16) << 24);
@@ -559,16 +557,12 @@ __device__ __forceinline__ uint4 pack8(const float *re, const float *im, int par
   }
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
-// nrow operand rows of 512 B (four segments of 64 bf16), staged with stride TT_SROW, to nrow
-// contiguous global rows
-__device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat16 *dst, int nrow, int t) {
-  unsigned char *d = reinterpret_cast<unsigned char *>(dst);
-  for (int e = t; e < nrow * 32; e += TT_THREADS) {
-    const int r = e / 32, c = e % 32;
-    *reinterpret_cast<uint4 *>(d + (size_t)r * 512 + c * 16) =
-        *reinterpret_cast<const uint4 *>(stg + r * TT_SROW + c * 16);
-  }
-}
+
+// the step's operand stagings (L21 rows: A, U12 columns: B) and U12 as FP32 columns, all with
+// 128 B swizzled boxes of 128 rows x 128 B: the epilogue's TMA stores
+struct alignas(64) TriMaps {
+  CUtensorMap stA, stB, u;
+};
 
 // Panel products (see the block comment above).  The complex product
 // [Cr | Ci] = Xr [Wr | Wi] + Xi [-Wi | Wr] runs as two MMA phases over the
@@ -577,9 +571,8 @@ __device__ __forceinline__ void copy_rows(const unsigned char *stg, __nv_bfloat1
 // different tiles overlap); the epilogue stages all 128 tile rows per round
 // in the same shared memory (67.6 KB).
 __global__ void __launch_bounds__(TT_THREADS, 2)
-k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int nsteps, const z32 *Linv,
-         const z32 *Uinv, __nv_bfloat16 *Astage, __nv_bfloat16 *Bstage, int Ncap, int b0, int ntA, int ntU,
-         int *err) {
+k_tc_tri(const __grid_constant__ TriMaps maps, z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB,
+         int nsteps, const z32 *Linv, const z32 *Uinv, int b0, int ntA, int ntU, int *err) {
   extern __shared__ unsigned char smraw[];
   const uint32_t sbase = (smem_u32(smraw) + 1023u) & ~1023u;
   unsigned char *gA = smraw + (sbase - smem_u32(smraw));    // A hi, A lo, B hi, B lo
@@ -756,84 +749,84 @@ k_tc_tri(z32 *M, size_t strideM, int N, int ncols, int J, int jb, int NB, int ns
   asm volatile("tcgen05.fence::after_thread_sync;");
 
   // ---- epilogue: warp w reads TMEM lanes 32 (w % 4).. (tile rows) and output columns
-  //      16 (w / 4) .. + 15; the results reach global memory through shared memory (the
-  //      operand buffers, free once the MMAs completed), so that every store is coalesced
+  //      16 (w / 4) .. + 15.  Results reach global memory by TMA stores of four 128 B swizzled
+  //      boxes (128 rows x 128 B each) written into the operand region, free once the MMAs
+  //      completed: 16-byte piece p of row r of box q at q * 16 KB + r * 128 + (p ^ (r & 7)) * 16
+  //      (conflict-free for eight consecutive rows).  Rows and columns outside the matrix or the
+  //      staging are clipped by the tensor maps; rows of the tile beyond the panel are zero.
   if (ok) {
     const int quad = warp & 3, grp = warp >> 2;
     const int r = quad * 32 + lane;
     const int n0 = grp * 16;
-    unsigned char *stg = gA;
+    unsigned char *box = gA;
     const uint32_t tl = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)n0;
-    // the thread's 32 output values of part `piece` (16 columns each), re then im
-    auto tload = [&](int piece, float (&re)[16], float (&im)[16]) {
-      tmem_ld16(tl + 16 * piece, re);
-      tmem_ld16(tl + 64 + 16 * piece, im);
+    auto sw = [&](int q, int p) { return q * TT_BOX + r * 128 + ((p ^ (r & 7)) << 4); };
+    // the thread's 32 output values (16 columns), re then im
+    auto tload = [&](float (&re)[16], float (&im)[16]) {
+      tmem_ld16(tl, re);
+      tmem_ld16(tl + 64, im);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
     };
-    if (lower) {
-      unsigned char *row = stg + r * TT_SROW + n0 * 2;
-      {
-        float re[16], im[16];
-        tload(0, re, im);
-        // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
-        if (r < nv) {
-          z32 *dst = Am + (size_t)(J + jb + m0 + r);
+    // the four staging segments (pieces n0 / 8 and n0 / 8 + 1 of each 128 B row are this
+    // thread's); negb: B's real-part rows [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo], else A's rows
+    // [Lr_hi, Li_hi, Lr_lo, Li_lo]
+    auto put_stage = [&](const float (&re)[16], const float (&im)[16], bool negb) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (n0 + j < jb) dst[(size_t)(J + n0 + j) * N] = make_float2(re[j], im[j]);
-        }
-        // k_split_a's rows [Lr_hi, Li_hi, Lr_lo, Li_lo] (NB = 64 each)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const int o = 16 * c;
-          *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 0, false);
-          *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 2, false);
-          *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 1, false);
-          *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(re + 8 * c, im + 8 * c, 3, false);
-        }
+      for (int c = 0; c < 2; ++c) {
+        const int p = n0 / 8 + c;
+        *reinterpret_cast<uint4 *>(box + sw(0, p)) = pack8(re + 8 * c, im + 8 * c, 0, false);
+        *reinterpret_cast<uint4 *>(box + sw(1, p)) = pack8(re + 8 * c, im + 8 * c, 2, negb);
+        *reinterpret_cast<uint4 *>(box + sw(2, p)) = pack8(re + 8 * c, im + 8 * c, 1, false);
+        *reinterpret_cast<uint4 *>(box + sw(3, p)) = pack8(re + 8 * c, im + 8 * c, 3, negb);
       }
+    };
+    // one thread stores the four boxes: staging rows m0.. (segment q at x = 64 q), or U12 rows
+    // J + 16 q.. of columns J + jb + m0..
+    auto store_boxes = [&](const CUtensorMap *map, bool fp32_u) {
+      fence_async_smem();
       __syncthreads();
-      copy_rows(stg, Astage + ((size_t)b * N + m0) * 4 * NB, nv, t);
-    } else {
-      const int pc = jb / 2;                       // 16-byte pieces of a U12 column (jb is even)
-      // round 0: the tile's U12 columns; 1: k_split_b's real-part rows [Ur_hi, -Ui_hi, Ur_lo, -Ui_lo]
-#pragma unroll 1
-      for (int rnd = 0; rnd < 2; ++rnd) {
-        if (rnd) __syncthreads();
-        {
-          float re[16], im[16];
-          tload(0, re, im);
-          const int nn = n0;
-          if (rnd == 0) {
-            unsigned char *col = stg + r * TT_FROW + nn * 8;
+      if (t == 0) {
 #pragma unroll
-            for (int j = 0; j < 16; j += 2)
-              *reinterpret_cast<float4 *>(col + j * 8) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
-          } else {
-            unsigned char *row = stg + r * TT_SROW + nn * 2;
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-              const float *xr = re + 8 * c, *xi = im + 8 * c;
-              const int o = 16 * c;
-              *reinterpret_cast<uint4 *>(row + 0 * 128 + o) = pack8(xr, xi, 0, false);
-              *reinterpret_cast<uint4 *>(row + 1 * 128 + o) = pack8(xr, xi, 2, true);
-              *reinterpret_cast<uint4 *>(row + 2 * 128 + o) = pack8(xr, xi, 1, false);
-              *reinterpret_cast<uint4 *>(row + 3 * 128 + o) = pack8(xr, xi, 3, true);
-            }
-          }
+        for (int q = 0; q < 4; ++q) {
+          if (fp32_u) tma_store_3d(map, sA + q * TT_BOX, 2 * (J + 16 * q), J + jb + m0, b);
+          else tma_store_3d(map, sA + q * TT_BOX, 64 * q, m0, b);
         }
-        __syncthreads();
-        if (rnd == 0) {
-          for (int e = t; e < nv * pc; e += TT_THREADS) {
-            const int cc = e / pc, pp = e % pc;
-            *reinterpret_cast<float4 *>(Am + (size_t)(J + jb + m0 + cc) * N + J + 2 * pp) =
-                *reinterpret_cast<const float4 *>(stg + cc * TT_FROW + pp * 16);
-          }
-        } else {
-          copy_rows(stg, Bstage + ((size_t)b * Ncap + m0) * 4 * NB, nv, t);
-        }
+        bulk_commit();
       }
+    };
+    if (lower) {
+      float re[16], im[16];
+      tload(re, im);
+      // L21 into the matrix (row J+jb+m0+r, columns J+n): a warp stores 32 consecutive rows
+      if (r < nv) {
+        z32 *dst = Am + (size_t)(J + jb + m0 + r);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (n0 + j < jb) dst[(size_t)(J + n0 + j) * N] = make_float2(re[j], im[j]);
+      }
+      put_stage(re, im, false);
+      store_boxes(&maps.stA, false);
+    } else {
+      {
+        // U12 columns: box q holds rows J + 16 q .. + 15 of the tile's 128 columns (row r = column)
+        float re[16], im[16];
+        tload(re, im);
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+          *reinterpret_cast<float4 *>(box + sw(grp, p)) =
+              make_float4(re[2 * p], im[2 * p], re[2 * p + 1], im[2 * p + 1]);
+      }
+      store_boxes(&maps.u, true);
+      // the boxes are read before the staging overwrites them
+      if (t == 0) bulk_wait_read();
+      __syncthreads();
+      float re[16], im[16];
+      tload(re, im);
+      put_stage(re, im, true);
+      store_boxes(&maps.stB, false);
     }
+    // the stores have completed (the next kernels read them) before the CTA leaves
+    if (t == 0) bulk_wait_all();
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -906,6 +899,7 @@ struct TcCtx {
   int nsm = 0;
   bool persist = false;        // C tiles by TMA: needs 16-byte column and matrix strides
   CUtensorMap mapA[P_MAXST], mapB[P_MAXST], mapC;
+  CUtensorMap mapU;            // the matrix as FP32 columns, 128 B swizzled boxes (panel products' stores)
 };
 
 bool make_map(CUtensorMap *map, void *base, uint64_t inner, uint64_t rows, uint64_t batch) {
@@ -931,6 +925,21 @@ bool make_map_c(CUtensorMap *map, void *base, uint64_t N, uint64_t ncols, uint64
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// the matrix as FP32 for the panel products' U12 stores: dims (2N floats per column, columns,
+// matrices), box 16 complex rows x 128 columns, 128 B swizzle
+bool make_map_u(CUtensorMap *map, void *base, uint64_t N, uint64_t ncols, uint64_t strideM, uint64_t batch) {
+  encode_fn_t enc = tmap_encoder();
+  if (!enc) return false;
+  cuuint64_t dims[3] = {2 * N, ncols, batch};
+  cuuint64_t strides[2] = {N * 8, strideM * 8};
+  cuuint32_t box[3] = {32, 128, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
@@ -968,6 +977,7 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
   // the persistent kernel: C column stride (N * 8 B) and matrix stride on 16 bytes
   if (e == cudaSuccess && lb.N % 2 == 0 && lb.strideM % 2 == 0 &&
       make_map_c(&c->mapC, M, lb.N, lb.ncols, lb.strideM, lb.batch) &&
+      make_map_u(&c->mapU, M, lb.N, lb.ncols, lb.strideM, lb.batch) &&
       cudaFuncSetAttribute(k_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES) ==
           cudaSuccess) {
     int dev = 0;
@@ -1107,9 +1117,13 @@ cudaError_t tc_tri_step(void *ctxp, int first, int count, int J, int jb, int set
   if (ntA + ntU == 0 || count <= 0) return cudaSuccess;
   cudaError_t e = smem_limit(k_tc_tri, TT_SMEM_BYTES);
   if (e != cudaSuccess) return e;
+  TriMaps maps;
+  maps.stA = c->mapA[set];
+  maps.stB = c->mapB[set];
+  maps.u = c->mapU;
   k_tc_tri<<<(unsigned)((ntA + ntU) * count), TT_THREADS, TT_SMEM_BYTES, st>>>(
-      c->M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, lb.nsteps(), (const z32 *)lb.Linv, (const z32 *)lb.Uinv,
-      c->A[set], c->B[set], c->Ncap, first, ntA, ntU, c->err);
+      maps, c->M, lb.strideM, lb.N, lb.ncols, J, jb, lb.NB, lb.nsteps(), (const z32 *)lb.Linv,
+      (const z32 *)lb.Uinv, first, ntA, ntU, c->err);
   return ADGA_LAUNCH_CHECK();
 }
 
