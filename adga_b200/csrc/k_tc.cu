@@ -490,7 +490,11 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
 //   * the epilogue (thread = row of the tile) writes the FP32 result into the
 //     matrix and the step's operand staging of the trailing update
 //     (k_split_a's layout for L21, k_split_b's for U12), so no split kernel
-//     runs for the step.
+//     runs for the step: L21's FP32 rows straight from registers, the staging
+//     rows and U12's FP32 columns through 128 B swizzled boxes in the freed
+//     operand region, stored by TMA;
+//   * each thread first prefetches one line of the tile into L2, so that the
+//     tile's DRAM latency overlaps the B build.
 // The wait on the MMAs is bounded (WAIT_NS); on a timeout the CTA records an
 // error and skips its epilogue.
 // ---------------------------------------------------------------------------
