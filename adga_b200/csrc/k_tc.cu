@@ -262,7 +262,7 @@ __device__ __forceinline__ void mma_prod(uint32_t dacc, uint32_t sa, uint32_t sr
 // and each staging's row / column offset for the region's first C row / column
 constexpr int P_MAXST = 4;
 struct alignas(64) PMaps {
-  CUtensorMap a[P_MAXST], b[P_MAXST], c;
+  CUtensorMap a[P_MAXST], b[P_MAXST], c, c64;   // c64: C halves of 64 rows (regions of at most 64 rows)
 };
 struct POff {
   int ar[P_MAXST], bc[P_MAXST];
@@ -389,11 +389,14 @@ k_tc_persist(const __grid_constant__ PMaps maps, z32 *M, size_t strideM, int N, 
           if (u > 0) ok = mbar_wait(bar_cempty, (u - 1) & 1, err, 14);
           if (!ok) break;
           ++u;
-          mbar_expect_tx(bar_cfull, P_CH_BYTES);
+          // a region of at most 64 rows (the next step's rows in a delayed group) loads only those
+          const bool r64 = Mrows <= 64;
+          const CUtensorMap *mc = r64 ? &maps.c64 : &maps.c;
+          mbar_expect_tx(bar_cfull, r64 ? P_CH_BYTES / 2 : P_CH_BYTES);
           // x counts floats: rows crow0 + m.. as (re, im) pairs (crow0 even: 16-byte aligned)
-          tma_load_3d(scbase, &maps.c, bar_cfull, 2 * (crow0 + tm * BM), ccol0 + tn * BN + h * P_CH_COLS, b);
+          tma_load_3d(scbase, mc, bar_cfull, 2 * (crow0 + tm * BM), ccol0 + tn * BN + h * P_CH_COLS, b);
           if (h == 0 && tn * BN + P_CH_COLS < Ncols)
-            tma_prefetch_l2_3d(&maps.c, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
+            tma_prefetch_l2_3d(mc, 2 * (crow0 + tm * BM), ccol0 + tn * BN + P_CH_COLS, b);
         }
         if (!ok) break;
       }
@@ -412,6 +415,7 @@ k_tc_persist(const __grid_constant__ PMaps maps, z32 *M, size_t strideM, int N, 
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int m = tm * BM + row;
       const bool rowok = m < Mrows;
+      const int cld = Mrows <= 64 ? 64 : BM;     // rows per column of the C half in shared memory
       z32 *Cb = M + (size_t)b * strideM + (size_t)(crow0 + m);
       for (int h = 0; h < 2 && ok; ++h) {
         if (tn * BN + h * P_CH_COLS >= Ncols) break;     // no C loaded: outside the region
@@ -429,7 +433,7 @@ k_tc_persist(const __grid_constant__ PMaps maps, z32 *M, size_t strideM, int N, 
           tmem_ld16(tl + BN + c, im);
           z32 cv[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) cv[j] = cs[(grp * 32 + c + j) * BM + row];
+          for (int j = 0; j < 16; ++j) cv[j] = cs[(grp * 32 + c + j) * cld + (rowok ? row : 0)];
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
@@ -903,6 +907,7 @@ struct TcCtx {
   int nsm = 0;
   bool persist = false;        // C tiles by TMA: needs 16-byte column and matrix strides
   CUtensorMap mapA[P_MAXST], mapB[P_MAXST], mapC;
+  CUtensorMap mapC64;          // C halves of 64 rows
   CUtensorMap mapU;            // the matrix as FP32 columns, 128 B swizzled boxes (panel products' stores)
 };
 
@@ -919,13 +924,14 @@ bool make_map(CUtensorMap *map, void *base, uint64_t inner, uint64_t rows, uint6
   return r == CUDA_SUCCESS;
 }
 
-// C as FP32: dims (2N floats per column, columns, matrices), box 128 rows x 64 columns
-bool make_map_c(CUtensorMap *map, void *base, uint64_t N, uint64_t ncols, uint64_t strideM, uint64_t batch) {
+// C as FP32: dims (2N floats per column, columns, matrices), box `rows` rows x 64 columns
+bool make_map_c(CUtensorMap *map, void *base, uint64_t N, uint64_t ncols, uint64_t strideM, uint64_t batch,
+                uint32_t rows) {
   encode_fn_t enc = tmap_encoder();
   if (!enc) return false;
   cuuint64_t dims[3] = {2 * N, ncols, batch};
   cuuint64_t strides[2] = {N * 8, strideM * 8};
-  cuuint32_t box[3] = {2 * BM, P_CH_COLS, 1};
+  cuuint32_t box[3] = {2 * rows, P_CH_COLS, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -980,7 +986,8 @@ cudaError_t tc_trail_setup(void **ctx_out, z32 *M, const LUBatch &lb, cudaStream
     e = cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   // the persistent kernel: C column stride (N * 8 B) and matrix stride on 16 bytes
   if (e == cudaSuccess && lb.N % 2 == 0 && lb.strideM % 2 == 0 &&
-      make_map_c(&c->mapC, M, lb.N, lb.ncols, lb.strideM, lb.batch) &&
+      make_map_c(&c->mapC, M, lb.N, lb.ncols, lb.strideM, lb.batch, BM) &&
+      make_map_c(&c->mapC64, M, lb.N, lb.ncols, lb.strideM, lb.batch, 64) &&
       make_map_u(&c->mapU, M, lb.N, lb.ncols, lb.strideM, lb.batch) &&
       cudaFuncSetAttribute(k_tc_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES) ==
           cudaSuccess) {
@@ -1017,6 +1024,7 @@ cudaError_t persist_region(TcCtx *c, int nst, const int *ar, const int *bc, int 
     off.bc[i] = i < nst ? bc[i] : 0;
   }
   maps.c = c->mapC;
+  maps.c64 = c->mapC64;
   k_tc_persist<<<grid, P_THREADS, P_SMEM_BYTES, st>>>(maps, c->M, lb.strideM, lb.N, crow0, ccol0, off, nst,
                                                        lb.NB / BK, Mrows, Ncols, first, count, c->err);
   return ADGA_LAUNCH_CHECK();
